@@ -1,0 +1,317 @@
+#!/usr/bin/env python
+"""Benchmark: batched exact pi(x) queries on B200.
+
+Workload (one step): 4096 queries x = floor(10^e), e ~ U[9, 14] drawn from
+numpy default_rng(0), all answered by one call of the public batch API
+(cudapix_b200.pi_batch -> cpx_pi_batch), every answer exact.  Synthetic
+inputs; the reference publishes no dataset or numbers for this path.
+
+  value            queries/s over the device timeline of the batch kernels
+                   (CUDA events on the context stream; query list already
+                   planned, tables resident)
+  e2e              queries/s through the C ABI with host buffers: planning,
+                   host->device copy of the queries, kernels, device->host read
+  plain            the same queries one pi_deleglise_rivat call (one launch
+                   sequence) each, with p50/p99 latency
+  cpu_baseline     the oracle's OpenMP restatement of the term pipeline on
+                   the host cores, on a bounded sample of the same queries
+
+`--impl reference` times that CPU restatement alone (the reference itself
+cannot be built: its CUDASieve / CUDA-uint128 dependencies are not vendored).
+Multi-GPU (`torchrun ... --gpus N`): independent replicas, each GPU answers
+its own 4096-query batch; barrier + max over ranks; value = all queries / max time.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "pi(x) queries/sec (batched, exact)"
+UNIT = "queries/s"
+
+
+def workload(n, seed=0, lo=9.0, hi=14.0):
+    e = np.random.default_rng(seed).uniform(lo, hi, n)
+    return [int(10.0**v) for v in e]
+
+
+class Clocks:
+    """nvidia-smi sampler running during the timed region."""
+
+    def __init__(self, dev):
+        self.dev = dev
+        self.proc = None
+        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_{os.getpid()}.csv")
+
+    def __enter__(self):
+        try:
+            os.makedirs(os.path.dirname(self.path), exist_ok=True)
+            self.f = open(self.path, "w")
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.dev}",
+                 "--query-gpu=index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+                 "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+                 "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        if self.proc:
+            time.sleep(0.25)
+            self.proc.terminate()
+            try:
+                self.proc.wait(5)
+            except Exception:
+                self.proc.kill()
+            self.f.close()
+
+    def summary(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        rows = []
+        for line in open(self.path):
+            p = [s.strip() for s in line.split(",")]
+            if len(p) < 9:
+                continue
+            try:
+                rows.append((float(p[1]), float(p[2]), p[5:9]))
+            except ValueError:
+                continue
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for _, _, r in rows for i, v in enumerate(r) if v.lower() == "active"})
+        return {"sm_mhz": statistics.median(r[0] for r in rows), "sm_max_mhz": max(r[1] for r in rows),
+                "reasons": reasons, "samples": len(rows)}
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            m = json.load(f)
+        return m["hbm_gbs"], "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def profile_traffic():
+    """DRAM bytes per launch of the dominant kernel from the committed ncu summary."""
+    p = os.path.join(ROOT, "profiles", "traffic.json")
+    try:
+        with open(p) as f:
+            return json.load(f)
+    except Exception:
+        return None
+
+
+def cpu_baseline(xs, budget_s):
+    import oracle
+
+    nthreads = os.cpu_count() or 1
+    done, t0 = 0, time.perf_counter()
+    for x in xs:
+        y = oracle.default_y(x, *alpha_frac(x))
+        oracle.pi_dr(x, y, 6, nthreads)
+        done += 1
+        if time.perf_counter() - t0 > budget_s:
+            break
+    dt = time.perf_counter() - t0
+    return {"value": done / dt, "unit": UNIT, "cores": nthreads, "kind": "port",
+            "sample": f"first {done} of the {len(xs)} workload queries (x log-uniform in [1e9, 1e14]), "
+                      f"oracle/oracle.c orc_pi_dr, OpenMP {nthreads} threads, {dt:.1f} s"}
+
+
+def alpha_frac(x):
+    # the library's default alpha (reference alpha(x), src/main.cpp:128-194), as num/den
+    import cudapix_b200 as cpx
+    from cudapix_b200 import _lib
+
+    return _lib.load().cpx_alpha_milli(_lib.U128.of(x)), 1000
+
+
+def dist_setup():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    return world, rank, local
+
+
+def allmax(v, world):
+    if world == 1:
+        return v
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([float(v)], device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.barrier()
+
+
+def run_reference(args, world, rank):
+    if rank != 0:
+        return
+    xs = workload(args.queries)
+    nthreads = os.cpu_count() or 1
+    import oracle
+
+    per_step = []
+    sample = None
+    for k in range(args.warmup + args.steps):
+        t0 = time.perf_counter()
+        done = 0
+        for x in xs:
+            oracle.pi_dr(x, oracle.default_y(x, *alpha_frac(x)), 6, nthreads)
+            done += 1
+            if time.perf_counter() - t0 > args.ref_step_s:
+                break
+        dt = time.perf_counter() - t0
+        if k >= args.warmup:
+            per_step.append((done, dt))
+        sample = f"per step the first {done} of the {len(xs)} workload queries, oracle/oracle.c orc_pi_dr, OpenMP {nthreads} threads"
+    q = sum(d for d, _ in per_step)
+    t = sum(s for _, s in per_step)
+    v = q / t
+    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1000 * t / len(per_step), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "int64/int128", "data": "synthetic",
+            "config": {"workload": "batch4096: x = floor(10^e), e ~ U[9,14], numpy default_rng(0)",
+                       "queries": args.queries, "c": 6, "alpha": "reference alpha(x)"},
+            "cpu_baseline": {"value": v, "unit": UNIT, "cores": nthreads, "kind": "port", "sample": sample},
+            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--queries", type=int, default=4096)
+    ap.add_argument("--plain", type=int, default=256, help="queries timed through the plain per-query path")
+    ap.add_argument("--cpu-budget", type=float, default=15.0)
+    ap.add_argument("--ref-step-s", type=float, default=20.0)
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+    world, rank, local = dist_setup()
+    if args.impl == "reference":
+        run_reference(args, world, rank)
+        return
+
+    import cudapix_b200 as cpx
+
+    ctx = cpx.Context(local)
+    ctx.set_timing(True)
+    xs = workload(args.queries, seed=0)
+    ref = None
+    for _ in range(max(args.warmup, 3)):
+        out = cpx.pi_batch(xs, ctx=ctx)
+        if ref is None:
+            ref = out
+        assert out == ref, "batch results changed between runs"
+
+    launches0 = ctx.launches
+    dev_ms, e2e_ms, hard_ms, hard_bytes = [], [], [], []
+    barrier(world)
+    with Clocks(local) as clk:
+        for _ in range(args.steps):
+            ctx.flush_l2()
+            ctx.timer_start()
+            out = cpx.pi_batch(xs, ctx=ctx)
+            e2e_ms.append(ctx.timer_stop())
+            dev_ms.append(ctx.last_batch_ms())
+            hm, hb = ctx.last_hard_stats()
+            hard_ms.append(hm)
+            hard_bytes.append(hb)
+            assert out == ref
+    barrier(world)
+    import ctypes
+
+    h2d, d2h = ctypes.c_uint64(), ctypes.c_uint64()
+    ctx.call("cpx_last_batch_io", ctypes.byref(h2d), ctypes.byref(d2h))
+    io = (h2d.value, d2h.value)
+    launches = (ctx.launches - launches0) // args.steps
+    t_dev = allmax(sum(dev_ms) / 1000.0, world)
+    t_e2e = allmax(sum(e2e_ms) / 1000.0, world)
+    nq = world * args.queries * args.steps
+    value = nq / t_dev
+
+    # plain path: one full launch sequence per query, on a fixed subsample
+    plain = None
+    if args.plain and rank == 0:
+        sub = xs[: args.plain]
+        lat = []
+        for x in sub:
+            ctx.timer_start()
+            p = cpx.pi_deleglise_rivat(x, 0, 6, ctx=ctx)
+            lat.append(ctx.timer_stop())
+            assert p == ref[xs.index(x)]
+        lat.sort()
+        plain = {"value": len(sub) / (sum(lat) / 1000.0), "unit": UNIT, "queries": len(sub),
+                 "p50_ms": lat[len(lat) // 2], "p99_ms": lat[min(len(lat) - 1, int(len(lat) * 0.99))]}
+
+    if rank != 0:
+        return
+    hbm, kind = peaks()
+    hb = hard_bytes[-1]
+    hs = statistics.median(hard_ms) / 1000.0
+    tr = profile_traffic()
+    roof = {"bound": "hbm", "kernel": "k_hard (special-leaf phi sieve)", "achieved": (hb / hs) / 1e9 if hs else None,
+            "peak": hbm, "unit": "GB/s", "frac": ((hb / hs) / 1e9) / hbm if hs else None,
+            "peak_kind": kind, "traffic": tr.get("k_hard_dram_bytes_per_launch") if tr else None,
+            "note": "achieved = S2 bitmap bytes (one pass of the segment bitmap per active prime per segment) / "
+                    "k_hard duration; these passes run in shared memory, so the HBM fraction is a proxy"}
+    cpu = None if args.no_cpu else cpu_baseline(xs, args.cpu_budget)
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": max(args.warmup, 3), "ms_per_step": 1000 * t_dev / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "int64/int128", "data": "synthetic",
+        "config": {"workload": "batch4096: x = floor(10^e), e ~ U[9,14], numpy default_rng(0)",
+                   "queries": args.queries, "c": 6, "alpha": "reference alpha(x)",
+                   "l2": "flushed before every timed step (256 MiB write)",
+                   "parallelism": f"replicas x{world}"},
+        "e2e": {"value": nq / t_e2e, "unit": UNIT, "h2d_bytes_per_step": io[0], "d2h_bytes_per_step": io[1]},
+        "gpu_launches": int(launches),
+        "plain": plain,
+        "batched_over_plain": (value / plain["value"]) if plain else None,
+        "e2e_over_plain": ((nq / t_e2e) / plain["value"]) if plain else None,
+        "s2_gbs": (hb / hs) / 1e9 if hs else None,
+        "roofline": roof,
+        "cpu_baseline": cpu,
+        "clocks": clk.summary(),
+    }
+    print(json.dumps(line), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

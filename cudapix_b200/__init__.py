@@ -1,0 +1,508 @@
+"""cudapix_b200 -- exact pi(x) by Deleglise-Rivat on B200 (sm_100a).
+
+Python mirror of the reference's term entry points (curtisseizert/CUDApix),
+over the C ABI in include/cpx.h.  Names and argument meanings follow the
+reference:
+
+    P2(x, y)                      include/P2.cuh:16-17
+    S2_trivial(x, y)              include/trivial.cuh:8,12
+    Ordinary(x, y, c)             include/ordinary.cuh:6-7
+    S2hard(x, y, c)               include/sieve/S2_hard_host.cuh:35-36
+    pi_deleglise_rivat(x, y, c)   include/Deleglise-Rivat/deleglise-rivat.hpp:28,64
+    mutest(top)                   include/mutest.cuh:3
+    gen_d_mu / gen_d_lpf / gen_h_mu / gen_h_lpf / gen_d_mu_lpf
+                                  include/sieve/lpf_mu.cuh:12-24
+    get_d_piTable(hi), PiTable    include/pitable.cuh:7,12-51
+    Phi                           include/phi.cuh:17-36
+    Phisieve                      include/sieve/phisieve_host.cuh:6-40
+    get_device_primes / count_primes   CUDASieve (external dependency)
+
+Errors raise CpxError (the reference checked none).  Every value is an exact
+Python int; 64- and 128-bit overloads are chosen by the size of x.
+"""
+import ctypes
+
+from ._lib import CpxError, ExtensionMissing, Params, Terms, U128, header_symbols, load  # noqa: F401
+
+__all__ = [
+    "Context", "context", "P2", "S2_trivial", "Ordinary", "S2_easy", "S2hard", "pi_deleglise_rivat",
+    "pi_terms", "pi", "pi_batch", "mutest", "gen_d_mu", "gen_d_lpf", "gen_h_mu", "gen_h_lpf", "gen_d_mu_lpf",
+    "get_d_piTable", "PiTable", "Phi", "Phisieve", "get_device_primes", "count_primes", "DeviceArray",
+    "default_y", "iroots", "CpxError", "ExtensionMissing",
+]
+
+_U64 = (1 << 64) - 1
+
+
+class DeviceArray:
+    """A cudaMalloc'd buffer returned by the library (caller-owned, like the
+    reference's gen_d_* / get_d_piTable pointers)."""
+
+    def __init__(self, ptr, n, ctype, owned=True):
+        self.ptr, self.n, self.ctype, self.owned = ptr, n, ctype, owned
+
+    def to_host(self):
+        import numpy as np
+
+        dt = np.dtype(self.ctype)
+        out = np.empty(self.n, dtype=dt)
+        if self.n:
+            _check(None, load().cpx_copy_to_host(out.ctypes.data, self.ptr, self.n * dt.itemsize))
+        return out
+
+    def free(self):
+        if self.owned and self.ptr:
+            load().cpx_free(self.ptr)
+        self.ptr = None
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass
+
+
+def _check(ctx, rc):
+    if rc != 0:
+        msg = load().cpx_last_error(ctx.h).decode() if ctx is not None else "device copy failed"
+        raise CpxError(rc, msg)
+
+
+class Context:
+    """Owns a CUDA stream and the resident tables on one device."""
+
+    def __init__(self, device=0):
+        L = load()
+        h = ctypes.c_void_p()
+        rc = L.cpx_create(device, ctypes.byref(h))
+        if rc != 0:
+            raise CpxError(rc, f"cannot create a context on device {device}")
+        self.h = h
+        self.L = L
+        self.device = device
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.L.cpx_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def call(self, name, *args):
+        _check(self, getattr(self.L, name)(self.h, *args))
+
+    @property
+    def stream(self):
+        return self.L.cpx_stream(self.h)
+
+    @property
+    def launches(self):
+        return self.L.cpx_launch_count(self.h)
+
+    def set_hard_params(self, log2_bits, threads):
+        self.call("cpx_set_hard_params", log2_bits, threads)
+
+    def set_timing(self, on=True):
+        self.call("cpx_set_timing", 1 if on else 0)
+
+    def last_hard_stats(self):
+        ms, by = ctypes.c_float(), ctypes.c_double()
+        self.call("cpx_last_hard_stats", ctypes.byref(ms), ctypes.byref(by))
+        return ms.value, by.value
+
+    def last_batch_ms(self):
+        ms = ctypes.c_float()
+        self.call("cpx_last_batch_ms", ctypes.byref(ms))
+        return ms.value
+
+    def timer_start(self):
+        self.call("cpx_timer_start")
+
+    def timer_stop(self):
+        ms = ctypes.c_float()
+        self.call("cpx_timer_stop", ctypes.byref(ms))
+        return ms.value
+
+    def flush_l2(self):
+        self.call("cpx_flush_l2")
+
+    def mem_info(self):
+        f, t = ctypes.c_uint64(), ctypes.c_uint64()
+        self.call("cpx_mem_info", ctypes.byref(f), ctypes.byref(t))
+        return f.value, t.value
+
+
+_default = {}
+
+
+def context(device=0):
+    if device not in _default:
+        _default[device] = Context(device)
+    return _default[device]
+
+
+def _wide(x):
+    return x > _U64
+
+
+def iroots(x):
+    s, c, q = ctypes.c_uint64(), ctypes.c_uint64(), ctypes.c_uint64()
+    load().cpx_iroots(U128.of(x), ctypes.byref(s), ctypes.byref(c), ctypes.byref(q))
+    return s.value, c.value, q.value
+
+
+def default_y(x, alpha=None):
+    """y = floor(alpha * icbrt(x)) (src/main.cpp:59-64), alpha an int or
+    Fraction; None = the reference's alpha(x) (src/main.cpp:128-194)."""
+    from fractions import Fraction
+
+    if alpha is None:
+        num, den = 0, 0
+    else:
+        f = Fraction(alpha).limit_denominator(1000)
+        num, den = f.numerator, f.denominator
+    y = ctypes.c_uint64()
+    load().cpx_default_y(U128.of(x), num, den, ctypes.byref(y))
+    return y.value
+
+
+# ---------------------------------------------------------------- terms
+
+def P2(x, y, ctx=None):
+    ctx = ctx or context()
+    if _wide(x):
+        o = U128()
+        ctx.call("cpx_P2_u128", U128.of(x), y, ctypes.byref(o))
+        return o.value(signed=True)
+    o = ctypes.c_uint64()
+    ctx.call("cpx_P2_u64", x, y, ctypes.byref(o))
+    return o.value
+
+
+def S2_trivial(x, y, ctx=None):
+    ctx = ctx or context()
+    if _wide(x):
+        o = U128()
+        ctx.call("cpx_trivial_u128", U128.of(x), y, ctypes.byref(o))
+        return o.value(signed=True)
+    o = ctypes.c_uint64()
+    ctx.call("cpx_trivial_u64", x, y, ctypes.byref(o))
+    return o.value
+
+
+def Ordinary(x, y, c=6, ctx=None):
+    ctx = ctx or context()
+    if _wide(x):
+        o = U128()
+        ctx.call("cpx_ordinary_u128", U128.of(x), y, c, ctypes.byref(o))
+        return o.value(signed=True)
+    o = ctypes.c_int64()
+    ctx.call("cpx_ordinary_u64", x, y, c, ctypes.byref(o))
+    return o.value
+
+
+def S2_easy(x, y, ctx=None):
+    ctx = ctx or context()
+    if _wide(x):
+        o = U128()
+        ctx.call("cpx_S2_easy_u128", U128.of(x), y, ctypes.byref(o))
+        return o.value(signed=True)
+    o = ctypes.c_int64()
+    ctx.call("cpx_S2_easy_u64", x, y, ctypes.byref(o))
+    return o.value
+
+
+def S2hard(x, y, c=6, ctx=None):
+    ctx = ctx or context()
+    if _wide(x):
+        o = U128()
+        ctx.call("cpx_S2_hard_u128", U128.of(x), y, c, ctypes.byref(o))
+        return o.value(signed=True)
+    o = ctypes.c_int64()
+    ctx.call("cpx_S2_hard_u64", x, y, c, ctypes.byref(o))
+    return o.value
+
+
+def pi_terms(x, y=0, c=6, ctx=None):
+    """Every term of pi(x) as a dict (P2, ordinary, trivial, easy, hard, pi_y, pi, x, y, z, c)."""
+    ctx = ctx or context()
+    t = Terms()
+    if _wide(x):
+        o = U128()
+        ctx.call("cpx_pi_u128", U128.of(x), y, c, ctypes.byref(o), ctypes.byref(t))
+    else:
+        o = ctypes.c_uint64()
+        ctx.call("cpx_pi_u64", x, y, c, ctypes.byref(o), ctypes.byref(t))
+    return t.as_dict()
+
+
+def pi_deleglise_rivat(x, y=0, c=6, ctx=None):
+    return pi_terms(x, y, c, ctx)["pi"]
+
+
+def pi(x, ctx=None):
+    return pi_deleglise_rivat(x, 0, 6, ctx)
+
+
+def pi_batch(xs, alpha=None, c=6, hard_log2_bits=0, hard_threads=0, ctx=None):
+    """pi(x) for every x in xs in one batched device pass."""
+    from fractions import Fraction
+
+    ctx = ctx or context()
+    n = len(xs)
+    arr = (U128 * max(n, 1))()
+    for i, x in enumerate(xs):
+        arr[i] = U128.of(x)
+    out = (U128 * max(n, 1))()
+    p = Params()
+    if alpha is not None:
+        f = Fraction(alpha).limit_denominator(1000)
+        p.alpha_num, p.alpha_den = f.numerator, f.denominator
+    p.c = c
+    p.hard_log2_bits = hard_log2_bits
+    p.hard_threads = hard_threads
+    ctx.call("cpx_pi_batch", arr, n, ctypes.byref(p), out)
+    return [out[i].value() for i in range(n)]
+
+
+# ---------------------------------------------------------- sieves / tables
+
+def mutest(top, ctx=None):
+    ctx = ctx or context()
+    o = ctypes.c_int64()
+    ctx.call("cpx_mutest", top, ctypes.byref(o))
+    return o.value
+
+
+def gen_d_mu(bottom, top, ctx=None):
+    ctx = ctx or context()
+    p = ctypes.c_void_p()
+    ctx.call("cpx_gen_d_mu", bottom, top, ctypes.byref(p))
+    return DeviceArray(p.value, (top - bottom) // 2, "int8")
+
+
+def gen_d_lpf(bottom, top, wide=False, ctx=None):
+    ctx = ctx or context()
+    p = ctypes.c_void_p()
+    if wide or top > (1 << 32):
+        ctx.call("cpx_gen_d_lpf64", bottom, top, ctypes.byref(p))
+        return DeviceArray(p.value, (top - bottom) // 2, "uint64")
+    ctx.call("cpx_gen_d_lpf32", bottom, top, ctypes.byref(p))
+    return DeviceArray(p.value, (top - bottom) // 2, "uint32")
+
+
+def gen_d_mu_lpf(bottom, top, ctx=None):
+    """Returns (mu int8, lpf uint64) device arrays (src/sieve/lpf_mu.cu:282-302)."""
+    ctx = ctx or context()
+    n = (top - bottom) // 2
+    L = load()
+    pm, pl = ctypes.c_void_p(), ctypes.c_void_p()
+    _check(None, L.cpx_device_alloc(max(n, 1), ctypes.byref(pm)))
+    _check(None, L.cpx_device_alloc(max(n, 1) * 8, ctypes.byref(pl)))
+    ctx.call("cpx_gen_d_mu_lpf", bottom, top, pm, pl)
+    return DeviceArray(pm.value, n, "int8"), DeviceArray(pl.value, n, "uint64")
+
+
+def gen_h_mu(bottom, top, ctx=None):
+    import numpy as np
+
+    ctx = ctx or context()
+    out = np.zeros((top - bottom) // 2, dtype=np.int8)
+    ctx.call("cpx_gen_h_mu", bottom, top, out.ctypes.data)
+    return out
+
+
+def gen_h_lpf(bottom, top, ctx=None):
+    import numpy as np
+
+    ctx = ctx or context()
+    out = np.zeros((top - bottom) // 2, dtype=np.uint32)
+    ctx.call("cpx_gen_h_lpf32", bottom, top, out.ctypes.data)
+    return out
+
+
+def get_d_piTable(hi, ctx=None):
+    """Dense table t[k] = pi(2k - 1), k < hi/2 (src/pitable.cu:10-25)."""
+    ctx = ctx or context()
+    p = ctypes.c_void_p()
+    ctx.call("cpx_pitable", hi, ctypes.byref(p))
+    return DeviceArray(p.value, hi // 2, "uint32")
+
+
+def get_device_primes(bottom, top, ctx=None):
+    """Primes in [bottom, top) (CudaSieve::getDevicePrimes)."""
+    ctx = ctx or context()
+    p, n = ctypes.c_void_p(), ctypes.c_uint64()
+    ctx.call("cpx_primes", bottom, top, ctypes.byref(p), ctypes.byref(n))
+    return DeviceArray(p.value, n.value, "uint64")
+
+
+def count_primes(bottom, top, ctx=None):
+    """Number of primes in [bottom, top) (CudaSieve::countPrimes)."""
+    ctx = ctx or context()
+    n = ctypes.c_uint64()
+    ctx.call("cpx_count_primes", bottom, top, ctypes.byref(n))
+    return n.value
+
+
+class PiTable:
+    """Windowed pi table (src/pitable.cu:27-218): table[k] = pi(base + 2k - 1) - pi_base
+    for k < range/2 + 2, walked up or down in windows of `range`."""
+
+    def __init__(self, *args, ctx=None):
+        self.ctx = ctx or context()
+        if len(args) == 1:
+            self.base, self.bottom, self.range = 0, 0, int(args[0])
+        elif len(args) in (2, 3):
+            self.base, self.bottom = int(args[0]), int(args[1])
+            rng = int(args[2]) if len(args) == 3 else 0
+            self.range = rng if rng else min(self.getMaxRange(), self.base - self.bottom)
+        else:
+            raise TypeError("PiTable(range) or PiTable(base, bottom, range=0)")
+        self._buf = None
+        self._alloc()
+        self.pi_base = None
+
+    def _alloc(self):
+        L = load()
+        p = ctypes.c_void_p()
+        _check(None, L.cpx_device_alloc((self.range // 2 + 2) * 4, ctypes.byref(p)))
+        if self._buf is not None:
+            self._buf.free()
+        self._buf = DeviceArray(p.value, self.range // 2 + 2, "uint32")
+
+    def getMaxRange(self):
+        free, _ = self.ctx.mem_info()
+        return int(free / 2.5)
+
+    def get_base(self):
+        return self.base
+
+    def get_range(self):
+        return self.range
+
+    def get_bottom(self):
+        return self.bottom
+
+    def get_pi_base(self):
+        if self.base == 0:
+            return 0
+        return count_primes(0, self.base, ctx=self.ctx)
+
+    def set_base(self, base):
+        self.base = int(base)
+
+    def set_range(self, rng):
+        self.range = int(rng)
+        self._alloc()
+
+    def set_bottom(self, bottom):
+        self.bottom = int(bottom)
+
+    def _fill(self):
+        pb = ctypes.c_uint64()
+        self.ctx.call("cpx_pitable_window", self.base, self.range, self._buf.ptr, ctypes.byref(pb))
+        self.pi_base = pb.value
+        return self._buf
+
+    def getCurrent(self):
+        return self._fill()
+
+    def getNextUp(self):
+        self.base += self.range
+        return self._fill()
+
+    def getNextDown(self):
+        if self.bottom < self.base - self.range:
+            self.base -= self.range
+        else:
+            self.range = self.base - self.bottom
+            self.base = self.bottom
+        return self._fill()
+
+    def getNextBaseUp(self):
+        return self.base + self.range
+
+    def getNextBaseDown(self):
+        return max(self.bottom, self.base - self.range)
+
+
+class Phi:
+    """phi(x, a) and phi prefix ranges (src/phi.cu:14-109).
+
+    Index convention of the reference: phi(x, a) excludes the primes up to
+    smallPrimes[a] / h_primeList[a - 12] (0-based), i.e. the first a + 1
+    primes; phi_std(x, a) is the textbook phi with the first a primes."""
+
+    def __init__(self, max_, p_max=None, ctx=None):
+        self.ctx = ctx or context()
+        self.max = int(max_)
+        self.p_max = p_max
+
+    def phi(self, x, a):
+        return self.phi_std(x, a + 1)
+
+    def phi_std(self, x, a):
+        o = ctypes.c_uint64()
+        self.ctx.call("cpx_phi", x, a, ctypes.byref(o))
+        return o.value
+
+    def generateRange(self, num, a):
+        """t[i] = phi(2i + 1, a + 1) (inclusive count), i < num/2."""
+        p = ctypes.c_void_p()
+        self.ctx.call("cpx_phi_range", num, a + 1, ctypes.byref(p))
+        return DeviceArray(p.value, num // 2, "uint32")
+
+
+class Phisieve:
+    """Odd-only bit sieve with a count table counts[i] = phi(2i - 1, a)
+    (src/sieve/phisieve_host.cu:12-89)."""
+
+    def __init__(self, maxPrime, blockSize=1 << 28, ctx=None):
+        self.ctx = ctx or context()
+        self.blockSize = int(blockSize)
+        h = ctypes.c_void_p()
+        self.ctx.call("cpx_phisieve_create", maxPrime, self.blockSize, ctypes.byref(h))
+        self.h = h
+
+    def _c(self, name, *args):
+        rc = getattr(load(), name)(self.h, *args)
+        if rc != 0:
+            raise CpxError(rc, load().cpx_last_error(self.ctx.h).decode())
+
+    def firstSieve(self, c):
+        self._c("cpx_phisieve_first", c)
+
+    def markNext(self):
+        self._c("cpx_phisieve_mark_next")
+
+    def updateCount(self):
+        self._c("cpx_phisieve_update")
+
+    def get_a_current(self):
+        a = ctypes.c_uint32()
+        self._c("cpx_phisieve_counts", None, ctypes.byref(a))
+        return a.value
+
+    def getCountDevice(self):
+        p, a = ctypes.c_void_p(), ctypes.c_uint32()
+        self._c("cpx_phisieve_counts", ctypes.byref(p), ctypes.byref(a))
+        return DeviceArray(p.value, self.blockSize, "uint32", owned=False)
+
+    def getCountHost(self):
+        return self.getCountDevice().to_host()
+
+    def close(self):
+        if getattr(self, "h", None):
+            load().cpx_phisieve_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -1,0 +1,137 @@
+// cpx_int.cuh -- exact integer helpers shared by host and device code.
+//
+// Replaces the CUDA-uint128 dependency of the reference (its uint128_t,
+// mul128, _isqrt/_icbrt/_iqrt call sites are listed at
+// src/Deleglise-Rivat/deleglise-rivat.cpp:99-102, src/P2.cu:23,
+// src/main.cpp:61,165).  Every root here is an exact floor root computed in
+// integers; no floating point value ever reaches a count.
+#pragma once
+#include <cstdint>
+
+#if defined(__CUDACC__)
+#define CPX_HD __host__ __device__ __forceinline__
+#else
+#define CPX_HD inline
+#endif
+
+typedef unsigned __int128 u128;
+typedef __int128 i128;
+
+// ------------------------------------------------------------------ roots
+// Integer Newton iteration from an over-estimate (a power of two above the
+// root), which decreases monotonically to the floor root.
+
+CPX_HD int cpx_bitlen128(u128 x)
+{
+    uint64_t hi = (uint64_t)(x >> 64), lo = (uint64_t)x;
+#if defined(__CUDA_ARCH__)
+    if (hi) return 128 - __clzll((long long)hi);
+    return lo ? 64 - __clzll((long long)lo) : 0;
+#else
+    if (hi) return 128 - __builtin_clzll(hi);
+    return lo ? 64 - __builtin_clzll(lo) : 0;
+#endif
+}
+
+CPX_HD uint64_t cpx_isqrt(u128 x)
+{
+    if (x < 2) return (uint64_t)x;
+    int b = cpx_bitlen128(x);
+    u128 r = (u128)1 << ((b + 1) / 2); // r >= sqrt(x)
+    for (;;) {
+        u128 n = (r + x / r) >> 1;
+        if (n >= r) break;
+        r = n;
+    }
+    return (uint64_t)r;
+}
+
+CPX_HD uint64_t cpx_icbrt(u128 x)
+{
+    if (x < 8) return x ? 1 : 0;
+    int b = cpx_bitlen128(x);
+    u128 r = (u128)1 << ((b + 2) / 3); // r >= cbrt(x)
+    for (;;) {
+        u128 n = (2 * r + x / (r * r)) / 3;
+        if (n >= r) break;
+        r = n;
+    }
+    return (uint64_t)r;
+}
+
+CPX_HD uint64_t cpx_iroot4(u128 x) { return cpx_isqrt((u128)cpx_isqrt(x)); }
+
+// --------------------------------------------------------- table lookups
+// Compressed prime table: entry w covers the odd numbers 128w+1 .. 128w+127,
+// .x = bitmap (bit j <-> 128w + 2j + 1 is prime), .y = number of odd primes
+// below 128w.  pi(n) = [n >= 2] + .y + popcount(.x & mask(n)).
+
+struct __align__(16) cpx_pient {
+    uint64_t bits;
+    uint64_t pre;
+};
+
+CPX_HD uint64_t cpx_pi_from_entry(cpx_pient e, uint64_t n)
+{
+    uint32_t j = (uint32_t)(((n - 1) & 127) >> 1);
+    uint64_t mask = (2ull << j) - 1; // j == 63 wraps to all ones
+#if defined(__CUDA_ARCH__)
+    return 1 + e.pre + (uint64_t)__popcll(e.bits & mask);
+#else
+    return 1 + e.pre + (uint64_t)__builtin_popcountll(e.bits & mask);
+#endif
+}
+
+#if defined(__CUDACC__)
+__device__ __forceinline__ uint64_t cpx_pi_dev(const cpx_pient *__restrict__ T, uint64_t n)
+{
+    if (n < 2) return 0;
+    const ulonglong2 v = __ldg(reinterpret_cast<const ulonglong2 *>(T) + ((n - 1) >> 7));
+    cpx_pient e{v.x, v.y};
+    return cpx_pi_from_entry(e, n);
+}
+
+// ------------------------------------------------ 128-bit atomic accumulate
+// Two 64-bit atomics; the carry out of the low word is added to the high word
+// by the same thread, which makes the final 128-bit total exact in any order.
+__device__ __forceinline__ void cpx_atomic_add_i128(unsigned long long *dst, i128 v)
+{
+    unsigned long long lo = (unsigned long long)(u128)v;
+    unsigned long long hi = (unsigned long long)((u128)v >> 64);
+    unsigned long long old = atomicAdd(dst, lo);
+    hi += (old + lo < old) ? 1ull : 0ull;
+    if (hi) atomicAdd(dst + 1, hi);
+}
+
+__device__ __forceinline__ i128 cpx_shfl_down_i128(i128 v, int d)
+{
+    unsigned long long lo = (unsigned long long)(u128)v, hi = (unsigned long long)((u128)v >> 64);
+    lo = __shfl_down_sync(0xffffffffu, lo, d);
+    hi = __shfl_down_sync(0xffffffffu, hi, d);
+    return (i128)(((u128)hi << 64) | lo);
+}
+
+__device__ __forceinline__ i128 cpx_warp_sum_i128(i128 v)
+{
+#pragma unroll
+    for (int d = 16; d > 0; d >>= 1) v += cpx_shfl_down_i128(v, d);
+    return v;
+}
+
+// Block-wide sum of an i128 held by every thread; result valid in thread 0.
+// `sh` needs 32 entries.  All threads of the block must call it.
+__device__ __forceinline__ i128 cpx_block_sum_i128(i128 v, i128 *sh)
+{
+    v = cpx_warp_sum_i128(v);
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    __syncthreads();
+    if (lane == 0) sh[w] = v;
+    __syncthreads();
+    i128 r = 0;
+    if (threadIdx.x < 32) {
+        r = (threadIdx.x < (blockDim.x >> 5)) ? sh[threadIdx.x] : (i128)0;
+        r = cpx_warp_sum_i128(r);
+    }
+    return r;
+}
+#endif

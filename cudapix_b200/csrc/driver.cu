@@ -1,0 +1,292 @@
+// driver.cu -- host planning and execution of a batch of pi(x) queries (or of
+// single terms) over the resident tables.
+//
+// Restates the reference driver (src/Deleglise-Rivat/deleglise-rivat.cpp:13-80:
+// bounds, pi values at the bounds, the term identity) with exact integer
+// roots, and replaces its one-term-at-a-time, synchronise-after-every-launch
+// flow with one pass of a handful of kernels over every query of a batch.
+#include <algorithm>
+#include <cmath>
+
+#include "driver.h"
+#include "terms.cuh"
+
+namespace cpx {
+
+static const uint32_t kSmallPrimes[9] = {1, 2, 3, 5, 7, 11, 13, 17, 19};
+
+uint32_t alpha_milli(u128 x)
+{
+    // alpha(x) of src/main.cpp:128-194: a cubic in log x.  Only chooses y.
+    const double lx = std::log((double)x);
+    double a, b, c, d;
+    if ((double)x <= 1e21) {
+        a = 0.000711339, b = -0.0160586, c = 0.123034, d = 0.802942;
+    } else {
+        a = 0.00149066, b = -0.0375705, c = 0.282139, d = 0.591972;
+    }
+    double al = a * lx * lx * lx + b * lx * lx + c * lx + d;
+    if (al < 1.0) al = 1.0;
+    return (uint32_t)std::lround(al * 1000.0);
+}
+
+uint64_t default_y(u128 x, uint32_t num, uint32_t den)
+{
+    if (num == 0 || den == 0) {
+        num = alpha_milli(x);
+        den = 1000;
+    }
+    // the reference's rule (src/main.cpp:59-64): y = alpha * floor(x^(1/3)),
+    // truncated to an integer; here alpha = num/den and every step is exact
+    const uint64_t cb = cpx_icbrt(x);
+    uint64_t y = (uint64_t)((u128)cb * num / den);
+    const uint64_t lo = cb, hi = cpx_isqrt(x);
+    if (y < lo) y = lo;
+    if (hi > 0 && y >= hi) y = hi - 1;
+    return y;
+}
+
+static const std::vector<uint32_t> &host_primes(cpx_ctx *ctx)
+{
+    Tables &tb = ctx->tab;
+    if (ctx->hP_version != tb.prm_max) {
+        ctx->hP.resize(tb.prm_n);
+        CPX_CUDA(cudaMemcpy(ctx->hP.data(), tb.P, tb.prm_n * 4, cudaMemcpyDeviceToHost));
+        ctx->hP_version = tb.prm_max;
+    }
+    return ctx->hP;
+}
+
+static uint64_t host_pi(const std::vector<uint32_t> &P, uint64_t v)
+{
+    return (uint64_t)(std::upper_bound(P.begin(), P.end(), (uint64_t)v,
+                                       [](uint64_t a, uint32_t b) { return a < b; }) -
+                      P.begin());
+}
+
+bool dr_domain_ok(u128 x, uint64_t y, uint32_t c)
+{
+    if (c < 1 || c > 8) return false;
+    if (x < 1000000) return false;
+    const uint64_t sx = cpx_isqrt(x), cx = cpx_icbrt(x), r4 = cpx_iroot4(x);
+    const uint32_t pc = kSmallPrimes[c];
+    if (y < cx || y >= sx) return false;
+    if (r4 < pc) return false;
+    if (cpx_isqrt(x / y) < pc) return false;
+    if (y >= 0x7FFFFFF0ull) return false;
+    return true;
+}
+
+static uint32_t pick_lbits(cpx_ctx *ctx, uint64_t z, uint32_t threads, uint32_t forced)
+{
+    const uint32_t minb = (threads >= 512) ? 16 : (threads >= 256 ? 15 : 14);
+    if (forced) return std::max(minb, std::min<uint32_t>(forced, 20));
+    // segment count at least ~one wave when z is small; cap at the context default
+    uint32_t lb = ctx->hard_log2_bits;
+    while (lb > minb && ((z + 1) >> (lb + 1)) < (uint64_t)ctx->sm_count * 2) lb--;
+    return std::max(minb, lb);
+}
+
+void run_batch(cpx_ctx *ctx, const BatchReq &rq)
+{
+    const uint32_t Q = (uint32_t)rq.n;
+    if (Q == 0) return;
+    const uint32_t c = rq.c;
+    if (c < 1 || c > 8) fail(CPX_EINVAL, "c must be in 1..8");
+    const uint32_t threads = rq.threads ? rq.threads : ctx->hard_threads;
+    if (threads != 128 && threads != 256 && threads != 512) fail(CPX_EINVAL, "hard threads must be 128/256/512");
+    const unsigned mask = rq.terms;
+
+    // ---- host planning: roots, y, validity, table bounds
+    std::vector<QD> qd(Q);
+    uint64_t N = 1 << 16, Y = 0, Pneed = 64;
+    bool wide = false;
+    for (uint32_t i = 0; i < Q; i++) {
+        QD &d = qd[i];
+        memset(&d, 0, sizeof(d));
+        const u128 x = rq.xs[i];
+        d.x = x;
+        d.c = c;
+        if (x >> 64) wide = true;
+        const uint64_t sx = cpx_isqrt(x), cx = cpx_icbrt(x), r4 = cpx_iroot4(x);
+        uint64_t y = rq.ys ? rq.ys[i] : 0;
+        if (mask == TERM_PI) {
+            if (!y) y = default_y(x, rq.alpha_num, rq.alpha_den);
+            if (!dr_domain_ok(x, y, c)) {
+                if (x >= ((u128)1 << 32)) fail(CPX_EINVAL, "y outside the Deleglise-Rivat domain for this x");
+                d.direct = 1;
+                d.y = 0;
+                N = std::max<uint64_t>(N, (uint64_t)x + 1);
+                continue;
+            }
+        } else if (y == 0) {
+            fail(CPX_EINVAL, "y must be >= 1");
+        }
+        if (y >= 0x7FFFFFF0ull && (mask & (TERM_ORD | TERM_HARD)))
+            fail(CPX_ERANGE, "y must be below 2^31 for the mu/lpf table");
+        const u128 z128 = x / y;
+        if (z128 >> 63) fail(CPX_ERANGE, "x / y must be below 2^63");
+        d.y = y;
+        d.z = (uint64_t)z128;
+        d.sx = sx;
+        d.cx = cx;
+        d.r4 = r4;
+        d.tx = cpx_isqrt(z128);
+        if (mask & TERM_P2) N = std::max<uint64_t>(N, std::max(d.z, sx) + 1);
+        if (mask & TERM_TRIV) N = std::max<uint64_t>(N, std::max(y, cx) + 1);
+        if (mask & TERM_EASY) N = std::max<uint64_t>(N, std::max(sx, y) + 1);
+        if (mask & (TERM_ORD | TERM_HARD)) Y = std::max(Y, y);
+        if (mask & TERM_HARD) Pneed = std::max<uint64_t>(Pneed, r4 + 1);
+        if (mask == TERM_PI) N = std::max<uint64_t>(N, y + 1);
+    }
+    if (N > rq.max_table_n) fail(CPX_ERANGE, "pi table bound exceeds the configured limit");
+
+    // ---- tables
+    ensure_primes(ctx, std::max<uint64_t>(Pneed, cpx_isqrt(Y + 1) + 2));
+    bool any_direct = false;
+    for (const QD &d : qd) any_direct |= d.direct != 0;
+    const bool need_tab = (mask & (TERM_P2 | TERM_TRIV | TERM_EASY)) || mask == TERM_PI || any_direct;
+    if (need_tab) ensure_pitable(ctx, N);
+    if (Y) ensure_mulpf(ctx, Y + 8);
+    if (mask & TERM_ORD) ensure_wheel(ctx, c);
+    const std::vector<uint32_t> &hP = host_primes(ctx);
+
+    // ---- units per kernel family
+    std::vector<uint64_t> pre(6 * (size_t)(Q + 1), 0);
+    uint64_t *p_ord = pre.data(), *p_p2 = p_ord + (Q + 1), *p_triv = p_p2 + (Q + 1), *p_easy = p_triv + (Q + 1),
+             *p_seg = p_easy + (Q + 1), *p_comb = p_seg + (Q + 1);
+    uint64_t hard_entries = 0;
+    uint32_t lbits_max = 0;
+    for (uint32_t i = 0; i < Q; i++) {
+        QD &d = qd[i];
+        uint64_t n_ord = 0, n_p2 = 0, n_triv = 0, n_easy = 0, n_seg = 0, n_comb = 0;
+        if (!d.direct) {
+            const u128 x = d.x;
+            if (mask & TERM_ORD) n_ord = ((d.y + 1) / 2 + 3) / 4;
+            if ((mask & TERM_P2) && d.sx > d.y) n_p2 = ((d.sx - 1) >> 7) - (d.y >> 7) + 1;
+            if (mask & TERM_TRIV) n_triv = (d.cx > d.tx) ? ((d.cx - 1) >> 7) - (d.tx >> 7) + 1 : 1;
+            if ((mask & TERM_EASY) && d.cx > d.r4) n_easy = ((d.cx - 1) >> 7) - (d.r4 >> 7) + 1;
+            if (mask & TERM_HARD) {
+                d.nb = (uint32_t)host_pi(hP, d.r4);
+                if (d.nb > c) {
+                    d.lbits = pick_lbits(ctx, d.z, threads, rq.lbits);
+                    lbits_max = std::max(lbits_max, d.lbits);
+                    const uint64_t span = 2ull << d.lbits;
+                    d.nseg = (d.z + 1 + span - 1) / span;
+                    n_seg = d.nseg;
+                    n_comb = d.nb - c;
+                    for (uint32_t b = c + 1; b <= d.nb; b++) {
+                        const u128 K = (u128)span * hP[b - 1] * hP[b - 1];
+                        const u128 cnt = 1 + (x - 1) / K;
+                        hard_entries += (uint64_t)std::min<u128>(cnt, d.nseg);
+                    }
+                }
+            }
+        }
+        p_ord[i + 1] = p_ord[i] + n_ord;
+        p_p2[i + 1] = p_p2[i] + n_p2;
+        p_triv[i + 1] = p_triv[i] + n_triv;
+        p_easy[i + 1] = p_easy[i] + n_easy;
+        p_seg[i + 1] = p_seg[i] + n_seg;
+        p_comb[i + 1] = p_comb[i] + n_comb;
+    }
+    if (!lbits_max) lbits_max = 15;
+
+    // ---- device buffers
+    Plan pl;
+    pl.Q = Q;
+    pl.c = c;
+    pl.wide = wide;
+    pl.hard_threads = threads;
+    pl.lbits_max = lbits_max;
+    pl.n_ord = p_ord[Q];
+    pl.n_p2 = p_p2[Q];
+    pl.n_triv = p_triv[Q];
+    pl.n_easy = p_easy[Q];
+    pl.n_seg = p_seg[Q];
+    pl.n_comb = p_comb[Q];
+    pl.hard_entries = hard_entries;
+    const size_t qd_bytes = sizeof(QD) * Q, pre_bytes = pre.size() * 8;
+    const size_t acc_words = (size_t)Q * kAccStride;
+    unsigned char *dbuf = (unsigned char *)ctx->b_work[0].get(qd_bytes + pre_bytes + acc_words * 8 + 64);
+    QD *d_qd = reinterpret_cast<QD *>(dbuf);
+    uint64_t *d_pre = reinterpret_cast<uint64_t *>(dbuf + qd_bytes);
+    unsigned long long *d_acc = reinterpret_cast<unsigned long long *>(dbuf + qd_bytes + pre_bytes);
+    pl.qd = d_qd;
+    pl.pre_ord = d_pre;
+    pl.pre_p2 = d_pre + (Q + 1);
+    pl.pre_triv = d_pre + 2 * (Q + 1);
+    pl.pre_easy = d_pre + 3 * (Q + 1);
+    pl.pre_seg = d_pre + 4 * (Q + 1);
+    pl.pre_comb = d_pre + 5 * (Q + 1);
+    pl.acc = d_acc;
+    pl.ticket = ctx->b_work[1].as<unsigned int>(4);
+    if (pl.n_seg) {
+        pl.seg_B = ctx->b_work[2].as<uint32_t>(pl.n_seg + 1);
+        pl.seg_off = ctx->b_work[3].as<uint64_t>(pl.n_seg + 1);
+        pl.hard_cnt = ctx->b_work[4].as<uint32_t>(hard_entries + 1);
+        pl.hard_ms = ctx->b_work[5].as<int32_t>(hard_entries + 1);
+    }
+    u128 *d_out = ctx->b_work[6].as<u128>(Q);
+
+    // one staging copy host -> device
+    std::vector<unsigned char> stage(qd_bytes + pre_bytes);
+    memcpy(stage.data(), qd.data(), qd_bytes);
+    memcpy(stage.data() + qd_bytes, pre.data(), pre_bytes);
+    CPX_CUDA(cudaMemcpyAsync(dbuf, stage.data(), stage.size(), cudaMemcpyHostToDevice, ctx->stream));
+    CPX_CUDA(cudaMemsetAsync(d_acc, 0, acc_words * 8, ctx->stream));
+
+    // ---- kernels
+    if (ctx->timing) CPX_CUDA(cudaEventRecord(ctx->ev_b0, ctx->stream));
+    if (mask & TERM_ORD) launch_ordinary(ctx, pl);
+    if (mask & TERM_P2) launch_p2(ctx, pl);
+    if (mask & TERM_TRIV) launch_trivial(ctx, pl);
+    if (mask & TERM_EASY) launch_easy(ctx, pl);
+    if (mask & TERM_HARD) launch_hard(ctx, pl);
+    launch_finalize(ctx, pl, d_out, mask == TERM_PI);
+    if (ctx->timing) CPX_CUDA(cudaEventRecord(ctx->ev_b1, ctx->stream));
+
+    // ---- results
+    std::vector<unsigned long long> acc(acc_words);
+    CPX_CUDA(cudaMemcpyAsync(acc.data(), d_acc, acc_words * 8, cudaMemcpyDeviceToHost, ctx->stream));
+    CPX_CUDA(cudaStreamSynchronize(ctx->stream));
+    ctx->last_h2d = stage.size();
+    ctx->last_d2h = acc_words * 8;
+    for (uint32_t i = 0; i < Q; i++) {
+        const unsigned long long *A = acc.data() + (size_t)i * kAccStride;
+        auto rd = [&](int t) { return (i128)(((u128)A[2 * t + 1] << 64) | A[2 * t]); };
+        if (rq.out_pi) rq.out_pi[i] = (u128)rd(ACC_PI);
+        if (rq.out_terms) {
+            i128 *o = rq.out_terms + (size_t)i * 7;
+            o[0] = rd(ACC_P2);
+            o[1] = rd(ACC_ORD);
+            o[2] = rd(ACC_TRIV);
+            o[3] = rd(ACC_EASY);
+            o[4] = rd(ACC_HARD);
+            o[5] = rd(ACC_PIY);
+            o[6] = rd(ACC_PI);
+        }
+        if (rq.out_y) rq.out_y[i] = qd[i].y;
+    }
+    if (ctx->timing) CPX_CUDA(cudaEventElapsedTime(&ctx->last_batch_ms, ctx->ev_b0, ctx->ev_b1));
+    if (ctx->timing && pl.n_seg) {
+        float ms = 0.f;
+        CPX_CUDA(cudaEventElapsedTime(&ms, ctx->ev_hard0, ctx->ev_hard1));
+        ctx->last_hard_ms = ms;
+        // algorithmic bytes: one pass over the segment bitmap per active level
+        double bytes = 0.0;
+        for (uint32_t i = 0; i < Q; i++) {
+            const QD &d = qd[i];
+            if (d.direct || d.nb <= c) continue;
+            const uint64_t span = 2ull << d.lbits;
+            for (uint32_t b = c + 1; b <= d.nb; b++) {
+                const u128 K = (u128)span * hP[b - 1] * hP[b - 1];
+                const u128 cnt = 1 + (d.x - 1) / K;
+                bytes += (double)std::min<u128>(cnt, d.nseg) * (double)(1u << d.lbits) / 8.0;
+            }
+        }
+        ctx->last_hard_bytes = bytes;
+    }
+}
+
+}  // namespace cpx

@@ -1,0 +1,35 @@
+// driver.h -- batch execution entry point shared by the C-ABI layer.
+#pragma once
+#include "cpx_internal.h"
+
+namespace cpx {
+
+enum : unsigned {
+    TERM_P2 = 1,
+    TERM_ORD = 2,
+    TERM_TRIV = 4,
+    TERM_EASY = 8,
+    TERM_HARD = 16,
+    TERM_PI = 31  // every term plus the identity
+};
+
+struct BatchReq {
+    const u128 *xs = nullptr;
+    const uint64_t *ys = nullptr;  // per-query y (0 or null: default rule)
+    size_t n = 0;
+    uint32_t c = 6;
+    uint32_t alpha_num = 0, alpha_den = 0;  // 0/0: reference alpha(x)
+    uint32_t lbits = 0, threads = 0;        // hard-leaf tuning (0 = context default)
+    unsigned terms = TERM_PI;
+    uint64_t max_table_n = 1ull << 40;      // largest pi-table bound accepted
+    u128 *out_pi = nullptr;                 // n entries
+    i128 *out_terms = nullptr;              // 7 per query: P2 ord triv easy hard pi_y pi
+    uint64_t *out_y = nullptr;
+};
+
+void run_batch(cpx_ctx *ctx, const BatchReq &rq);
+uint64_t default_y(u128 x, uint32_t num, uint32_t den);
+uint32_t alpha_milli(u128 x);
+bool dr_domain_ok(u128 x, uint64_t y, uint32_t c);
+
+}  // namespace cpx

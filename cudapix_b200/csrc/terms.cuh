@@ -1,0 +1,51 @@
+// terms.cuh -- query descriptors and launch entry points of the term kernels.
+#pragma once
+#include "cpx_internal.h"
+
+namespace cpx {
+
+// One pi(x) evaluation as the device sees it.  Roots are exact floor roots
+// computed on the host.
+struct __align__(16) QD {
+    u128 x;
+    uint64_t y, z, sx, cx, r4, tx;  // tx = isqrt(x / y): trivial-leaf bound
+    uint32_t c, nb;                 // nb = pi(r4)
+    uint32_t lbits, direct;         // hard segment = 2^lbits odd numbers; direct = count by table
+    uint64_t nseg;                  // hard-leaf segments over [0, z]
+};
+
+// accumulator slots per query (each a signed 128-bit value = 2 words)
+enum { ACC_P2 = 0, ACC_ORD, ACC_TRIV, ACC_EASY, ACC_HARD, ACC_PIY, ACC_PI, ACC_N };
+constexpr int kAccStride = 2 * ACC_N;  // u64 words per query
+
+// Unit prefix arrays (Q + 1 entries each, pre[0] = 0) over the queries of a
+// batch, one per kernel family.
+struct Plan {
+    uint32_t Q = 0;
+    const QD *qd = nullptr;
+    const uint64_t *pre_ord = nullptr, *pre_p2 = nullptr, *pre_triv = nullptr, *pre_easy = nullptr,
+                   *pre_seg = nullptr, *pre_comb = nullptr;
+    uint64_t n_ord = 0, n_p2 = 0, n_triv = 0, n_easy = 0, n_seg = 0, n_comb = 0;
+    uint64_t hard_entries = 0;
+    uint32_t c = 6;
+    bool wide = false;  // some x >= 2^64
+    uint32_t hard_threads = 256;
+    uint32_t lbits_max = 18;
+    // device work arrays
+    uint32_t *seg_B = nullptr;
+    uint64_t *seg_off = nullptr;
+    uint32_t *hard_cnt = nullptr;
+    int32_t *hard_ms = nullptr;
+    unsigned long long *acc = nullptr;
+    unsigned int *ticket = nullptr;
+};
+
+void launch_ordinary(cpx_ctx *ctx, const Plan &pl);
+void launch_p2(cpx_ctx *ctx, const Plan &pl);
+void launch_trivial(cpx_ctx *ctx, const Plan &pl);
+void launch_easy(cpx_ctx *ctx, const Plan &pl);
+void launch_hard(cpx_ctx *ctx, const Plan &pl);
+void launch_finalize(cpx_ctx *ctx, const Plan &pl, u128 *d_out_pi, bool full);
+size_t hard_smem_bytes(uint32_t lbits, uint32_t threads, bool wide);
+
+}  // namespace cpx

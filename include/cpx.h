@@ -1,0 +1,197 @@
+/*
+ * cpx.h -- C ABI of cudapix_b200, a B200 (sm_100a) implementation of the
+ * Deleglise-Rivat combinatorial prime count pi(x) with the term split of
+ * curtisseizert/CUDApix.
+ *
+ * Every entry point returns an int status (CPX_OK = 0) and writes results
+ * through out-pointers; cpx_last_error() gives the message of the last
+ * failure on a context.  Device buffers handed to callers are cudaMalloc'd,
+ * so the reference's `cudaFree(ptr)` keeps working; cpx_free() is the same.
+ * A context owns one CUDA stream, the resident tables (compressed pi table,
+ * prime list, packed mu/lpf array, wheel table) and all scratch; calls on one
+ * context are serialised by a mutex.  No call resets the device.
+ *
+ * Reference interfaces replaced (file:line in curtisseizert/CUDApix):
+ *   P2           include/P2.cuh:16-17
+ *   S2_trivial   include/trivial.cuh:8,12
+ *   Ordinary     include/ordinary.cuh:6-7
+ *   Phi          include/phi.cuh:17-36
+ *   Phisieve     include/sieve/phisieve_host.cuh:6-40
+ *   PiTable / get_d_piTable   include/pitable.cuh:7,12-51
+ *   mutest       include/mutest.cuh:3
+ *   gen_d_lpf / gen_h_lpf / gen_d_mu / gen_h_mu / gen_d_mu_lpf
+ *                include/sieve/lpf_mu.cuh:12-24
+ *   S2hardHost::S2hard        include/sieve/S2_hard_host.cuh:35-36
+ *   deleglise_rivat64/128::pi_deleglise_rivat
+ *                include/Deleglise-Rivat/deleglise-rivat.hpp:28,64
+ *   CudaSieve::getDevicePrimes / countPrimes (external CUDASieve, call sites
+ *                e.g. src/P2.cu:100,103, src/Deleglise-Rivat/deleglise-rivat.cpp:33-37)
+ */
+#ifndef CPX_H
+#define CPX_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum {
+    CPX_OK = 0,
+    CPX_EINVAL = 1,   /* argument outside the supported domain */
+    CPX_EOOM = 2,     /* device memory exhausted */
+    CPX_ECUDA = 3,    /* CUDA runtime error */
+    CPX_ETIMEOUT = 4, /* a bounded device wait gave up */
+    CPX_ERANGE = 5,   /* result or size beyond a stated limit */
+    CPX_ESTATE = 6    /* object used in the wrong state */
+};
+
+typedef struct cpx_ctx cpx_ctx;
+/* unsigned 128-bit value split in two words */
+typedef struct {
+    uint64_t lo, hi;
+} cpx_u128;
+
+/* All terms of one pi(x) evaluation, signed 128-bit (two's complement in
+ * lo/hi).  pi = ordinary + trivial + easy + hard + pi_y - 1 - P2. */
+typedef struct {
+    cpx_u128 P2, ordinary, trivial, easy, hard, pi_y, pi;
+    uint64_t x_lo, x_hi, y, z;
+    uint32_t c, pad;
+} cpx_terms;
+
+/* ---- context ---------------------------------------------------------- */
+int cpx_create(int device, cpx_ctx **out);
+int cpx_destroy(cpx_ctx *ctx);
+const char *cpx_last_error(cpx_ctx *ctx);
+const char *cpx_version(void);
+/* the context's cudaStream_t, for callers that time or order work on it */
+void *cpx_stream(cpx_ctx *ctx);
+/* kernels launched by this context since creation */
+uint64_t cpx_launch_count(cpx_ctx *ctx);
+int cpx_free(void *device_ptr);
+/* plain device memory helpers for callers without their own CUDA runtime */
+int cpx_device_alloc(size_t bytes, void **device_ptr);
+int cpx_copy_to_host(void *host_dst, const void *device_src, size_t bytes);
+int cpx_copy_to_device(void *device_dst, const void *host_src, size_t bytes);
+/* number of CUDA devices visible (0 when there is no GPU) */
+int cpx_device_count(void);
+/* free and total device memory of the context's device (cudaMemGetInfo) */
+int cpx_mem_info(cpx_ctx *ctx, uint64_t *free_bytes, uint64_t *total_bytes);
+/* hard-leaf sieve tuning: segment = 2^log2_bits odd numbers (15..20),
+ * threads per CTA in {128, 256, 512}. */
+int cpx_set_hard_params(cpx_ctx *ctx, uint32_t log2_bits, uint32_t threads);
+/* time of the last hard-leaf sieve (CUDA events on the context stream) and
+ * its algorithmic byte count (one pass over the segment bitmap per active
+ * prime per segment). */
+int cpx_last_hard_stats(cpx_ctx *ctx, float *ms, double *bytes);
+int cpx_set_timing(cpx_ctx *ctx, int enable);
+/* device time of the last batch's kernels (first launch to last, CUDA events
+ * on the context stream); valid when timing is enabled */
+int cpx_last_batch_ms(cpx_ctx *ctx, float *ms);
+/* bytes the last batch copied host->device and device->host */
+int cpx_last_batch_io(cpx_ctx *ctx, uint64_t *h2d_bytes, uint64_t *d2h_bytes);
+/* CUDA-event stopwatch on the context stream: start records an event; stop
+ * records another, synchronises and returns the elapsed milliseconds */
+int cpx_timer_start(cpx_ctx *ctx);
+int cpx_timer_stop(cpx_ctx *ctx, float *ms);
+/* overwrite a device buffer larger than L2 (256 MiB) on the context stream,
+ * so that the next timed call starts with a cold L2 */
+int cpx_flush_l2(cpx_ctx *ctx);
+
+/* ---- parameters (host, exact integer) ---------------------------------- */
+int cpx_iroots(cpx_u128 x, uint64_t *sqrt_x, uint64_t *cbrt_x, uint64_t *qrt_x);
+/* y = floor(alpha * icbrt(x)) for alpha = num/den (num = 0: the reference's
+ * alpha(x)), clamped to [icbrt(x), isqrt(x) - 1] (src/main.cpp:59-64). */
+int cpx_default_y(cpx_u128 x, uint32_t alpha_num, uint32_t alpha_den, uint64_t *y);
+/* alpha(x) of the reference (src/main.cpp:128-194) scaled by 1000; only
+ * chooses y, never enters a count. */
+uint32_t cpx_alpha_milli(cpx_u128 x);
+
+/* ---- terms -------------------------------------------------------------- */
+/* P2(x, y) = sum_{y < p <= sqrt x} [pi(x/p) - pi(p) + 1]      (src/P2.cu:99) */
+int cpx_P2_u64(cpx_ctx *ctx, uint64_t x, uint64_t y, uint64_t *out);
+int cpx_P2_u128(cpx_ctx *ctx, cpx_u128 x, uint64_t y, cpx_u128 *out);
+/* trivial leaves S1 + U                                    (src/trivial.cu:31) */
+int cpx_trivial_u64(cpx_ctx *ctx, uint64_t x, uint64_t y, uint64_t *out);
+int cpx_trivial_u128(cpx_ctx *ctx, cpx_u128 x, uint64_t y, cpx_u128 *out);
+/* ordinary leaves sum_{n <= y, lpf(n) > p_c} mu(n) phi(x/n, c), 1 <= c <= 8
+ *                                                         (src/ordinary.cu:33) */
+int cpx_ordinary_u64(cpx_ctx *ctx, uint64_t x, uint64_t y, uint16_t c, int64_t *out);
+int cpx_ordinary_u128(cpx_ctx *ctx, cpx_u128 x, uint64_t y, uint16_t c, cpx_u128 *out);
+/* easy special leaves: (p, q) with iroot4(x) < p <= icbrt(x), q prime,
+ * max(p, y/p) < q <= min(y, x/p^2), value pi(x/(pq)) - pi(p) + 2 */
+int cpx_S2_easy_u64(cpx_ctx *ctx, uint64_t x, uint64_t y, int64_t *out);
+int cpx_S2_easy_u128(cpx_ctx *ctx, cpx_u128 x, uint64_t y, cpx_u128 *out);
+/* hard special leaves: p_b <= iroot4(x), b > c, by the segmented phi sieve
+ *                                          (src/sieve/S2_hard_host.cu:172) */
+int cpx_S2_hard_u64(cpx_ctx *ctx, uint64_t x, uint64_t y, uint16_t c, int64_t *out);
+int cpx_S2_hard_u128(cpx_ctx *ctx, cpx_u128 x, uint64_t y, uint16_t c, cpx_u128 *out);
+/* pi(x) by the term identity; terms may be NULL.  y = 0 picks the default
+ * y rule; the DR domain needs icbrt(x) <= y < isqrt(x); smaller x is counted
+ * directly.                   (src/Deleglise-Rivat/deleglise-rivat.cpp:50-80) */
+int cpx_pi_u64(cpx_ctx *ctx, uint64_t x, uint64_t y, uint16_t c, uint64_t *pi, cpx_terms *terms);
+int cpx_pi_u128(cpx_ctx *ctx, cpx_u128 x, uint64_t y, uint16_t c, cpx_u128 *pi, cpx_terms *terms);
+
+/* ---- sieves and tables -------------------------------------------------- */
+/* mu(n) and lpf(n) for odd n = lo + 2i + 1, i < (hi - lo) / 2, lo even.
+ * lpf(1) = 0xFFFFFFFF; lpf(p) = p.  Outputs are cudaMalloc'd, caller frees.
+ *                                              (src/sieve/lpf_mu.cu:199-302) */
+int cpx_gen_d_mu(cpx_ctx *ctx, uint64_t lo, uint64_t hi, int8_t **d_mu);
+int cpx_gen_d_lpf32(cpx_ctx *ctx, uint64_t lo, uint64_t hi, uint32_t **d_lpf);
+int cpx_gen_d_lpf64(cpx_ctx *ctx, uint64_t lo, uint64_t hi, uint64_t **d_lpf);
+int cpx_gen_d_mu_lpf(cpx_ctx *ctx, uint64_t lo, uint64_t hi, int8_t *d_mu, uint64_t *d_lpf);
+/* host copies into caller buffers of (hi - lo) / 2 entries */
+int cpx_gen_h_mu(cpx_ctx *ctx, uint64_t lo, uint64_t hi, int8_t *h_mu);
+int cpx_gen_h_lpf32(cpx_ctx *ctx, uint64_t lo, uint64_t hi, uint32_t *h_lpf);
+/* Mertens sum over 1 <= n < top                              (src/mutest.cu:6) */
+int cpx_mutest(cpx_ctx *ctx, uint64_t top, int64_t *out);
+/* dense pi table of get_d_piTable: out[k] = pi(2k - 1), k < hi / 2, hi < 2^32
+ *                                                          (src/pitable.cu:10) */
+int cpx_pitable(cpx_ctx *ctx, uint64_t hi, uint32_t **d_out);
+/* windowed table of PiTable: out[k] = pi(base + 2k - 1) - pi(base - 1) for
+ * k < range/2 + 2 into a caller buffer; *pi_base = pi(base - 1).  base even.
+ *                                                      (src/pitable.cu:27-218) */
+int cpx_pitable_window(cpx_ctx *ctx, uint64_t base, uint64_t range, uint32_t *d_out,
+                       uint64_t *pi_base);
+/* primes in [lo, hi) (CudaSieve::getDevicePrimes); cudaMalloc'd output */
+int cpx_primes(cpx_ctx *ctx, uint64_t lo, uint64_t hi, uint64_t **d_out, uint64_t *count);
+/* number of primes in [lo, hi) (CudaSieve::countPrimes) */
+int cpx_count_primes(cpx_ctx *ctx, uint64_t lo, uint64_t hi, uint64_t *count);
+/* phi(x, a): #{1 <= n <= x : no prime factor among the first a primes}
+ *                                                             (src/phi.cu:42) */
+int cpx_phi(cpx_ctx *ctx, uint64_t x, uint32_t a, uint64_t *out);
+/* Phi::generateRange: out[i] = phi(2i + 1, a) for i < num/2 (cudaMalloc'd)
+ *                                                             (src/phi.cu:75) */
+int cpx_phi_range(cpx_ctx *ctx, uint32_t num, uint32_t a, uint32_t **d_out);
+
+/* Phisieve: odd-only bit sieve of 'bits' bits over [0, 2*bits) with a count
+ * table counts[i] = phi(2i - 1, a) (exclusive scan of the bits), where a is
+ * the number of primes sieved so far.     (src/sieve/phisieve_host.cu:12-89) */
+typedef struct cpx_phisieve cpx_phisieve;
+int cpx_phisieve_create(cpx_ctx *ctx, uint32_t max_prime, uint32_t bits, cpx_phisieve **out);
+int cpx_phisieve_destroy(cpx_phisieve *ps);
+int cpx_phisieve_first(cpx_phisieve *ps, uint16_t c);
+int cpx_phisieve_mark_next(cpx_phisieve *ps);
+int cpx_phisieve_update(cpx_phisieve *ps);
+int cpx_phisieve_counts(cpx_phisieve *ps, uint32_t **d_counts, uint32_t *a_current);
+
+/* ---- batched and served evaluation -------------------------------------- */
+typedef struct {
+    uint32_t alpha_num, alpha_den; /* y rule; 0/0 = reference alpha(x) */
+    uint16_t c;                    /* pre-sieve primes, default 6 */
+    uint16_t pad;
+    uint32_t hard_log2_bits;       /* 0 = context default */
+    uint32_t hard_threads;         /* 0 = context default */
+} cpx_params;
+
+/* pi(x_i) for n queries in one batched device pass over shared tables sized
+ * to the largest query.  out[i] = pi(x_i). */
+int cpx_pi_batch(cpx_ctx *ctx, const cpx_u128 *xs, size_t n, const cpx_params *params,
+                 cpx_u128 *out);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* CPX_H */

@@ -1,0 +1,837 @@
+/*
+ * oracle.c -- CPU restatement of the Deleglise-Rivat pi(x) term pipeline of
+ * curtisseizert/CUDApix.  TEST INFRASTRUCTURE ONLY: it is the checker for the
+ * CUDA library and the timed CPU baseline of bench.py; the product never
+ * links or calls it.
+ *
+ * Parity pin: published pi(10^k) values (OEIS A006880) and sympy-generated
+ * vectors (tests/golden/).  The reference holds no golden vectors and cannot
+ * be built here (its CUDASieve / CUDA-uint128 dependencies are not vendored),
+ * so parity with the reference's own outputs is not pinned.
+ *
+ * Definitions followed (reference file:line):
+ *   P2       = sum_{y < p <= sqrt x} [pi(x/p) - pi(p) + 1]         src/P2.cu:99-156
+ *   trivial  = S1 + U                                              src/trivial.cu:31-62
+ *              S1 = C(pi(y) - pi(cbrt x), 2)
+ *              U  = sum_{sqrt(x/y) < p <= cbrt x} [pi(y) - pi(x/p^2)]
+ *   ordinary = sum_{odd n <= y, lpf(n) > p_c} mu(n) phi(x/n, c)    src/ordinary.cu:33-67,111-125
+ *   pi(x)    = ordinary + trivial + easy + hard + pi(y) - 1 - P2   src/Deleglise-Rivat/deleglise-rivat.cpp:77
+ * The reference splits easy + hard differently and its sum is wrong by about
+ * 1 ppm (README.md:3,8); this restatement uses the exact split below, shared
+ * with the CUDA library:
+ *   easy = sum over leaves (p, q), q prime, iroot4(x) < p <= icbrt(x),
+ *          max(p, y/p) < q <= min(y, x/p^2) of [pi(x/(pq)) - pi(p) + 2]
+ *   hard = - sum_{b = c+1}^{pi(iroot4 x)} sum_{y/p_b < m <= y, lpf(m) > p_b}
+ *          mu(m) phi(x/(p_b m), b-1)
+ * All roots are exact integer floor roots (the reference used doubles,
+ * e.g. src/trivial.cu:33-34).
+ */
+#include "oracle.h"
+
+#include <math.h>
+#include <omp.h>
+#include <stdlib.h>
+#include <string.h>
+
+typedef unsigned __int128 u128;
+typedef __int128 i128;
+
+static u128 mk128(uint64_t lo, uint64_t hi) { return ((u128)hi << 64) | lo; }
+static void put128(i128 v, uint64_t *out)
+{
+    out[0] = (uint64_t)(u128)v;
+    out[1] = (uint64_t)((u128)v >> 64);
+}
+
+/* ------------------------------------------------------------------ roots */
+
+static uint64_t isqrt128(u128 x)
+{
+    if (x == 0) return 0;
+    long double d = sqrtl((long double)x);
+    uint64_t r = d >= 18446744073709551615.0L ? UINT64_MAX : (uint64_t)d;
+    while ((u128)r * r > x) r--;
+    while (r < UINT64_MAX && (u128)(r + 1) * (r + 1) <= x) r++;
+    return r;
+}
+
+/* cube of r, saturating at UINT128 max */
+static u128 cube_sat(uint64_t r)
+{
+    const uint64_t rmax = 6981463658331ull; /* floor(cbrt(2^128 - 1)) */
+    if (r > rmax) return ~(u128)0;
+    return (u128)r * r * r;
+}
+
+static uint64_t icbrt128(u128 x)
+{
+    if (x == 0) return 0;
+    long double d = cbrtl((long double)x);
+    uint64_t r = (uint64_t)d;
+    while (r > 0 && cube_sat(r) > x) r--;
+    while (cube_sat(r + 1) <= x) r++;
+    return r;
+}
+
+uint64_t orc_isqrt(uint64_t lo, uint64_t hi) { return isqrt128(mk128(lo, hi)); }
+uint64_t orc_icbrt(uint64_t lo, uint64_t hi) { return icbrt128(mk128(lo, hi)); }
+uint64_t orc_iroot4(uint64_t lo, uint64_t hi) { return isqrt128(isqrt128(mk128(lo, hi))); }
+
+/* ----------------------------------------------------------- small primes */
+
+/* all primes <= n (n < 2^32), ascending; *cnt receives the count */
+static uint32_t *primes_upto(uint64_t n, uint64_t *cnt)
+{
+    if (n < 2) {
+        *cnt = 0;
+        return (uint32_t *)malloc(sizeof(uint32_t));
+    }
+    uint64_t half = n / 2 + 1; /* index i <-> 2i+1 */
+    uint8_t *comp = (uint8_t *)calloc(half, 1);
+    for (uint64_t i = 1; (2 * i + 1) * (2 * i + 1) <= n; i++) {
+        if (comp[i]) continue;
+        uint64_t p = 2 * i + 1;
+        for (uint64_t m = p * p; m <= n; m += 2 * p) comp[m / 2] = 1;
+    }
+    uint64_t c = 1;
+    for (uint64_t i = 1; 2 * i + 1 <= n; i++) c += !comp[i];
+    uint32_t *P = (uint32_t *)malloc(c * sizeof(uint32_t));
+    uint64_t k = 0;
+    P[k++] = 2;
+    for (uint64_t i = 1; 2 * i + 1 <= n; i++)
+        if (!comp[i]) P[k++] = (uint32_t)(2 * i + 1);
+    free(comp);
+    *cnt = c;
+    return P;
+}
+
+/* Sieve the odd numbers n = lo + 2i + 1, i < nbits (lo even, nbits % 64 == 0)
+ * into bits[] with 1 = prime.  sp = odd primes (ascending) with sp^2 <= top. */
+static void sieve_odd_segment(uint64_t lo, uint64_t nbits, const uint32_t *sp, uint64_t nsp,
+                              uint64_t *bits)
+{
+    uint64_t nw = nbits / 64;
+    memset(bits, 0xff, nw * 8);
+    uint64_t top = lo + 2 * nbits; /* exclusive */
+    for (uint64_t k = 0; k < nsp; k++) {
+        uint64_t p = sp[k];
+        if (p * p >= top) break;
+        uint64_t start = p * p;
+        if (start < lo + 1) {
+            /* first odd multiple of p that is >= lo + 1 */
+            uint64_t m = (lo + 1 + p - 1) / p * p;
+            if ((m & 1) == 0) m += p;
+            start = m;
+        }
+        for (uint64_t n = start; n < top; n += 2 * p) {
+            uint64_t i = (n - lo - 1) >> 1;
+            bits[i >> 6] &= ~(1ull << (i & 63));
+        }
+    }
+    if (lo == 0) bits[0] &= ~1ull; /* 1 is not prime */
+}
+
+/* ------------------------------------------------------ compressed pi table */
+
+/* word w covers odd n = 128 w + 2 j + 1, j < 64; pre[w] = # odd primes < 128 w */
+typedef struct {
+    uint64_t nmax, nwords;
+    uint64_t *bits, *pre;
+} pitab_t;
+
+static void pitab_free(pitab_t *t)
+{
+    free(t->bits);
+    free(t->pre);
+    t->bits = t->pre = 0;
+}
+
+static pitab_t pitab_build(uint64_t nmax)
+{
+    pitab_t t;
+    t.nmax = nmax;
+    t.nwords = nmax / 128 + 1;
+    const uint64_t chunk_words = 1 << 14; /* 2^20 odd numbers per chunk */
+    uint64_t nchunks = (t.nwords + chunk_words - 1) / chunk_words;
+    t.nwords = nchunks * chunk_words;
+    t.bits = (uint64_t *)malloc(t.nwords * 8);
+    t.pre = (uint64_t *)malloc(t.nwords * 8);
+    uint64_t nsp;
+    uint32_t *P = primes_upto(isqrt128((u128)t.nwords * 128) + 1, &nsp);
+    uint64_t *ctot = (uint64_t *)calloc(nchunks, 8);
+#pragma omp parallel for schedule(dynamic, 4)
+    for (uint64_t c = 0; c < nchunks; c++) {
+        uint64_t *b = t.bits + c * chunk_words;
+        sieve_odd_segment(c * chunk_words * 128, chunk_words * 64, P + 1, nsp - 1, b);
+        uint64_t s = 0;
+        for (uint64_t w = 0; w < chunk_words; w++) s += __builtin_popcountll(b[w]);
+        ctot[c] = s;
+    }
+    uint64_t run = 0;
+    for (uint64_t c = 0; c < nchunks; c++) {
+        uint64_t v = ctot[c];
+        ctot[c] = run;
+        run += v;
+    }
+#pragma omp parallel for schedule(static)
+    for (uint64_t c = 0; c < nchunks; c++) {
+        uint64_t s = ctot[c];
+        for (uint64_t w = c * chunk_words; w < (c + 1) * chunk_words; w++) {
+            t.pre[w] = s;
+            s += __builtin_popcountll(t.bits[w]);
+        }
+    }
+    free(ctot);
+    free(P);
+    return t;
+}
+
+static inline uint64_t pitab_pi(const pitab_t *t, uint64_t n)
+{
+    if (n < 2) return 0;
+    uint64_t w = (n - 1) >> 7;
+    uint32_t j = (uint32_t)(((n - 1) & 127) >> 1);
+    uint64_t mask = (j == 63) ? ~0ull : ((2ull << j) - 1);
+    return 1 + t->pre[w] + (uint64_t)__builtin_popcountll(t->bits[w] & mask);
+}
+
+/* ------------------------------------------------------------- prime count */
+
+uint64_t orc_pi_sieve(uint64_t x)
+{
+    if (x < 2) return 0;
+    uint64_t nsp;
+    uint32_t *P = primes_upto(isqrt128(x) + 1, &nsp);
+    const uint64_t seg_bits = 1 << 20;
+    uint64_t nodd = (x + 1) / 2; /* odd numbers 1..x */
+    uint64_t nseg = (nodd + seg_bits - 1) / seg_bits;
+    uint64_t total = 0;
+#pragma omp parallel reduction(+ : total)
+    {
+        uint64_t *b = (uint64_t *)malloc(seg_bits / 8);
+#pragma omp for schedule(dynamic, 1)
+        for (uint64_t s = 0; s < nseg; s++) {
+            uint64_t lo = s * seg_bits * 2;
+            sieve_odd_segment(lo, seg_bits, P + 1, nsp - 1, b);
+            uint64_t lim = nodd - s * seg_bits; /* bits valid in this segment */
+            if (lim > seg_bits) lim = seg_bits;
+            for (uint64_t w = 0; w < lim / 64; w++) total += __builtin_popcountll(b[w]);
+            if (lim % 64) total += __builtin_popcountll(b[lim / 64] & ((1ull << (lim % 64)) - 1));
+        }
+        free(b);
+    }
+    free(P);
+    return total + 1; /* the prime 2 */
+}
+
+uint64_t orc_primes(uint64_t lo, uint64_t hi, uint64_t *out, uint64_t cap)
+{
+    if (hi <= lo) return 0;
+    uint64_t nsp;
+    uint32_t *P = primes_upto(isqrt128(hi) + 1, &nsp);
+    uint64_t k = 0;
+    if (lo <= 2 && 2 < hi) {
+        if (k < cap) out[k] = 2;
+        k++;
+    }
+    const uint64_t seg_bits = 1 << 16;
+    uint64_t *b = (uint64_t *)malloc(seg_bits / 8);
+    for (uint64_t base = (lo / 2) * 2; base < hi; base += 2 * seg_bits) {
+        sieve_odd_segment(base, seg_bits, P + 1, nsp - 1, b);
+        for (uint64_t i = 0; i < seg_bits; i++) {
+            if (!((b[i >> 6] >> (i & 63)) & 1)) continue;
+            uint64_t n = base + 2 * i + 1;
+            if (n < lo) continue;
+            if (n >= hi) break;
+            if (k < cap) out[k] = n;
+            k++;
+        }
+    }
+    free(b);
+    free(P);
+    return k;
+}
+
+/* -------------------------------------------------------------- mu and lpf */
+
+static void mu_lpf_range(uint64_t lo, uint64_t len, const uint32_t *P, uint64_t np, int8_t *mu,
+                         uint64_t *lpf)
+{
+    uint64_t *rem = (uint64_t *)malloc(len * 8);
+    for (uint64_t i = 0; i < len; i++) {
+        rem[i] = lo + 2 * i + 1;
+        mu[i] = 1;
+        lpf[i] = 0;
+    }
+    uint64_t top = lo + 2 * len;
+    for (uint64_t k = 1; k < np; k++) { /* odd primes, ascending */
+        uint64_t p = P[k];
+        if (p * p >= top) break;
+        uint64_t m = (lo + 1 + p - 1) / p * p;
+        if ((m & 1) == 0) m += p;
+        for (; m < top; m += 2 * p) {
+            uint64_t i = (m - lo - 1) >> 1;
+            if (lpf[i] == 0) lpf[i] = p;
+            if ((m / p) % p == 0) mu[i] = 0;
+            else mu[i] = (int8_t)-mu[i];
+            while (rem[i] % p == 0) rem[i] /= p;
+        }
+    }
+    for (uint64_t i = 0; i < len; i++) {
+        uint64_t n = lo + 2 * i + 1;
+        if (n == 1) {
+            lpf[i] = 0xFFFFFFFFull;
+            mu[i] = 1;
+            continue;
+        }
+        if (rem[i] > 1) {
+            mu[i] = (int8_t)-mu[i];
+            if (lpf[i] == 0) lpf[i] = rem[i];
+        }
+    }
+    free(rem);
+}
+
+void orc_mu_lpf(uint64_t lo, uint64_t hi, int8_t *mu, uint32_t *lpf)
+{
+    uint64_t len = (hi - lo) / 2;
+    uint64_t np;
+    uint32_t *P = primes_upto(isqrt128(hi) + 1, &np);
+    const uint64_t chunk = 1 << 16;
+    uint64_t nch = (len + chunk - 1) / chunk;
+#pragma omp parallel
+    {
+        uint64_t *l64 = (uint64_t *)malloc(chunk * 8);
+#pragma omp for schedule(dynamic, 1)
+        for (uint64_t c = 0; c < nch; c++) {
+            uint64_t n0 = c * chunk, cl = len - n0 < chunk ? len - n0 : chunk;
+            mu_lpf_range(lo + 2 * n0, cl, P, np, mu + n0, l64);
+            for (uint64_t i = 0; i < cl; i++) lpf[n0 + i] = (uint32_t)l64[i];
+        }
+        free(l64);
+    }
+    free(P);
+}
+
+int64_t orc_mertens(uint64_t top)
+{
+    if (top <= 1) return 0;
+    uint64_t len = top / 2 + 1;
+    int8_t *mu = (int8_t *)malloc(len);
+    uint32_t *lpf = (uint32_t *)malloc(len * 4);
+    orc_mu_lpf(0, 2 * len, mu, lpf);
+    int64_t s = 0;
+    for (uint64_t n = 1; n < top; n++) {
+        if (n & 1) s += mu[n / 2];
+        else if (n % 4 != 0) s -= mu[(n / 2) / 2];
+    }
+    free(mu);
+    free(lpf);
+    return s;
+}
+
+void orc_pitable_dense(uint64_t hi, uint32_t *out)
+{
+    uint64_t K = hi / 2;
+    pitab_t t = pitab_build(hi + 2);
+    for (uint64_t k = 0; k < K; k++) out[k] = k == 0 ? 0 : (uint32_t)pitab_pi(&t, 2 * k - 1);
+    pitab_free(&t);
+}
+
+void orc_pitable_window(uint64_t base, uint64_t range, uint32_t *out, uint64_t *pi_base)
+{
+    uint64_t K = range / 2 + 2;
+    pitab_t t = pitab_build(base + 2 * K + 2);
+    uint64_t pb = base == 0 ? 0 : pitab_pi(&t, base - 1);
+    for (uint64_t k = 0; k < K; k++) {
+        uint64_t n = base + 2 * k; /* value at k is pi(base + 2k - 1) */
+        out[k] = (k == 0) ? 0 : (uint32_t)(pitab_pi(&t, n - 1) - pb);
+    }
+    *pi_base = pb;
+    pitab_free(&t);
+}
+
+/* ------------------------------------------------------------ phi and wheel */
+
+static const uint32_t SMALLP[9] = {1, 2, 3, 5, 7, 11, 13, 17, 19};
+
+typedef struct {
+    uint64_t W, tot;
+    uint32_t *cnt; /* cnt[r] = #{1 <= n <= r : gcd(n, W) = 1}, r < W */
+} wheel_t;
+
+static wheel_t wheel_make(uint32_t c)
+{
+    wheel_t w;
+    w.W = 1;
+    for (uint32_t i = 1; i <= c; i++) w.W *= SMALLP[i];
+    w.cnt = (uint32_t *)malloc(w.W * 4);
+    uint32_t s = 0;
+    for (uint64_t r = 0; r < w.W; r++) {
+        int ok = r >= 1;
+        for (uint32_t i = 1; i <= c && ok; i++)
+            if (r % SMALLP[i] == 0) ok = 0;
+        s += ok;
+        w.cnt[r] = s;
+    }
+    w.tot = s;
+    return w;
+}
+
+static inline u128 wheel_phi(const wheel_t *w, u128 m)
+{
+    return (m / w->W) * w->tot + w->cnt[(uint64_t)(m % w->W)];
+}
+
+typedef struct {
+    const uint32_t *P; /* P[0] = 2 */
+    uint64_t np;
+    const pitab_t *tab;
+    const wheel_t *wh; /* wheel for a = 6 */
+} phictx_t;
+
+/* phi(v, a) by Legendre's recursion with the usual cut-offs */
+static int64_t phi_rec(const phictx_t *C, uint64_t v, uint32_t a)
+{
+    if (a == 0) return (int64_t)v;
+    if (v == 0) return 0;
+    if (v <= C->P[a - 1]) return 1;
+    if (a == 6) return (int64_t)wheel_phi(C->wh, v);
+    if (a < C->np && C->tab && v <= C->tab->nmax &&
+        (u128)C->P[a] * C->P[a] > v) /* v < p_{a+1}^2 */
+        return (int64_t)pitab_pi(C->tab, v) - a + 1;
+    if (a < 6) {
+        int64_t s = phi_rec(C, v, a - 1) - phi_rec(C, v / C->P[a - 1], a - 1);
+        return s;
+    }
+    return phi_rec(C, v, a - 1) - phi_rec(C, v / C->P[a - 1], a - 1);
+}
+
+uint64_t orc_phi(uint64_t x, uint32_t a)
+{
+    if (a == 0) return x;
+    uint64_t np;
+    uint64_t plim = 1000;
+    uint32_t *P = primes_upto(plim, &np);
+    while (np <= a + 1) {
+        free(P);
+        plim *= 4;
+        P = primes_upto(plim, &np);
+    }
+    uint64_t tmax = x < 100000000ull ? x : 100000000ull;
+    pitab_t tab = pitab_build(tmax + 1);
+    wheel_t wh = wheel_make(6);
+    phictx_t C = {P, np, &tab, &wh};
+    int64_t r;
+    if (a <= 6) {
+        r = phi_rec(&C, x, a);
+    } else {
+        /* phi(x, a) = phi(x, 6) - sum_{k=7}^{a} phi(x / p_k, k - 1) */
+        int64_t s = (int64_t)wheel_phi(&wh, x);
+#pragma omp parallel for schedule(dynamic, 1) reduction(- : s)
+        for (uint32_t k = 7; k <= a; k++) s -= phi_rec(&C, x / P[k - 1], k - 1);
+        r = s;
+    }
+    wheel_t *pw = &wh;
+    free(pw->cnt);
+    pitab_free(&tab);
+    free(P);
+    return (uint64_t)r;
+}
+
+void orc_phisieve_counts(uint32_t a, uint64_t nbits, uint32_t *out)
+{
+    uint64_t np;
+    uint64_t plim = 1000;
+    uint32_t *P = primes_upto(plim, &np);
+    while (np < a + 1) {
+        free(P);
+        plim *= 4;
+        P = primes_upto(plim, &np);
+    }
+    uint8_t *bit = (uint8_t *)malloc(nbits);
+    memset(bit, 1, nbits);
+    for (uint32_t k = 1; k < a; k++) { /* odd primes p_2 .. p_a */
+        uint64_t p = P[k];
+        for (uint64_t n = p; (n - 1) / 2 < nbits; n += 2 * p) bit[(n - 1) / 2] = 0;
+    }
+    uint32_t s = 0;
+    for (uint64_t i = 0; i < nbits; i++) {
+        out[i] = s;
+        s += bit[i];
+    }
+    free(bit);
+    free(P);
+}
+
+/* ------------------------------------------------------------------ terms */
+
+typedef struct {
+    u128 x;
+    uint64_t y, z, sqrtx, cbrtx, qrtx;
+    uint32_t c;
+    uint32_t *P; /* primes <= max(y, sqrtx) + margin, P[0] = 2 */
+    uint64_t np;
+    pitab_t tab; /* pi table to max(z, sqrtx) */
+    int have_tab;
+} drctx_t;
+
+static void dr_init(drctx_t *D, u128 x, uint64_t y, uint32_t c, uint64_t tabmax)
+{
+    D->x = x;
+    D->y = y;
+    D->c = c;
+    D->z = (uint64_t)(x / y);
+    D->sqrtx = isqrt128(x);
+    D->cbrtx = icbrt128(x);
+    D->qrtx = isqrt128(D->sqrtx);
+    uint64_t pmax = D->y > D->sqrtx ? D->y : D->sqrtx;
+    D->P = primes_upto(pmax + 64, &D->np);
+    D->have_tab = tabmax > 0;
+    if (D->have_tab) D->tab = pitab_build(tabmax);
+}
+
+static void dr_free(drctx_t *D)
+{
+    free(D->P);
+    if (D->have_tab) pitab_free(&D->tab);
+}
+
+static i128 term_P2(const drctx_t *D)
+{
+    if (D->y >= D->sqrtx) return 0;
+    uint64_t a = pitab_pi(&D->tab, D->y), b = pitab_pi(&D->tab, D->sqrtx);
+    i128 s = 0;
+#pragma omp parallel
+    {
+        i128 ls = 0;
+#pragma omp for schedule(static)
+        for (uint64_t i = a + 1; i <= b; i++) {
+            uint64_t p = D->P[i - 1];
+            uint64_t q = (uint64_t)(D->x / p);
+            ls += (i128)pitab_pi(&D->tab, q) - (i128)i + 1;
+        }
+#pragma omp critical
+        s += ls;
+    }
+    return s;
+}
+
+static i128 term_trivial(const drctx_t *D)
+{
+    uint64_t piy = pitab_pi(&D->tab, D->y), pic = pitab_pi(&D->tab, D->cbrtx);
+    i128 s = 0;
+    if (piy > pic) s += (i128)(piy - pic) * (piy - pic - 1) / 2;
+    uint64_t lo = isqrt128(D->x / D->y); /* p > lo */
+    for (uint64_t i = 0; i < D->np; i++) {
+        uint64_t p = D->P[i];
+        if (p > D->cbrtx) break;
+        if (p <= lo) continue;
+        uint64_t q = (uint64_t)(D->x / ((u128)p * p));
+        s += (i128)piy - (i128)pitab_pi(&D->tab, q);
+    }
+    return s;
+}
+
+static i128 term_ordinary(const drctx_t *D, const int8_t *mu, const uint32_t *lpf)
+{
+    wheel_t wh = wheel_make(D->c);
+    uint32_t pc = SMALLP[D->c];
+    i128 s = 0;
+    uint64_t len = (D->y + 1) / 2; /* odd n <= y */
+#pragma omp parallel
+    {
+        i128 ls = 0;
+#pragma omp for schedule(static)
+        for (uint64_t i = 0; i < len; i++) {
+            if (mu[i] == 0 || lpf[i] <= pc) continue;
+            uint64_t n = 2 * i + 1;
+            u128 m = D->x / n;
+            i128 ph = (i128)wheel_phi(&wh, m);
+            ls += mu[i] > 0 ? ph : -ph;
+        }
+#pragma omp critical
+        s += ls;
+    }
+    free(wh.cnt);
+    return s;
+}
+
+static i128 term_easy(const drctx_t *D)
+{
+    i128 s = 0;
+    uint64_t blo = pitab_pi(&D->tab, D->qrtx) + 1, bhi = pitab_pi(&D->tab, D->cbrtx);
+#pragma omp parallel
+    {
+        i128 ls = 0;
+#pragma omp for schedule(dynamic, 1)
+        for (uint64_t b = blo; b <= bhi; b++) {
+            uint64_t p = D->P[b - 1];
+            u128 xp = D->x / p;
+            uint64_t qlo = D->y / p;
+            if (qlo < p) qlo = p;
+            u128 xpp = xp / p;
+            uint64_t qhi = xpp < D->y ? (uint64_t)xpp : D->y;
+            if (qhi <= qlo) continue;
+            uint64_t ilo = pitab_pi(&D->tab, qlo) + 1, ihi = pitab_pi(&D->tab, qhi);
+            for (uint64_t j = ilo; j <= ihi; j++) {
+                uint64_t q = D->P[j - 1];
+                uint64_t u = (uint64_t)(xp / q);
+                ls += (i128)pitab_pi(&D->tab, u) - (i128)b + 2;
+            }
+        }
+#pragma omp critical
+        s += ls;
+    }
+    return s;
+}
+
+/* hard leaves by a segmented phi sieve over [0, z]; chunks of consecutive
+ * segments run in parallel and are stitched together by per-level carries. */
+static i128 term_hard(const drctx_t *D, const int8_t *mu, const uint32_t *lpf)
+{
+    uint64_t nb = 0; /* pi(qrtx) */
+    while (nb < D->np && D->P[nb] <= D->qrtx) nb++;
+    uint32_t c = D->c;
+    if (nb <= c) return 0;
+    const uint64_t L = 1 << 16; /* odd numbers per segment */
+    const uint64_t NW = L / 64;
+    uint64_t nseg = (D->z + 1 + 2 * L - 1) / (2 * L);
+    int nt = omp_get_max_threads();
+    uint64_t nch = (uint64_t)nt * 8;
+    if (nch > nseg) nch = nseg;
+    int64_t *cntT = (int64_t *)calloc(nch * (nb + 1), 8);
+    int64_t *msT = (int64_t *)calloc(nch * (nb + 1), 8);
+    i128 *Sc = (i128 *)calloc(nch, sizeof(i128));
+#pragma omp parallel
+    {
+        uint64_t *bits = (uint64_t *)malloc(NW * 8);
+        uint32_t *pre = (uint32_t *)malloc((NW + 1) * 4);
+#pragma omp for schedule(dynamic, 1)
+        for (uint64_t ch = 0; ch < nch; ch++) {
+            uint64_t s0 = nseg * ch / nch, s1 = nseg * (ch + 1) / nch;
+            int64_t *cnt = cntT + ch * (nb + 1), *ms = msT + ch * (nb + 1);
+            i128 S = 0;
+            uint64_t B = nb; /* largest b with lo * p_b^2 < x; non-increasing in lo */
+            for (uint64_t sg = s0; sg < s1; sg++) {
+                uint64_t lo = sg * 2 * L, hi = lo + 2 * L;
+                while (B > c && lo != 0 && (u128)lo * D->P[B - 1] * D->P[B - 1] >= D->x) B--;
+                if (B <= c) continue;
+                memset(bits, 0xff, NW * 8);
+                for (uint32_t k = 1; k < c; k++) { /* odd primes p_2..p_c */
+                    uint64_t p = D->P[k];
+                    uint64_t m = (lo + 1 + p - 1) / p * p;
+                    if ((m & 1) == 0) m += p;
+                    for (; m < hi; m += 2 * p) {
+                        uint64_t i = (m - lo - 1) >> 1;
+                        bits[i >> 6] &= ~(1ull << (i & 63));
+                    }
+                }
+                int64_t total = 0;
+                for (uint64_t w = 0; w < NW; w++) total += __builtin_popcountll(bits[w]);
+                for (uint64_t b = c + 1; b <= B; b++) {
+                    uint64_t p = D->P[b - 1];
+                    u128 xp = D->x / p;
+                    uint64_t mlo = D->y / p; /* m > mlo */
+                    u128 t = xp / hi;
+                    if (t > mlo) mlo = (uint64_t)t;
+                    uint64_t mhi = D->y;
+                    if (lo != 0) {
+                        u128 t2 = xp / lo;
+                        if (t2 < mhi) mhi = (uint64_t)t2;
+                    }
+                    int have_pre = 0;
+                    uint64_t m = mlo + 1;
+                    if ((m & 1) == 0) m++;
+                    for (; m <= mhi; m += 2) {
+                        uint64_t i = (m - 1) / 2;
+                        if (mu[i] == 0 || lpf[i] <= p) continue;
+                        if (!have_pre) {
+                            uint32_t r = 0;
+                            for (uint64_t w = 0; w < NW; w++) {
+                                pre[w] = r;
+                                r += __builtin_popcountll(bits[w]);
+                            }
+                            pre[NW] = r;
+                            have_pre = 1;
+                        }
+                        uint64_t u = (uint64_t)(xp / m);
+                        uint64_t k = (u - lo + 1) / 2; /* bits [0, k) have n <= u */
+                        int64_t loc = pre[k >> 6];
+                        if (k & 63) loc += __builtin_popcountll(bits[k >> 6] & ((1ull << (k & 63)) - 1));
+                        int64_t phi = cnt[b] + loc;
+                        S += mu[i] > 0 ? -(i128)phi : (i128)phi;
+                        ms[b] += -mu[i];
+                    }
+                    cnt[b] += total;
+                    /* cross off p_b (including p_b itself) */
+                    uint64_t mm = (lo + 1 + p - 1) / p * p;
+                    if ((mm & 1) == 0) mm += p;
+                    for (; mm < hi; mm += 2 * p) {
+                        uint64_t i = (mm - lo - 1) >> 1;
+                        uint64_t bit = 1ull << (i & 63);
+                        if (bits[i >> 6] & bit) {
+                            bits[i >> 6] &= ~bit;
+                            total--;
+                        }
+                    }
+                }
+            }
+            Sc[ch] = S;
+        }
+        free(bits);
+        free(pre);
+    }
+    i128 H = 0;
+    int64_t *carry = (int64_t *)calloc(nb + 1, 8);
+    for (uint64_t ch = 0; ch < nch; ch++) {
+        H += Sc[ch];
+        for (uint64_t b = c + 1; b <= nb; b++) {
+            H += (i128)carry[b] * msT[ch * (nb + 1) + b];
+            carry[b] += cntT[ch * (nb + 1) + b];
+        }
+    }
+    free(carry);
+    free(cntT);
+    free(msT);
+    free(Sc);
+    return H;
+}
+
+static uint64_t tabmax_for(u128 x, uint64_t y)
+{
+    uint64_t z = (uint64_t)(x / y), sx = isqrt128(x);
+    uint64_t m = z > sx ? z : sx;
+    if (y > m) m = y;
+    return m + 2;
+}
+
+void orc_P2(uint64_t x_lo, uint64_t x_hi, uint64_t y, uint64_t *out)
+{
+    u128 x = mk128(x_lo, x_hi);
+    drctx_t D;
+    dr_init(&D, x, y, 6, tabmax_for(x, y));
+    put128(term_P2(&D), out);
+    dr_free(&D);
+}
+
+void orc_trivial(uint64_t x_lo, uint64_t x_hi, uint64_t y, uint64_t *out)
+{
+    u128 x = mk128(x_lo, x_hi);
+    drctx_t D;
+    uint64_t cb = icbrt128(x);
+    dr_init(&D, x, y, 6, (y > cb ? y : cb) + 2);
+    put128(term_trivial(&D), out);
+    dr_free(&D);
+}
+
+void orc_ordinary(uint64_t x_lo, uint64_t x_hi, uint64_t y, uint32_t c, uint64_t *out)
+{
+    u128 x = mk128(x_lo, x_hi);
+    uint64_t len = (y + 1) / 2;
+    int8_t *mu = (int8_t *)malloc(len + 1);
+    uint32_t *lpf = (uint32_t *)malloc((len + 1) * 4);
+    orc_mu_lpf(0, 2 * len, mu, lpf);
+    drctx_t D;
+    D.x = x;
+    D.y = y;
+    D.c = c;
+    put128(term_ordinary(&D, mu, lpf), out);
+    free(mu);
+    free(lpf);
+}
+
+void orc_easy(uint64_t x_lo, uint64_t x_hi, uint64_t y, uint64_t *out)
+{
+    u128 x = mk128(x_lo, x_hi);
+    drctx_t D;
+    uint64_t sx = isqrt128(x);
+    dr_init(&D, x, y, 6, (sx > y ? sx : y) + 2);
+    put128(term_easy(&D), out);
+    dr_free(&D);
+}
+
+void orc_hard(uint64_t x_lo, uint64_t x_hi, uint64_t y, uint32_t c, uint64_t *out)
+{
+    u128 x = mk128(x_lo, x_hi);
+    uint64_t len = y / 2 + 1;
+    int8_t *mu = (int8_t *)malloc(len);
+    uint32_t *lpf = (uint32_t *)malloc(len * 4);
+    orc_mu_lpf(0, 2 * len, mu, lpf);
+    drctx_t D;
+    dr_init(&D, x, y, c, 0);
+    put128(term_hard(&D, mu, lpf), out);
+    dr_free(&D);
+    free(mu);
+    free(lpf);
+}
+
+void orc_pi_dr(uint64_t x_lo, uint64_t x_hi, uint64_t y, uint32_t c, int nthreads,
+               uint64_t *terms)
+{
+    int saved = omp_get_max_threads();
+    if (nthreads > 0) omp_set_num_threads(nthreads);
+    u128 x = mk128(x_lo, x_hi);
+    uint64_t len = y / 2 + 1;
+    int8_t *mu = (int8_t *)malloc(len);
+    uint32_t *lpf = (uint32_t *)malloc(len * 4);
+    orc_mu_lpf(0, 2 * len, mu, lpf);
+    drctx_t D;
+    dr_init(&D, x, y, c, tabmax_for(x, y));
+    i128 p2 = term_P2(&D);
+    i128 s0 = term_ordinary(&D, mu, lpf);
+    i128 tr = term_trivial(&D);
+    i128 ez = term_easy(&D);
+    i128 hd = term_hard(&D, mu, lpf);
+    i128 piy = (i128)pitab_pi(&D.tab, y);
+    i128 pix = s0 + tr + ez + hd + piy - 1 - p2;
+    put128(p2, terms + 0);
+    put128(s0, terms + 2);
+    put128(tr, terms + 4);
+    put128(ez, terms + 6);
+    put128(hd, terms + 8);
+    put128(piy, terms + 10);
+    put128(pix, terms + 12);
+    dr_free(&D);
+    free(mu);
+    free(lpf);
+    if (nthreads > 0) omp_set_num_threads(saved);
+}
+
+/* ------------------------------------------------------------------ Lehmer */
+
+uint64_t orc_pi_lehmer(uint64_t x)
+{
+    if (x < 100000) return orc_pi_sieve(x);
+    uint64_t r4 = isqrt128(isqrt128(x)), r3 = icbrt128(x), r2 = isqrt128(x);
+    uint64_t np;
+    uint32_t *P = primes_upto(r2 + 64, &np);
+    uint64_t a = 0;
+    while (P[a] <= r4) a++;
+    uint64_t tmax = x / P[a] + 2; /* pi(x / p_i) for i > a */
+    if (tmax < r2 + 2) tmax = r2 + 2;
+    pitab_t tab = pitab_build(tmax);
+    uint64_t b = pitab_pi(&tab, r2), c3 = pitab_pi(&tab, r3);
+    wheel_t wh = wheel_make(6);
+    phictx_t C = {P, np, &tab, &wh};
+    int64_t phix = (int64_t)wheel_phi(&wh, x);
+#pragma omp parallel for schedule(dynamic, 1) reduction(- : phix)
+    for (uint64_t k = 7; k <= a; k++) phix -= phi_rec(&C, x / P[k - 1], (uint32_t)k - 1);
+    i128 s = (i128)phix + (i128)(b + a - 2) * (i128)(b - a + 1) / 2;
+    i128 sub = 0;
+#pragma omp parallel for schedule(dynamic, 16) reduction(+ : sub)
+    for (uint64_t i = a + 1; i <= b; i++) {
+        uint64_t w = x / P[i - 1];
+        i128 t = (i128)pitab_pi(&tab, w);
+        if (i <= c3) {
+            uint64_t bi = pitab_pi(&tab, isqrt128(w));
+            for (uint64_t j = i; j <= bi; j++) t += (i128)pitab_pi(&tab, w / P[j - 1]) - (i128)(j - 1);
+        }
+        sub += t;
+    }
+    s -= sub;
+    free(wh.cnt);
+    pitab_free(&tab);
+    free(P);
+    return (uint64_t)s;
+}
