@@ -562,7 +562,7 @@ __global__ void __launch_bounds__(512) k_hard(const QD *__restrict__ qd, uint32_
             // cross off p_b, counting bits that were still set
             uint32_t cleared = 0;
             if (p < 64) {
-                const uint32_t Mp = (p < 32) ? (1u | (1u << p)) : 1u;
+                const uint32_t Mp = every_pth_bit(p);  // p < 32 has several multiples per word
                 const uint32_t st = 64u % p;
                 uint32_t r = (s_r0[k] + (64u * w0) % p) % p;
                 for (uint32_t j = 0; j < CPT; j++) {
