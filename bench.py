@@ -207,8 +207,45 @@ def run_reference(args, world, rank):
     print(json.dumps(line), flush=True)
 
 
+def run_single(args, world, rank, local):
+    """One query of size --single (e.g. 1e15 or 1e17) with y = alpha * icbrt(x):
+    latency per query through the plain API, term by term timing of the hard leaves."""
+    import cudapix_b200 as cpx
+
+    ctx = cpx.Context(local)
+    ctx.set_timing(True)
+    x = int(float(args.single)) if "e" in args.single.lower() else int(args.single)
+    y = cpx.default_y(x, args.alpha) if args.alpha else 0
+    ref = None
+    for _ in range(args.warmup):
+        t = cpx.pi_terms(x, y, 6, ctx=ctx)
+        ref = ref or t
+        assert t == ref
+    lat, hard = [], []
+    with Clocks(local) as clk:
+        for _ in range(args.steps):
+            ctx.flush_l2()
+            ctx.timer_start()
+            t = cpx.pi_terms(x, y, 6, ctx=ctx)
+            lat.append(ctx.timer_stop())
+            hard.append(ctx.last_hard_stats())
+            assert ref is None or t == ref
+    if rank != 0:
+        return
+    ms = statistics.median(lat)
+    hm, hb = hard[-1]
+    print(json.dumps({"metric": "pi(x) single-query latency", "value": ms, "unit": "ms", "n_gpus": world,
+                      "steps": args.steps, "warmup": args.warmup, "higher_is_better": False,
+                      "config": {"workload": f"single x={x} y={t['y']} z={t['z']} c=6", "alpha": args.alpha},
+                      "pi": t["pi"], "terms": {k: t[k] for k in ("P2", "ordinary", "trivial", "easy", "hard")},
+                      "hard_ms": hm, "s2_gbs": (hb / (hm / 1000)) / 1e9 if hm else None,
+                      "batch_device_ms": ctx.last_batch_ms(), "clocks": clk.summary()}), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
+    ap.add_argument("--single", default=None, help="time one query of this size instead of the batch")
+    ap.add_argument("--alpha", type=float, default=0.0, help="y = alpha * icbrt(x) for --single (0: reference alpha)")
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
@@ -222,6 +259,9 @@ def main():
     world, rank, local = dist_setup()
     if args.impl == "reference":
         run_reference(args, world, rank)
+        return
+    if args.single:
+        run_single(args, world, rank, local)
         return
 
     import cudapix_b200 as cpx

@@ -125,6 +125,7 @@ _SIGS = {
     "cpx_gen_h_mu": (ctypes.c_int, [P, u64, u64, P]),
     "cpx_gen_h_lpf32": (ctypes.c_int, [P, u64, u64, P]),
     "cpx_mutest": (ctypes.c_int, [P, u64, pi64]),
+    "cpx_mutest_noalloc": (ctypes.c_int, [P, u64, pi64]),
     "cpx_pitable": (ctypes.c_int, [P, u64, PP]),
     "cpx_pitable_window": (ctypes.c_int, [P, u64, u64, P, pu64]),
     "cpx_primes": (ctypes.c_int, [P, u64, u64, PP, pu64]),

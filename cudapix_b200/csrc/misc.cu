@@ -32,6 +32,15 @@ __global__ void k_mu_sums(const int8_t *__restrict__ mu, uint64_t n_odd, uint64_
     if ((threadIdx.x & 31) == 0 && s) atomicAdd(out, (unsigned long long)s);
 }
 
+// Mertens reduction of a caller mu array into a caller accumulator, on a
+// caller stream; launches only, allocates nothing.
+cudaError_t launch_mu_sums(cudaStream_t st, const int8_t *mu, uint64_t n_odd, uint64_t v1, uint64_t v2,
+                           unsigned long long *acc, unsigned grid)
+{
+    k_mu_sums<<<grid, 256, 0, st>>>(mu, n_odd, v1, v2, acc);
+    return cudaGetLastError();
+}
+
 int64_t mutest(cpx_ctx *ctx, uint64_t top)
 {
     if (top <= 1) return 0;

@@ -578,6 +578,20 @@ __global__ void __launch_bounds__(kThreads) k_mulpf(uint64_t lo0, uint64_t hi_al
     }
 }
 
+// mu of the odd n in [lo, hi) (hi <= 2^32) into a caller buffer with a
+// caller prime list, on a caller stream; launches only, allocates nothing.
+cudaError_t launch_mu_only(cudaStream_t st, uint64_t lo, uint64_t hi, const uint32_t *P, uint32_t np,
+                           int8_t *mu)
+{
+    const uint64_t seg = MuSeg<unsigned int>::N;
+    const uint64_t nblk = (hi - lo + 2 * seg - 1) / (2 * seg);
+    if (nblk == 0) return cudaSuccess;
+    const uint32_t nsmall = np > 54 ? 53 : (np ? np - 1 : 0);
+    k_mulpf<unsigned int><<<(unsigned)nblk, kThreads, 0, st>>>(lo, hi, P, np, nsmall, mu, nullptr, nullptr,
+                                                                nullptr);
+    return cudaGetLastError();
+}
+
 void mulpf_sieve(cpx_ctx *ctx, uint64_t lo, uint64_t hi, int8_t *mu, uint32_t *lpf32, uint64_t *lpf64,
                  int32_t *packed)
 {

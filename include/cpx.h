@@ -147,6 +147,16 @@ int cpx_gen_h_mu(cpx_ctx *ctx, uint64_t lo, uint64_t hi, int8_t *h_mu);
 int cpx_gen_h_lpf32(cpx_ctx *ctx, uint64_t lo, uint64_t hi, uint32_t *h_lpf);
 /* Mertens sum over 1 <= n < top                              (src/mutest.cu:6) */
 int cpx_mutest(cpx_ctx *ctx, uint64_t top, int64_t *out);
+/* The same Mertens sum without allocating any device memory; no counterpart
+ * in the reference.  For callers that cannot call cudaMalloc (their device
+ * memory belongs to another allocator, or cudaMalloc/cudaFree would
+ * synchronise a latency-critical path).  Scratch lives in one file-scope
+ * static device array of 16 MiB + 16 KiB that every GPU loading the library
+ * holds until exit; top must be <= 33554432 (CPX_ERANGE otherwise).  The
+ * first call on a device looks up the array's device address, so make it
+ * before any stream capture on that device.  Calls share the array: calls
+ * that overlap on the GPU race.  Uses the context's stream and device. */
+int cpx_mutest_noalloc(cpx_ctx *ctx, uint64_t top, int64_t *out);
 /* dense pi table of get_d_piTable: out[k] = pi(2k - 1), k < hi / 2, hi < 2^32
  *                                                          (src/pitable.cu:10) */
 int cpx_pitable(cpx_ctx *ctx, uint64_t hi, uint32_t **d_out);
