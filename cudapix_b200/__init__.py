@@ -205,14 +205,14 @@ def Ordinary(x, y, c=6, ctx=None):
     return o.value
 
 
-def S2_easy(x, y, ctx=None):
+def S2_easy(x, y, c=6, ctx=None):
     ctx = ctx or context()
     if _wide(x):
         o = U128()
-        ctx.call("cpx_S2_easy_u128", U128.of(x), y, ctypes.byref(o))
+        ctx.call("cpx_S2_easy_u128", U128.of(x), y, c, ctypes.byref(o))
         return o.value(signed=True)
     o = ctypes.c_int64()
-    ctx.call("cpx_S2_easy_u64", x, y, ctypes.byref(o))
+    ctx.call("cpx_S2_easy_u64", x, y, c, ctypes.byref(o))
     return o.value
 
 

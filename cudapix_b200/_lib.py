@@ -112,8 +112,8 @@ _SIGS = {
     "cpx_trivial_u128": (ctypes.c_int, [P, U128, u64, pU]),
     "cpx_ordinary_u64": (ctypes.c_int, [P, u64, u64, u16, pi64]),
     "cpx_ordinary_u128": (ctypes.c_int, [P, U128, u64, u16, pU]),
-    "cpx_S2_easy_u64": (ctypes.c_int, [P, u64, u64, pi64]),
-    "cpx_S2_easy_u128": (ctypes.c_int, [P, U128, u64, pU]),
+    "cpx_S2_easy_u64": (ctypes.c_int, [P, u64, u64, u16, pi64]),
+    "cpx_S2_easy_u128": (ctypes.c_int, [P, U128, u64, u16, pU]),
     "cpx_S2_hard_u64": (ctypes.c_int, [P, u64, u64, u16, pi64]),
     "cpx_S2_hard_u128": (ctypes.c_int, [P, U128, u64, u16, pU]),
     "cpx_pi_u64": (ctypes.c_int, [P, u64, u64, u16, pu64, ctypes.POINTER(Terms)]),

@@ -287,19 +287,19 @@ int cpx_ordinary_u128(cpx_ctx *ctx, cpx_u128 x, uint64_t y, uint16_t c, cpx_u128
         *out = C128s(t[1]);
     });
 }
-int cpx_S2_easy_u64(cpx_ctx *ctx, uint64_t x, uint64_t y, int64_t *out)
+int cpx_S2_easy_u64(cpx_ctx *ctx, uint64_t x, uint64_t y, uint16_t c, int64_t *out)
 {
     return guarded(ctx, [&] {
         i128 t[7];
-        one(ctx, x, y, 6, TERM_EASY, t);
+        one(ctx, x, y, c, TERM_EASY, t);
         *out = (int64_t)t[3];
     });
 }
-int cpx_S2_easy_u128(cpx_ctx *ctx, cpx_u128 x, uint64_t y, cpx_u128 *out)
+int cpx_S2_easy_u128(cpx_ctx *ctx, cpx_u128 x, uint64_t y, uint16_t c, cpx_u128 *out)
 {
     return guarded(ctx, [&] {
         i128 t[7];
-        one(ctx, U(x), y, 6, TERM_EASY, t);
+        one(ctx, U(x), y, c, TERM_EASY, t);
         *out = C128s(t[3]);
     });
 }

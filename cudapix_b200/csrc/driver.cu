@@ -77,6 +77,17 @@ bool dr_domain_ok(u128 x, uint64_t y, uint32_t c)
     return true;
 }
 
+// Segments (of `span` integers) that sieve level b, p = p_b: those with
+// hi > p^2 and (lo = 0 or p^2 lo < x); the same rule as k_hard_plan.
+static uint64_t segments_at_level(u128 x, uint64_t span, uint64_t p, uint64_t nseg)
+{
+    const u128 p2 = (u128)p * p;
+    const u128 first = p2 / span;
+    const u128 last = (x - 1) / (p2 * span);  // largest s >= 0 with s * span * p^2 < x
+    const u128 hi = std::min<u128>(last, (u128)nseg - 1);
+    return hi >= first ? (uint64_t)(hi - first + 1) : 0;
+}
+
 static uint32_t pick_lbits(cpx_ctx *ctx, uint64_t z, uint32_t threads, uint32_t forced)
 {
     const uint32_t minb = (threads >= 512) ? 16 : (threads >= 256 ? 15 : 14);
@@ -136,7 +147,15 @@ void run_batch(cpx_ctx *ctx, const BatchReq &rq)
         if (mask & TERM_TRIV) N = std::max<uint64_t>(N, std::max(y, cx) + 1);
         if (mask & TERM_EASY) N = std::max<uint64_t>(N, std::max(sx, y) + 1);
         if (mask & (TERM_ORD | TERM_HARD)) Y = std::max(Y, y);
-        if (mask & TERM_HARD) Pneed = std::max<uint64_t>(Pneed, r4 + 1);
+        if (mask & TERM_HARD) {
+            Pneed = std::max<uint64_t>(Pneed, r4 + 1);
+            // carries below p_b^2 come from the pi table; prime m of the sparse levels from its bitmap
+            N = std::max<uint64_t>(N, std::max<uint64_t>(r4 * r4 + 2, y + 1));
+        }
+        if (mask & TERM_EASY) {
+            Pneed = std::max<uint64_t>(Pneed, r4 + 1);  // composite easy leaves: p_b <= iroot4(x)
+            Y = std::max(Y, y);
+        }
         if (mask == TERM_PI) N = std::max<uint64_t>(N, y + 1);
     }
     if (N > rq.max_table_n) fail(CPX_ERANGE, "pi table bound exceeds the configured limit");
@@ -145,7 +164,7 @@ void run_batch(cpx_ctx *ctx, const BatchReq &rq)
     ensure_primes(ctx, std::max<uint64_t>(Pneed, cpx_isqrt(Y + 1) + 2));
     bool any_direct = false;
     for (const QD &d : qd) any_direct |= d.direct != 0;
-    const bool need_tab = (mask & (TERM_P2 | TERM_TRIV | TERM_EASY)) || mask == TERM_PI || any_direct;
+    const bool need_tab = (mask & (TERM_P2 | TERM_TRIV | TERM_EASY | TERM_HARD)) || mask == TERM_PI || any_direct;
     if (need_tab) ensure_pitable(ctx, N);
     if (Y) ensure_mulpf(ctx, Y + 8);
     if (mask & TERM_ORD) ensure_wheel(ctx, c);
@@ -157,15 +176,44 @@ void run_batch(cpx_ctx *ctx, const BatchReq &rq)
              *p_seg = p_easy + (Q + 1), *p_comb = p_seg + (Q + 1);
     uint64_t hard_entries = 0;
     uint32_t lbits_max = 0;
+    std::vector<EasyLvl> elv;
+    uint64_t n_ecomp = 0;
     for (uint32_t i = 0; i < Q; i++) {
         QD &d = qd[i];
         uint64_t n_ord = 0, n_p2 = 0, n_triv = 0, n_easy = 0, n_seg = 0, n_comb = 0;
         if (!d.direct) {
             const u128 x = d.x;
+            const uint64_t pc = kSmallPrimes[c];
             if (mask & TERM_ORD) n_ord = ((d.y + 1) / 2 + 3) / 4;
             if ((mask & TERM_P2) && d.sx > d.y) n_p2 = ((d.sx - 1) >> 7) - (d.y >> 7) + 1;
             if (mask & TERM_TRIV) n_triv = (d.cx > d.tx) ? ((d.cx - 1) >> 7) - (d.tx >> 7) + 1 : 1;
-            if ((mask & TERM_EASY) && d.cx > d.r4) n_easy = ((d.cx - 1) >> 7) - (d.r4 >> 7) + 1;
+            if ((mask & TERM_EASY) && d.cx > pc) n_easy = ((d.cx - 1) >> 7) - (pc >> 7) + 1;
+            if (mask & TERM_EASY) {
+                // composite easy leaves: levels b with p_b <= iroot4(x), p_b^2 < y and
+                // max(y/p_b, x/p_b^3) < y
+                const uint64_t nb4 = host_pi(hP, d.r4);
+                for (uint64_t b = c + 1; b <= nb4; b++) {
+                    const uint64_t p = hP[b - 1];
+                    if (p * p >= d.y) break;
+                    const u128 x3 = x / ((u128)p * p * p);
+                    uint64_t mlo = d.y / p;
+                    if (x3 > (u128)mlo) mlo = x3 >= (u128)d.y ? d.y : (uint64_t)x3;
+                    if (mlo >= d.y) continue;
+                    const uint64_t mfirst = (mlo + 1) | 1;
+                    EasyLvl r;
+                    r.q = i;
+                    r.b = (uint32_t)b;
+                    r.p = (uint32_t)p;
+                    r.pad = 0;
+                    r.i_lo = (mfirst - 1) / 2;
+                    r.i_hi = (d.y - 1) / 2 + 1;
+                    if (r.i_lo >= r.i_hi) continue;
+                    r.i_base = r.i_lo & ~uint64_t(3);
+                    r.unit0 = n_ecomp;
+                    n_ecomp += (r.i_hi - r.i_base + 1023) / 1024;
+                    elv.push_back(r);
+                }
+            }
             if (mask & TERM_HARD) {
                 d.nb = (uint32_t)host_pi(hP, d.r4);
                 if (d.nb > c) {
@@ -176,9 +224,7 @@ void run_batch(cpx_ctx *ctx, const BatchReq &rq)
                     n_seg = d.nseg;
                     n_comb = d.nb - c;
                     for (uint32_t b = c + 1; b <= d.nb; b++) {
-                        const u128 K = (u128)span * hP[b - 1] * hP[b - 1];
-                        const u128 cnt = 1 + (x - 1) / K;
-                        hard_entries += (uint64_t)std::min<u128>(cnt, d.nseg);
+                        hard_entries += segments_at_level(x, span, hP[b - 1], d.nseg);
                     }
                 }
             }
@@ -206,12 +252,19 @@ void run_batch(cpx_ctx *ctx, const BatchReq &rq)
     pl.n_seg = p_seg[Q];
     pl.n_comb = p_comb[Q];
     pl.hard_entries = hard_entries;
-    const size_t qd_bytes = sizeof(QD) * Q, pre_bytes = pre.size() * 8;
+    const size_t qd_bytes = sizeof(QD) * Q, pre_bytes = (pre.size() * 8 + 15) & ~size_t(15);
+    const size_t elv_bytes = elv.size() * sizeof(EasyLvl);
     const size_t acc_words = (size_t)Q * kAccStride;
-    unsigned char *dbuf = (unsigned char *)ctx->b_work[0].get(qd_bytes + pre_bytes + acc_words * 8 + 64);
+    unsigned char *dbuf =
+        (unsigned char *)ctx->b_work[0].get(qd_bytes + pre_bytes + elv_bytes + acc_words * 8 + 64);
     QD *d_qd = reinterpret_cast<QD *>(dbuf);
     uint64_t *d_pre = reinterpret_cast<uint64_t *>(dbuf + qd_bytes);
-    unsigned long long *d_acc = reinterpret_cast<unsigned long long *>(dbuf + qd_bytes + pre_bytes);
+    EasyLvl *d_elv = reinterpret_cast<EasyLvl *>(dbuf + qd_bytes + pre_bytes);
+    unsigned long long *d_acc =
+        reinterpret_cast<unsigned long long *>(dbuf + qd_bytes + pre_bytes + elv_bytes);
+    pl.elv = d_elv;
+    pl.n_elv = (uint32_t)elv.size();
+    pl.n_ecomp = n_ecomp;
     pl.qd = d_qd;
     pl.pre_ord = d_pre;
     pl.pre_p2 = d_pre + (Q + 1);
@@ -230,9 +283,10 @@ void run_batch(cpx_ctx *ctx, const BatchReq &rq)
     u128 *d_out = ctx->b_work[6].as<u128>(Q);
 
     // one staging copy host -> device
-    std::vector<unsigned char> stage(qd_bytes + pre_bytes);
+    std::vector<unsigned char> stage(qd_bytes + pre_bytes + elv_bytes);
     memcpy(stage.data(), qd.data(), qd_bytes);
-    memcpy(stage.data() + qd_bytes, pre.data(), pre_bytes);
+    memcpy(stage.data() + qd_bytes, pre.data(), pre.size() * 8);
+    if (elv_bytes) memcpy(stage.data() + qd_bytes + pre_bytes, elv.data(), elv_bytes);
     CPX_CUDA(cudaMemcpyAsync(dbuf, stage.data(), stage.size(), cudaMemcpyHostToDevice, ctx->stream));
     CPX_CUDA(cudaMemsetAsync(d_acc, 0, acc_words * 8, ctx->stream));
 
@@ -241,7 +295,10 @@ void run_batch(cpx_ctx *ctx, const BatchReq &rq)
     if (mask & TERM_ORD) launch_ordinary(ctx, pl);
     if (mask & TERM_P2) launch_p2(ctx, pl);
     if (mask & TERM_TRIV) launch_trivial(ctx, pl);
-    if (mask & TERM_EASY) launch_easy(ctx, pl);
+    if (mask & TERM_EASY) {
+        launch_easy(ctx, pl);
+        launch_easy_comp(ctx, pl);
+    }
     if (mask & TERM_HARD) launch_hard(ctx, pl);
     launch_finalize(ctx, pl, d_out, mask == TERM_PI);
     if (ctx->timing) CPX_CUDA(cudaEventRecord(ctx->ev_b1, ctx->stream));
@@ -280,9 +337,7 @@ void run_batch(cpx_ctx *ctx, const BatchReq &rq)
             if (d.direct || d.nb <= c) continue;
             const uint64_t span = 2ull << d.lbits;
             for (uint32_t b = c + 1; b <= d.nb; b++) {
-                const u128 K = (u128)span * hP[b - 1] * hP[b - 1];
-                const u128 cnt = 1 + (d.x - 1) / K;
-                bytes += (double)std::min<u128>(cnt, d.nseg) * (double)(1u << d.lbits) / 8.0;
+                bytes += (double)segments_at_level(d.x, span, hP[b - 1], d.nseg) * (double)(1u << d.lbits) / 8.0;
             }
         }
         ctx->last_hard_bytes = bytes;

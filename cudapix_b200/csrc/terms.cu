@@ -18,6 +18,7 @@
 namespace cpx {
 
 constexpr unsigned FULL = 0xffffffffu;
+__constant__ uint32_t c_pc[9] = {1, 2, 3, 5, 7, 11, 13, 17, 19};  // p_c for c = 0..8
 
 __device__ __forceinline__ uint32_t find_q(const uint64_t *__restrict__ pre, uint32_t Q, uint64_t u)
 {
@@ -256,10 +257,12 @@ __global__ void __launch_bounds__(kThreads) k_trivial(const QD *__restrict__ qd,
 }
 
 // ---------------------------------------------------------------------- easy
-// Leaves (p, q), q prime, iroot4(x) < p <= icbrt(x), max(p, y/p) < q <= min(y, x/p^2);
-// value phi(x/(pq), pi(p) - 1) = pi(x/(pq)) - pi(p) + 2.  A warp takes one
-// table entry of p candidates at a time (ticket counter); its lanes stride
-// over the table entries of the q range.
+// Easy leaves are the non-trivial leaves with u = x/(p_b m) < p_b^2, where
+// phi(u, b - 1) = pi(u) - b + 2 is one pi-table lookup.  k_easy takes the
+// prime m = q: p_c < p <= icbrt(x), max(p, y/p, x/p^3) < q <= min(y, x/p^2)
+// (for p > iroot4(x) the bound x/p^3 is below p).  A warp takes one table
+// entry of p candidates at a time (ticket counter); its lanes stride over the
+// table entries of the q range.  k_easy_comp takes the composite m.
 template <class XT>
 __global__ void __launch_bounds__(kThreads) k_easy(const QD *__restrict__ qd, uint32_t Q,
                                                    const uint64_t *__restrict__ pre, uint64_t total,
@@ -276,10 +279,10 @@ __global__ void __launch_bounds__(kThreads) k_easy(const QD *__restrict__ qd, ui
         const uint32_t q = find_q(pre, Q, unit);
         const QD &d = qd[q];
         const XT x = xload<XT>(d);
-        const uint64_t y = d.y, r4 = d.r4, cx = d.cx;
-        const uint64_t w = (r4 >> 7) + (unit - __ldg(pre + q));
+        const uint64_t y = d.y, pc = c_pc[d.c], cx = d.cx;
+        const uint64_t w = (pc >> 7) + (unit - __ldg(pre + q));
         const ulonglong2 e = __ldg(reinterpret_cast<const ulonglong2 *>(T) + w);
-        uint64_t pb = e.x & range_mask(w, r4, cx);
+        uint64_t pb = e.x & range_mask(w, pc, cx);
         i128 s = 0;
         while (pb) {
             const int j = __ffsll((long long)pb) - 1;
@@ -290,6 +293,11 @@ __global__ void __launch_bounds__(kThreads) k_easy(const QD *__restrict__ qd, ui
             uint64_t qlo = y / p;
             if (qlo < p) qlo = p;
             const XT xpp = xp / (XT)p;
+            {
+                // p <= iroot4(x): only q > x/p^3 (x/(pq) < p^2) are easy
+                const XT x3 = xpp / (XT)p;
+                if (x3 > (XT)qlo) qlo = (x3 >= (XT)y) ? y : (uint64_t)x3;
+            }
             const uint64_t qhi = (xpp < (XT)y) ? (uint64_t)xpp : y;
             if (qhi <= qlo) continue;
             const uint64_t wq0 = qlo >> 7, wq1 = (qhi - 1) >> 7;
@@ -310,6 +318,57 @@ __global__ void __launch_bounds__(kThreads) k_easy(const QD *__restrict__ qd, ui
         }
         const i128 ws = cpx_warp_sum_i128(s);
         if (lane == 0) acc_add(acc, q, ACC_EASY, ws);
+    }
+}
+
+// Composite easy leaves: p_b <= min(iroot4(x), sqrt y), m composite with
+// lpf(m) > p_b, mu(m) != 0, max(y/p_b, x/p_b^3) < m <= y; value
+// -mu(m) (pi(x/(p_b m)) - b + 2).  Work = (level record, chunk of 1024 odd m);
+// a warp walks its chunk 128 m at a time, one 16-byte load of packed mu*lpf per lane.
+template <class XT>
+__global__ void __launch_bounds__(kThreads) k_easy_comp(const QD *__restrict__ qd, const EasyLvl *__restrict__ lv,
+                                                        uint32_t nlv, uint64_t total,
+                                                        const int32_t *__restrict__ MU,
+                                                        const cpx_pient *__restrict__ T,
+                                                        unsigned long long *__restrict__ acc)
+{
+    const int lane = threadIdx.x & 31;
+    const uint64_t gw = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const uint64_t nw = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+    for (uint64_t unit = gw; unit < total; unit += nw) {
+        uint32_t lo = 0, hi = nlv;  // lv[lo].unit0 <= unit < lv[hi].unit0
+        while (hi - lo > 1) {
+            const uint32_t mid = (lo + hi) >> 1;
+            if (lv[mid].unit0 <= unit) lo = mid;
+            else hi = mid;
+        }
+        const EasyLvl r = lv[lo];
+        const QD &d = qd[r.q];
+        const XT xp = xload<XT>(d) / (XT)r.p;
+        const uint64_t base = r.i_base + (unit - r.unit0) * 1024;  // multiple of 4
+        int64_t s = 0;
+        for (int it = 0; it < 8; it++) {
+            const uint64_t i0 = base + 128 * it + 4 * lane;
+            if (i0 >= r.i_hi) break;
+            const int4 v4 = __ldg(reinterpret_cast<const int4 *>(MU) + (i0 >> 2));
+            const int32_t vals[4] = {v4.x, v4.y, v4.z, v4.w};
+#pragma unroll
+            for (int k = 0; k < 4; k++) {
+                const uint64_t i = i0 + k;
+                if (i < r.i_lo || i >= r.i_hi) continue;
+                const int32_t v = vals[k];
+                const uint64_t m = 2 * i + 1;
+                const uint32_t av = (uint32_t)(v > 0 ? v : -v);
+                if (v == 0 || av <= r.p || (uint64_t)av >= m) continue;  // mu = 0, lpf <= p, or m prime
+                const uint64_t uu = (uint64_t)(xp / (XT)m);
+                const int64_t val = (int64_t)cpx_pi_dev(T, uu) - (int64_t)r.b + 2;
+                s += (v > 0) ? -val : val;
+            }
+        }
+        LaneAcc a;
+        a.q = r.q;
+        a.v = s;
+        warp_flush(a, acc, ACC_EASY);
     }
 }
 
@@ -367,6 +426,7 @@ __global__ void __launch_bounds__(512) k_hard(const QD *__restrict__ qd, uint32_
                                               const uint32_t *__restrict__ seg_B,
                                               const uint64_t *__restrict__ seg_off,
                                               const uint32_t *__restrict__ P, const int32_t *__restrict__ MU,
+                                              const cpx_pient *__restrict__ Tpi,
                                               uint32_t *__restrict__ out_cnt, int32_t *__restrict__ out_ms,
                                               uint64_t cap, unsigned long long *__restrict__ acc,
                                               uint32_t lbits_max)
@@ -478,6 +538,11 @@ __global__ void __launch_bounds__(512) k_hard(const QD *__restrict__ qd, uint32_
                 const XT t2 = xp / (XT)lo;
                 if (t2 < (XT)mhi) mhi = (uint64_t)t2;
             }
+            {
+                // hard leaves only: x/(p m) >= p^2, i.e. m <= x/p^3
+                const XT t3 = xp / (XT)(p * p);
+                if (t3 < (XT)mhi) mhi = (uint64_t)t3;
+            }
             if (mhi < mlo) mhi = mlo;
             s_p[tid] = (uint32_t)p;
             s_xp[tid] = xp;
@@ -519,33 +584,60 @@ __global__ void __launch_bounds__(512) k_hard(const QD *__restrict__ qd, uint32_
                 __syncthreads();
                 const XT xp = s_xp[k];
                 int32_t msl = 0;
-                uint64_t m = (uint64_t)mlo + 1;
-                m |= 1;  // odd
-                for (m += 2 * (uint64_t)tid; m <= mhi; m += 2 * (uint64_t)T) {
-                    const int32_t v = __ldg(MU + ((m - 1) >> 1));
-                    const int32_t av = v > 0 ? v : -v;
-                    if (v == 0 || (uint32_t)av <= p) continue;
-                    const uint64_t uu = (uint64_t)(xp / (XT)m);
-                    const uint32_t kk = (uint32_t)((uu - lo + 1) >> 1);  // bits [0, kk) have n <= uu
-                    uint32_t cntv = 0;
-                    if (kk) {
-                        const uint32_t jb = kk - 1, w = jb >> 5, ch = w >> 2, ow = ch >> s;
-                        cntv = toff[ow] + cp16[ch];
-                        for (uint32_t i = 0; i < (ow >> 5); i++) cntv += wsum[i];
-                        const uint4 v4 = reinterpret_cast<const uint4 *>(bm)[swz(ch, s)];
-                        const uint32_t wi = w & 3, msk = (2u << (jb & 31)) - 1u;
-                        const uint32_t a0 = v4.x, a1 = v4.y, a2 = v4.z, a3 = v4.w;
-                        if (wi == 0) cntv += __popc(a0 & msk);
-                        else if (wi == 1) cntv += __popc(a0) + __popc(a1 & msk);
-                        else if (wi == 2) cntv += __popc(a0) + __popc(a1) + __popc(a2 & msk);
-                        else cntv += __popc(a0) + __popc(a1) + __popc(a2) + __popc(a3 & msk);
+                // survivors of the segment with n <= uu: per-thread, per-chunk
+                // prefixes plus a popcount inside the 16-byte chunk
+                auto seg_count = [&](uint64_t uu) -> uint32_t {
+                    const uint32_t kk = (uint32_t)((uu - lo + 1) >> 1);  // bits [0, kk)
+                    if (!kk) return 0u;
+                    const uint32_t jb = kk - 1, w = jb >> 5, ch = w >> 2, ow = ch >> s;
+                    uint32_t cv = toff[ow] + cp16[ch];
+                    for (uint32_t i = 0; i < (ow >> 5); i++) cv += wsum[i];
+                    const uint4 v4 = reinterpret_cast<const uint4 *>(bm)[swz(ch, s)];
+                    const uint32_t wi = w & 3, msk = (2u << (jb & 31)) - 1u;
+                    if (wi == 0) cv += __popc(v4.x & msk);
+                    else if (wi == 1) cv += __popc(v4.x) + __popc(v4.y & msk);
+                    else if (wi == 2) cv += __popc(v4.x) + __popc(v4.y) + __popc(v4.z & msk);
+                    else cv += __popc(v4.x) + __popc(v4.y) + __popc(v4.z) + __popc(v4.w & msk);
+                    return cv;
+                };
+                if ((uint64_t)p * p > y) {
+                    // m must be a prime q > p: walk the pi-table bitmap of (max(mlo, p), mhi]
+                    const uint64_t qa = mlo > p ? mlo : p;
+                    if (mhi > qa) {
+                        const uint64_t w0q = qa >> 7, w1q = (mhi - 1) >> 7;
+                        for (uint64_t wq = w0q + tid; wq <= w1q; wq += T) {
+                            const ulonglong2 e = __ldg(reinterpret_cast<const ulonglong2 *>(Tpi) + wq);
+                            uint64_t qb = e.x & range_mask(wq, qa, mhi);
+                            while (qb) {
+                                const int j = __ffsll((long long)qb) - 1;
+                                qb &= qb - 1;
+                                const uint64_t m = 128 * wq + 2 * j + 1;
+                                S += seg_count((uint64_t)(xp / (XT)m));  // mu(q) = -1
+                                msl += 1;
+                            }
+                        }
                     }
-                    if (v > 0) {
-                        S -= cntv;
-                        msl -= 1;
-                    } else {
-                        S += cntv;
-                        msl += 1;
+                } else {
+                    // any squarefree m with lpf(m) > p: 16-byte loads of packed mu*lpf
+                    const uint64_t i_lo = ((uint64_t)mlo + 1) >> 1, i_hi = ((uint64_t)mhi - 1) >> 1;  // m = 2i + 1
+                    for (uint64_t g = (i_lo >> 2) + tid; g <= (i_hi >> 2); g += T) {
+                        const int4 v4 = __ldg(reinterpret_cast<const int4 *>(MU) + g);
+                        const int32_t vals[4] = {v4.x, v4.y, v4.z, v4.w};
+#pragma unroll
+                        for (int kq = 0; kq < 4; kq++) {
+                            const uint64_t i = 4 * g + kq;
+                            const int32_t v = vals[kq];
+                            if (i < i_lo || i > i_hi || v == 0) continue;
+                            if ((uint32_t)(v > 0 ? v : -v) <= p) continue;
+                            const uint32_t cv = seg_count((uint64_t)(xp / (XT)(2 * i + 1)));
+                            if (v > 0) {
+                                S -= cv;
+                                msl -= 1;
+                            } else {
+                                S += cv;
+                                msl += 1;
+                            }
+                        }
                     }
                 }
 #pragma unroll
@@ -599,8 +691,12 @@ __global__ void __launch_bounds__(512) k_hard(const QD *__restrict__ qd, uint32_
     if (tid == 0) acc_add(acc, q, ACC_HARD, Sb);
 }
 
-// B(seg) = pi(min(r4, isqrt((x - 1) / lo))) (pi(r4) for lo = 0): the largest b
-// whose leaves can reach the segment; levels per segment = max(0, B - c).
+// B(seg) = pi(min(r4, isqrt((x - 1) / lo), isqrt(hi - 1))): the levels b a
+// segment sieves.  p_b^2 * lo < x bounds the levels whose leaves can reach
+// the segment or a later one; p_b^2 < hi skips the levels whose leaves all lie
+// above the segment, because below p_b^2 the carry phi(v, b - 1) is
+// 1 + pi(v) - (b - 1) and k_hard_combine reads it from the pi table.
+// Levels per segment = max(0, B - c).
 template <class XT>
 __global__ void k_hard_plan(const QD *__restrict__ qd, uint32_t Q, const uint64_t *__restrict__ pre_seg,
                             uint64_t total, const uint32_t *__restrict__ P, uint32_t np,
@@ -611,14 +707,17 @@ __global__ void k_hard_plan(const QD *__restrict__ qd, uint32_t Q, const uint64_
     const uint32_t q = find_q(pre_seg, Q, u);
     const QD &d = qd[q];
     const uint64_t seg = u - pre_seg[q];
-    const uint64_t lo = seg * 2 * (1ull << d.lbits);
+    const uint64_t lo = seg * 2 * (1ull << d.lbits), hi = lo + 2 * (1ull << d.lbits);
     uint32_t B;
-    if (lo == 0) {
-        B = d.nb;
-    } else {
+    {
         const XT x = xload<XT>(d);
-        uint64_t v = cpx_isqrt((u128)((x - 1) / (XT)lo));
-        if (v > d.r4) v = d.r4;
+        uint64_t v = d.r4;
+        if (lo) {
+            const uint64_t v1 = cpx_isqrt((u128)((x - 1) / (XT)lo));
+            if (v1 < v) v = v1;
+        }
+        const uint64_t v2 = cpx_isqrt((u128)(hi - 1));
+        if (v2 < v) v = v2;
         uint32_t a = 0, bnd = np;  // count of P[i] <= v
         while (a < bnd) {
             const uint32_t mid = (a + bnd) >> 1;
@@ -631,12 +730,17 @@ __global__ void k_hard_plan(const QD *__restrict__ qd, uint32_t Q, const uint64_
     seg_lv[u] = B > d.c ? B - d.c : 0;
 }
 
-// H += sum over segments of carry(seg, b) * msum(seg, b); carry = sum of the
-// earlier segments' level b-1 counts.  One thread per (query, b).
+// H += sum over segments of carry(seg, b) * msum(seg, b); carry = count of
+// survivors of level b-1 below the segment.  Level b is sieved from the first
+// segment reaching p_b^2; below p_b^2 the survivors of level b-1 are 1 and the
+// primes from p_b on, so the carry starts at 1 + max(0, pi(lo - 1) - (b - 1))
+// from the pi table and then adds the sieved segments' counts.  One thread per
+// (query, b).
 __global__ void k_hard_combine(const QD *__restrict__ qd, uint32_t Q, const uint64_t *__restrict__ pre_comb,
                                uint64_t total, const uint64_t *__restrict__ pre_seg,
                                const uint32_t *__restrict__ seg_B, const uint64_t *__restrict__ seg_off,
                                const uint32_t *__restrict__ cnt, const int32_t *__restrict__ ms, uint64_t cap,
+                               const uint32_t *__restrict__ P, const cpx_pient *__restrict__ T,
                                unsigned long long *__restrict__ acc)
 {
     const uint64_t u = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -644,9 +748,18 @@ __global__ void k_hard_combine(const QD *__restrict__ qd, uint32_t Q, const uint
     if (u < total) {
         const uint32_t q = find_q(pre_comb, Q, u);
         const uint64_t lvl = u - pre_comb[q];
-        const uint32_t b = qd[q].c + 1 + (uint32_t)lvl;
-        const uint64_t s0 = pre_seg[q], s1 = pre_seg[q + 1];
+        const QD &d = qd[q];
+        const uint32_t b = d.c + 1 + (uint32_t)lvl;
+        const uint64_t span = 2ull << d.lbits;
+        const uint64_t p = P[b - 1];
+        const uint64_t first = (p * p) / span;  // first segment with hi > p^2
+        const uint64_t s0 = pre_seg[q] + first, s1 = pre_seg[q + 1];
         uint64_t carry = 0;
+        if (first > 0 && s0 < s1) {
+            const uint64_t lo = first * span;
+            const uint64_t pl = cpx_pi_dev(T, lo - 1);
+            carry = 1 + (pl > b - 1 ? pl - (b - 1) : 0);
+        }
         i128 H = 0;
         for (uint64_t sg = s0; sg < s1; sg++) {
             if (seg_B[sg] < b) break;
@@ -772,6 +885,21 @@ void launch_easy(cpx_ctx *ctx, const Plan &pl)
     note_launch(ctx);
 }
 
+void launch_easy_comp(cpx_ctx *ctx, const Plan &pl)
+{
+    if (!pl.n_ecomp) return;
+    const unsigned grid = (unsigned)std::max<uint64_t>(
+        1, std::min<uint64_t>((pl.n_ecomp + (kThreads / 32) - 1) / (kThreads / 32), (uint64_t)ctx->sm_count * 16));
+    if (pl.wide)
+        k_easy_comp<u128><<<grid, kThreads, 0, ctx->stream>>>(pl.qd, pl.elv, pl.n_elv, pl.n_ecomp, ctx->tab.MU,
+                                                              ctx->tab.T, pl.acc);
+    else
+        k_easy_comp<uint64_t><<<grid, kThreads, 0, ctx->stream>>>(pl.qd, pl.elv, pl.n_elv, pl.n_ecomp, ctx->tab.MU,
+                                                                  ctx->tab.T, pl.acc);
+    CPX_LAUNCH("k_easy_comp");
+    note_launch(ctx);
+}
+
 size_t hard_smem_bytes(uint32_t lbits, uint32_t threads, bool wide)
 {
     return wide ? HardSmem<u128>::bytes(lbits, threads) : HardSmem<uint64_t>::bytes(lbits, threads);
@@ -789,7 +917,7 @@ template <class XT> static void hard_go(cpx_ctx *ctx, const Plan &pl)
     CPX_CUDA(cudaFuncSetAttribute(k_hard<XT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     if (ctx->timing) CPX_CUDA(cudaEventRecord(ctx->ev_hard0, ctx->stream));
     k_hard<XT><<<(unsigned)pl.n_seg, pl.hard_threads, smem, ctx->stream>>>(
-        pl.qd, pl.Q, pl.pre_seg, pl.n_seg, pl.seg_B, pl.seg_off, tb.P, tb.MU, pl.hard_cnt, pl.hard_ms,
+        pl.qd, pl.Q, pl.pre_seg, pl.n_seg, pl.seg_B, pl.seg_off, tb.P, tb.MU, tb.T, pl.hard_cnt, pl.hard_ms,
         pl.hard_entries, pl.acc, pl.lbits_max);
     CPX_LAUNCH("k_hard");
     if (ctx->timing) CPX_CUDA(cudaEventRecord(ctx->ev_hard1, ctx->stream));
@@ -797,7 +925,7 @@ template <class XT> static void hard_go(cpx_ctx *ctx, const Plan &pl)
     if (pl.n_comb) {
         k_hard_combine<<<(unsigned)((pl.n_comb + 255) / 256), 256, 0, ctx->stream>>>(
             pl.qd, pl.Q, pl.pre_comb, pl.n_comb, pl.pre_seg, pl.seg_B, pl.seg_off, pl.hard_cnt, pl.hard_ms,
-            pl.hard_entries, pl.acc);
+            pl.hard_entries, tb.P, tb.T, pl.acc);
         CPX_LAUNCH("k_hard_combine");
         note_launch(ctx);
     }

@@ -14,6 +14,14 @@ struct __align__(16) QD {
     uint64_t nseg;                  // hard-leaf segments over [0, z]
 };
 
+// One level of composite easy leaves of one query: odd m = 2i + 1 with
+// i in [i_lo, i_hi); work units of 1024 indices from i_base (i_lo rounded
+// down to a multiple of 4), numbered from unit0.
+struct __align__(16) EasyLvl {
+    uint32_t q, b, p, pad;
+    uint64_t i_lo, i_hi, i_base, unit0;
+};
+
 // accumulator slots per query (each a signed 128-bit value = 2 words)
 enum { ACC_P2 = 0, ACC_ORD, ACC_TRIV, ACC_EASY, ACC_HARD, ACC_PIY, ACC_PI, ACC_N };
 constexpr int kAccStride = 2 * ACC_N;  // u64 words per query
@@ -38,12 +46,17 @@ struct Plan {
     int32_t *hard_ms = nullptr;
     unsigned long long *acc = nullptr;
     unsigned int *ticket = nullptr;
+    // composite easy leaves
+    const EasyLvl *elv = nullptr;
+    uint32_t n_elv = 0;
+    uint64_t n_ecomp = 0;
 };
 
 void launch_ordinary(cpx_ctx *ctx, const Plan &pl);
 void launch_p2(cpx_ctx *ctx, const Plan &pl);
 void launch_trivial(cpx_ctx *ctx, const Plan &pl);
 void launch_easy(cpx_ctx *ctx, const Plan &pl);
+void launch_easy_comp(cpx_ctx *ctx, const Plan &pl);
 void launch_hard(cpx_ctx *ctx, const Plan &pl);
 void launch_finalize(cpx_ctx *ctx, const Plan &pl, u128 *d_out_pi, bool full);
 size_t hard_smem_bytes(uint32_t lbits, uint32_t threads, bool wide);

@@ -120,12 +120,14 @@ int cpx_trivial_u128(cpx_ctx *ctx, cpx_u128 x, uint64_t y, cpx_u128 *out);
  *                                                         (src/ordinary.cu:33) */
 int cpx_ordinary_u64(cpx_ctx *ctx, uint64_t x, uint64_t y, uint16_t c, int64_t *out);
 int cpx_ordinary_u128(cpx_ctx *ctx, cpx_u128 x, uint64_t y, uint16_t c, cpx_u128 *out);
-/* easy special leaves: (p, q) with iroot4(x) < p <= icbrt(x), q prime,
- * max(p, y/p) < q <= min(y, x/p^2), value pi(x/(pq)) - pi(p) + 2 */
-int cpx_S2_easy_u64(cpx_ctx *ctx, uint64_t x, uint64_t y, int64_t *out);
-int cpx_S2_easy_u128(cpx_ctx *ctx, cpx_u128 x, uint64_t y, cpx_u128 *out);
-/* hard special leaves: p_b <= iroot4(x), b > c, by the segmented phi sieve
- *                                          (src/sieve/S2_hard_host.cu:172) */
+/* easy special leaves: the non-trivial leaves (b > c, m) with
+ * u = x/(p_b m) < p_b^2, whose value -mu(m) phi(u, b-1) is
+ * -mu(m) (pi(u) - b + 2): prime m = q for p_b > iroot4(x) (max(p, y/p) < q <=
+ * min(y, x/p^2)) and every m > x/p_b^3 for p_b <= iroot4(x) */
+int cpx_S2_easy_u64(cpx_ctx *ctx, uint64_t x, uint64_t y, uint16_t c, int64_t *out);
+int cpx_S2_easy_u128(cpx_ctx *ctx, cpx_u128 x, uint64_t y, uint16_t c, cpx_u128 *out);
+/* hard special leaves: p_b <= iroot4(x), b > c, m <= x/p_b^3 (u >= p_b^2),
+ * by the segmented phi sieve               (src/sieve/S2_hard_host.cu:172) */
 int cpx_S2_hard_u64(cpx_ctx *ctx, uint64_t x, uint64_t y, uint16_t c, int64_t *out);
 int cpx_S2_hard_u128(cpx_ctx *ctx, cpx_u128 x, uint64_t y, uint16_t c, cpx_u128 *out);
 /* pi(x) by the term identity; terms may be NULL.  y = 0 picks the default

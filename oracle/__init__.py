@@ -50,10 +50,10 @@ def lib():
         L.orc_phi.argtypes = [U64, ctypes.c_uint32]
         L.orc_phisieve_counts.restype = None
         L.orc_phisieve_counts.argtypes = [ctypes.c_uint32, U64, ctypes.c_void_p]
-        for name in ("orc_P2", "orc_trivial", "orc_easy"):
+        for name in ("orc_P2", "orc_trivial"):
             getattr(L, name).restype = None
             getattr(L, name).argtypes = [U64, U64, U64, ctypes.c_void_p]
-        for name in ("orc_ordinary", "orc_hard"):
+        for name in ("orc_ordinary", "orc_hard", "orc_easy"):
             getattr(L, name).restype = None
             getattr(L, name).argtypes = [U64, U64, U64, ctypes.c_uint32, ctypes.c_void_p]
         L.orc_pi_dr.restype = None
@@ -162,8 +162,8 @@ def ordinary(x, y, c=6):
     return _call128(lib().orc_ordinary, *_split(x), y, c)
 
 
-def easy(x, y):
-    return _call128(lib().orc_easy, *_split(x), y)
+def easy(x, y, c=6):
+    return _call128(lib().orc_easy, *_split(x), y, c)
 
 
 def hard(x, y, c=6):

@@ -19,10 +19,15 @@
  * The reference splits easy + hard differently and its sum is wrong by about
  * 1 ppm (README.md:3,8); this restatement uses the exact split below, shared
  * with the CUDA library:
- *   easy = sum over leaves (p, q), q prime, iroot4(x) < p <= icbrt(x),
- *          max(p, y/p) < q <= min(y, x/p^2) of [pi(x/(pq)) - pi(p) + 2]
- *   hard = - sum_{b = c+1}^{pi(iroot4 x)} sum_{y/p_b < m <= y, lpf(m) > p_b}
- *          mu(m) phi(x/(p_b m), b-1)
+ *   a special leaf (b, m), b > c, y/p_b < m <= y, lpf(m) > p_b, mu(m) != 0,
+ *   contributes -mu(m) phi(x/(p_b m), b-1).  With u = x/(p_b m):
+ *   trivial = leaves with u < p_b (value 1);
+ *   easy    = the other leaves with u < p_b^2, where
+ *             phi(u, b-1) = pi(u) - b + 2: for p_b > iroot4(x) these are
+ *             (p, q) with q prime, max(p, y/p) < q <= min(y, x/p^2); for
+ *             p_b <= iroot4(x) they are the m > x/p_b^3;
+ *   hard    = leaves with u >= p_b^2 (so p_b <= iroot4(x), m <= x/p_b^3),
+ *             answered by the segmented phi sieve.
  * All roots are exact integer floor roots (the reference used doubles,
  * e.g. src/trivial.cu:33-34).
  */
@@ -557,10 +562,36 @@ static i128 term_ordinary(const drctx_t *D, const int8_t *mu, const uint32_t *lp
     return s;
 }
 
-static i128 term_easy(const drctx_t *D)
+static i128 term_easy(const drctx_t *D, const int8_t *mu, const uint32_t *lpf)
 {
     i128 s = 0;
     uint64_t blo = pitab_pi(&D->tab, D->qrtx) + 1, bhi = pitab_pi(&D->tab, D->cbrtx);
+    /* (ii) p_b <= iroot4(x): leaves with x/(p m) < p^2, i.e. m > x/p^3 */
+    const uint64_t c = D->c;
+#pragma omp parallel
+    {
+        i128 ls = 0;
+#pragma omp for schedule(dynamic, 1)
+        for (uint64_t b = c + 1; b < blo; b++) {
+            uint64_t p = D->P[b - 1];
+            u128 xp = D->x / p;
+            u128 x3 = xp / p / p;
+            uint64_t mlo = D->y / p;
+            if (x3 > (u128)mlo) mlo = x3 > (u128)D->y ? D->y : (uint64_t)x3;
+            uint64_t m = mlo + 1;
+            if ((m & 1) == 0) m++;
+            for (; m <= D->y; m += 2) {
+                uint64_t i = (m - 1) / 2;
+                if (mu[i] == 0 || lpf[i] <= p) continue;
+                uint64_t u = (uint64_t)(xp / m);
+                i128 v = (i128)pitab_pi(&D->tab, u) - (i128)b + 2;
+                ls += mu[i] > 0 ? -v : v;
+            }
+        }
+#pragma omp critical
+        s += ls;
+    }
+    /* (i) p_b > iroot4(x): prime q, non-trivial */
 #pragma omp parallel
     {
         i128 ls = 0;
@@ -639,6 +670,10 @@ static i128 term_hard(const drctx_t *D, const int8_t *mu, const uint32_t *lpf)
                     if (lo != 0) {
                         u128 t2 = xp / lo;
                         if (t2 < mhi) mhi = (uint64_t)t2;
+                    }
+                    { /* hard leaves only: x/(p m) >= p^2, i.e. m <= x/p^3 */
+                        u128 t3 = xp / p / p;
+                        if (t3 < mhi) mhi = (uint64_t)t3;
                     }
                     int have_pre = 0;
                     uint64_t m = mlo + 1;
@@ -741,14 +776,20 @@ void orc_ordinary(uint64_t x_lo, uint64_t x_hi, uint64_t y, uint32_t c, uint64_t
     free(lpf);
 }
 
-void orc_easy(uint64_t x_lo, uint64_t x_hi, uint64_t y, uint64_t *out)
+void orc_easy(uint64_t x_lo, uint64_t x_hi, uint64_t y, uint32_t c, uint64_t *out)
 {
     u128 x = mk128(x_lo, x_hi);
+    uint64_t len = y / 2 + 1;
+    int8_t *mu = (int8_t *)malloc(len);
+    uint32_t *lpf = (uint32_t *)malloc(len * 4);
+    orc_mu_lpf(0, 2 * len, mu, lpf);
     drctx_t D;
     uint64_t sx = isqrt128(x);
-    dr_init(&D, x, y, 6, (sx > y ? sx : y) + 2);
-    put128(term_easy(&D), out);
+    dr_init(&D, x, y, c, (sx > y ? sx : y) + 2);
+    put128(term_easy(&D, mu, lpf), out);
     dr_free(&D);
+    free(mu);
+    free(lpf);
 }
 
 void orc_hard(uint64_t x_lo, uint64_t x_hi, uint64_t y, uint32_t c, uint64_t *out)
@@ -781,7 +822,7 @@ void orc_pi_dr(uint64_t x_lo, uint64_t x_hi, uint64_t y, uint32_t c, int nthread
     i128 p2 = term_P2(&D);
     i128 s0 = term_ordinary(&D, mu, lpf);
     i128 tr = term_trivial(&D);
-    i128 ez = term_easy(&D);
+    i128 ez = term_easy(&D, mu, lpf);
     i128 hd = term_hard(&D, mu, lpf);
     i128 piy = (i128)pitab_pi(&D.tab, y);
     i128 pix = s0 + tr + ez + hd + piy - 1 - p2;

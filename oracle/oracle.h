@@ -53,7 +53,7 @@ void orc_phisieve_counts(uint32_t a, uint64_t nbits, uint32_t *out);
 void orc_P2(uint64_t x_lo, uint64_t x_hi, uint64_t y, uint64_t *out);
 void orc_trivial(uint64_t x_lo, uint64_t x_hi, uint64_t y, uint64_t *out);
 void orc_ordinary(uint64_t x_lo, uint64_t x_hi, uint64_t y, uint32_t c, uint64_t *out);
-void orc_easy(uint64_t x_lo, uint64_t x_hi, uint64_t y, uint64_t *out);
+void orc_easy(uint64_t x_lo, uint64_t x_hi, uint64_t y, uint32_t c, uint64_t *out);
 void orc_hard(uint64_t x_lo, uint64_t x_hi, uint64_t y, uint32_t c, uint64_t *out);
 
 /* Full pi(x) through the term identity

@@ -33,6 +33,7 @@ def test_other_c(ctx, cpx, orc, c):
     x, y = 10**11, 10**4 * 5
     assert cpx.Ordinary(x, y, c, ctx=ctx) == orc.ordinary(x, y, c)
     assert cpx.S2hard(x, y, c, ctx=ctx) == orc.hard(x, y, c)
+    assert cpx.S2_easy(x, y, c, ctx=ctx) == orc.easy(x, y, c)
     assert cpx.pi_deleglise_rivat(x, y, c, ctx=ctx) == 4118054813
 
 
