@@ -102,6 +102,9 @@ int cpx_destroy(cpx_ctx *ctx)
         ctx->b_win2.release();
         for (auto &b : ctx->b_work) b.release();
         ctx->b_flush.release();
+        ctx->b_jobs.release();
+        ctx->b_jobctl.release();
+        ctx->b_snap.release();
         if (ctx->ev_hard0) cudaEventDestroy(ctx->ev_hard0);
         if (ctx->ev_hard1) cudaEventDestroy(ctx->ev_hard1);
         for (cudaEvent_t ev : {ctx->ev_b0, ctx->ev_b1, ctx->ev_t0, ctx->ev_t1})

@@ -88,14 +88,40 @@ static uint64_t segments_at_level(u128 x, uint64_t span, uint64_t p, uint64_t ns
     return hi >= first ? (uint64_t)(hi - first + 1) : 0;
 }
 
-static uint32_t pick_lbits(cpx_ctx *ctx, uint64_t z, uint32_t threads, uint32_t forced)
+// Hard-leaf segment sizes for a batch.  A query never gets a segment longer
+// than needed to cover [0, z]; below the context default the sizes of the
+// largest queries shrink (one cap for all) until the whole batch has about
+// four segments per SM, so one large query still fills the GPU while a big
+// batch keeps long segments (fewer segment-levels to sieve).
+static void choose_lbits(cpx_ctx *ctx, std::vector<QD> &qd, uint32_t c, uint32_t threads, uint32_t forced)
 {
     const uint32_t minb = (threads >= 512) ? 16 : (threads >= 256 ? 15 : 14);
-    if (forced) return std::max(minb, std::min<uint32_t>(forced, 20));
-    // segment count at least ~one wave when z is small; cap at the context default
-    uint32_t lb = ctx->hard_log2_bits;
-    while (lb > minb && ((z + 1) >> (lb + 1)) < (uint64_t)ctx->sm_count * 2) lb--;
-    return std::max(minb, lb);
+    std::vector<uint32_t> nat(qd.size(), 0);
+    for (size_t i = 0; i < qd.size(); i++) {
+        const QD &d = qd[i];
+        if (d.direct || d.nb <= c) continue;
+        if (forced) {
+            nat[i] = std::max(minb, std::min<uint32_t>(forced, 20));
+            continue;
+        }
+        uint32_t lb = minb;
+        while (lb < ctx->hard_log2_bits && (2ull << lb) < d.z + 1) lb++;
+        nat[i] = lb;
+    }
+    uint32_t cap = forced ? 20 : ctx->hard_log2_bits;
+    const uint64_t target = (uint64_t)ctx->sm_count * 4;
+    for (;;) {
+        uint64_t segs = 0;
+        for (size_t i = 0; i < qd.size(); i++)
+            if (nat[i]) {
+                const uint32_t lb = std::min(nat[i], cap);
+                segs += (qd[i].z + 1 + (2ull << lb) - 1) / (2ull << lb);
+            }
+        if (forced || segs >= target || cap <= minb) break;
+        cap--;
+    }
+    for (size_t i = 0; i < qd.size(); i++)
+        if (nat[i]) qd[i].lbits = std::min(nat[i], cap);
 }
 
 void run_batch(cpx_ctx *ctx, const BatchReq &rq)
@@ -170,6 +196,12 @@ void run_batch(cpx_ctx *ctx, const BatchReq &rq)
     if (mask & TERM_ORD) ensure_wheel(ctx, c);
     const std::vector<uint32_t> &hP = host_primes(ctx);
 
+    if (mask & TERM_HARD) {
+        for (QD &d : qd)
+            if (!d.direct) d.nb = (uint32_t)host_pi(hP, d.r4);
+        choose_lbits(ctx, qd, c, threads, rq.lbits);
+    }
+
     // ---- units per kernel family
     std::vector<uint64_t> pre(6 * (size_t)(Q + 1), 0);
     uint64_t *p_ord = pre.data(), *p_p2 = p_ord + (Q + 1), *p_triv = p_p2 + (Q + 1), *p_easy = p_triv + (Q + 1),
@@ -215,9 +247,7 @@ void run_batch(cpx_ctx *ctx, const BatchReq &rq)
                 }
             }
             if (mask & TERM_HARD) {
-                d.nb = (uint32_t)host_pi(hP, d.r4);
                 if (d.nb > c) {
-                    d.lbits = pick_lbits(ctx, d.z, threads, rq.lbits);
                     lbits_max = std::max(lbits_max, d.lbits);
                     const uint64_t span = 2ull << d.lbits;
                     d.nseg = (d.z + 1 + span - 1) / span;
@@ -279,6 +309,14 @@ void run_batch(cpx_ctx *ctx, const BatchReq &rq)
         pl.seg_off = ctx->b_work[3].as<uint64_t>(pl.n_seg + 1);
         pl.hard_cnt = ctx->b_work[4].as<uint32_t>(hard_entries + 1);
         pl.hard_ms = ctx->b_work[5].as<int32_t>(hard_entries + 1);
+        // snapshot pool for heavy (segment, level) leaf sets: at most 8192 slots and 512 MiB
+        const size_t stride = hard_snapshot_stride(lbits_max);
+        pl.max_jobs = (uint32_t)std::min<size_t>(8192, (size_t(512) << 20) / stride);
+        pl.jobs = ctx->b_jobs.as<HardJob>(pl.max_jobs);
+        uint64_t *ctl = ctx->b_jobctl.as<uint64_t>(4);
+        pl.njobs = reinterpret_cast<unsigned int *>(ctl);
+        pl.job_units = ctl + 1;
+        pl.snap = static_cast<unsigned char *>(ctx->b_snap.get(pl.max_jobs * stride));
     }
     u128 *d_out = ctx->b_work[6].as<u128>(Q);
 

@@ -1,0 +1,683 @@
+// hard.cu -- hard special leaves: the segmented phi sieve.
+//
+// Restates the reference's hard-leaf sieve (S2hardHost / S2ctl,
+// src/sieve/S2_hard_host.cu:49-191, src/sieve/S2_hard_device.cu:12-382) with
+// this library's exact leaf split: a leaf (b, m) is hard when
+// u = x/(p_b m) >= p_b^2, i.e. p_b <= iroot4(x) and m <= x/p_b^3; it
+// contributes -mu(m) phi(u, b-1), which the sieve answers from the bitmap of
+// the segment holding u plus the survivors of level b-1 below the segment.
+//
+// One CTA owns one segment of 2^lbits odd numbers n = lo + 2i + 1 as a bitmap
+// in shared memory, with one 8-bit survivor counter per 16-byte chunk
+// (128 numbers).  For each level b it (1) records the segment's survivor count
+// at level b-1, (2) if the segment holds leaves of p_b, scans the counters into
+// per-thread prefixes and answers each leaf as
+//     thread prefix + counters of the owner's earlier chunks + popcounts in the chunk,
+// (3) crosses off p_b, counting the bits it clears and keeping the chunk
+// counters current.  Carries between segments are added by k_hard_combine.
+//
+// Bitmap layout: thread t owns chunks [CPT t, CPT (t+1)); chunk c is stored at
+// c ^ ((c >> log2 CPT) & 7) so the owners' 128-bit accesses are free of bank
+// conflicts.  Counters are indexed by the unswizzled chunk.
+#include <algorithm>
+
+#include "kern_common.cuh"
+
+namespace cpx {
+
+__device__ __forceinline__ uint32_t swz(uint32_t c, int s) { return s ? (c ^ ((c >> s) & 7u)) : c; }
+
+// bits k < 32 of a word whose first number is = r (mod p) that are multiples of p
+__device__ __forceinline__ uint32_t mult_mask(uint32_t r, uint32_t p, uint32_t Mp)
+{
+    const uint32_t k0 = (r == 0) ? 0u : ((r & 1u) ? (p - r) >> 1 : p - (r >> 1));
+    return k0 < 32 ? (Mp << k0) : 0u;
+}
+__device__ __forceinline__ uint32_t every_pth_bit(uint32_t p)
+{
+    uint32_t m = 0;
+    for (uint32_t k = 0; k < 32; k += p) m |= 1u << k;
+    return m;
+}
+
+// sum of the n 8-bit counters starting at c8 (c8 4-byte aligned when n >= 4)
+__device__ __forceinline__ uint32_t counter_sum(const uint8_t *c8, uint32_t n)
+{
+    uint32_t s = 0;
+    const uint32_t *cw = reinterpret_cast<const uint32_t *>(c8);
+    uint32_t k = 0;
+    for (; k < (n >> 2); k++) s = __dp4a(cw[k], 0x01010101u, s);
+    const uint32_t rem = n & 3;
+    if (rem) {
+        if (reinterpret_cast<uintptr_t>(c8) & 3) {
+            for (uint32_t i = 0; i < rem; i++) s += c8[4 * k + i];
+        } else {
+            s = __dp4a(cw[k] & ((1u << (8 * rem)) - 1u), 0x01010101u, s);
+        }
+    }
+    return s;
+}
+
+// A level whose candidate range in a segment holds at least kOffloadMin odd m
+// (8 per pi-table entry for prime-only levels) is answered by k_hard_leaves.
+constexpr uint64_t kOffloadMin = 4096;
+constexpr uint64_t kJobWords = 256;   // pi-table entries per k_hard_leaves unit (prime levels)
+constexpr uint64_t kJobGroups = 256;  // 4-m groups per k_hard_leaves unit (other levels)
+
+// bytes of one snapshot slot: 16-byte bitmap chunks + 32-bit survivor prefixes
+__host__ __device__ __forceinline__ size_t snap_stride(uint32_t lbits_max)
+{
+    const size_t nc = (size_t(1) << lbits_max) >> 7;
+    return (nc * 20 + 255) & ~size_t(255);
+}
+
+template <class XT> struct HardSmem {
+    static __host__ __device__ size_t bytes(uint32_t lbits, uint32_t threads)
+    {
+        const size_t L = size_t(1) << lbits;
+        size_t o = L / 8;                        // bitmap
+        o += ((L / 128) + 15) & ~size_t(15);     // chunk counters
+        o += threads * 4;                        // toff
+        o += 32 * 4;                             // wsum
+        o += threads * (4 * 5);                  // s_p, s_mlo, s_mhi, s_i0, s_r0
+        o = (o + 15) & ~size_t(15);
+        o += threads * sizeof(XT);               // s_xp
+        o += 64;                                 // s_clr[2], s_ms
+        o = (o + 15) & ~size_t(15);
+        o += 32 * sizeof(i128);                  // reductions
+        return o;
+    }
+};
+
+template <class XT>
+__global__ void __launch_bounds__(512) k_hard(const QD *__restrict__ qd, uint32_t Q,
+                                              const uint64_t *__restrict__ pre_seg, uint64_t total,
+                                              const uint32_t *__restrict__ seg_B,
+                                              const uint64_t *__restrict__ seg_off,
+                                              const uint32_t *__restrict__ P, const int32_t *__restrict__ MU,
+                                              const cpx_pient *__restrict__ Tpi,
+                                              uint32_t *__restrict__ out_cnt, int32_t *__restrict__ out_ms,
+                                              uint64_t cap, unsigned long long *__restrict__ acc,
+                                              uint32_t lbits_max, HardJob *__restrict__ jobs,
+                                              unsigned int *__restrict__ njobs, unsigned char *__restrict__ snap,
+                                              uint32_t max_jobs)
+{
+    extern __shared__ uint4 smem4[];
+    const uint64_t unit = blockIdx.x;
+    if (unit >= total) return;
+    const uint32_t B = seg_B[unit];
+    const uint32_t q = find_q(pre_seg, Q, unit);
+    const QD &d = qd[q];
+    const uint32_t c = d.c;
+    if (B <= c) return;  // uniform over the CTA
+    const uint32_t T = blockDim.x, tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const uint32_t L = 1u << d.lbits;
+    const uint32_t NC = L >> 7;    // chunks
+    const uint32_t CPT = NC / T;   // chunks per thread (>= 1)
+    const int s = __ffs(CPT) - 1;  // log2 CPT
+    const uint64_t seg = unit - pre_seg[q];
+    const uint64_t lo = seg * 2 * (uint64_t)L, hi = lo + 2 * (uint64_t)L;
+    const uint64_t off = seg_off[unit];
+    if (off + (B - c) > cap) return;  // the host sized the ragged outputs exactly; never write past them
+    const XT x = xload<XT>(d);
+    const uint64_t y = d.y;
+
+    // carve the shared block (sized for lbits_max)
+    unsigned char *sp = reinterpret_cast<unsigned char *>(smem4);
+    const size_t Lmax = size_t(1) << lbits_max;
+    uint32_t *bm = reinterpret_cast<uint32_t *>(sp);
+    size_t o = Lmax / 8;
+    uint8_t *cnt8 = reinterpret_cast<uint8_t *>(sp + o);
+    o += ((Lmax / 128) + 15) & ~size_t(15);
+    uint32_t *toff = reinterpret_cast<uint32_t *>(sp + o);
+    o += T * 4;
+    uint32_t *wsum = reinterpret_cast<uint32_t *>(sp + o);
+    o += 32 * 4;
+    uint32_t *s_p = reinterpret_cast<uint32_t *>(sp + o);
+    uint32_t *s_mlo = s_p + T, *s_mhi = s_mlo + T, *s_i0 = s_mhi + T, *s_r0 = s_i0 + T;
+    o += T * 20;
+    o = (o + 15) & ~size_t(15);
+    XT *s_xp = reinterpret_cast<XT *>(sp + o);
+    o += T * sizeof(XT);
+    int *s_clr = reinterpret_cast<int *>(sp + o);
+    int *s_ms = s_clr + 2;
+    unsigned int *s_job = reinterpret_cast<unsigned int *>(s_clr + 3);
+    o += 64;
+    o = (o + 15) & ~size_t(15);
+    i128 *s_red = reinterpret_cast<i128 *>(sp + o);
+
+    const uint32_t c0 = CPT * tid;  // first owned chunk
+    const uint32_t w0 = 4 * c0;     // first owned word
+    // ---- pre-sieve with p_2 .. p_c; chunk counters
+    uint32_t cnt0 = 0;
+    {
+        uint32_t pr[8], rr[8], st[8], Mp[8];
+        const uint32_t np = c - 1;
+#pragma unroll
+        for (uint32_t i = 0; i < 8; i++) {
+            if (i < np) {
+                pr[i] = P[i + 1];
+                rr[i] = (uint32_t)(((lo + 1) % pr[i] + (64ull * w0) % pr[i]) % pr[i]);
+                st[i] = 64u % pr[i];
+                Mp[i] = every_pth_bit(pr[i]);
+            }
+        }
+        for (uint32_t j = 0; j < CPT; j++) {
+            uint32_t wv[4];
+#pragma unroll
+            for (int k = 0; k < 4; k++) {
+                uint32_t m = 0;
+#pragma unroll
+                for (uint32_t i = 0; i < 8; i++) {
+                    if (i < np) {
+                        m |= mult_mask(rr[i], pr[i], Mp[i]);
+                        rr[i] += st[i];
+                        if (rr[i] >= pr[i]) rr[i] -= pr[i];
+                    }
+                }
+                wv[k] = ~m;
+            }
+            const uint32_t cc = __popc(wv[0]) + __popc(wv[1]) + __popc(wv[2]) + __popc(wv[3]);
+            cnt0 += cc;
+            cnt8[c0 + j] = (uint8_t)cc;
+            reinterpret_cast<uint4 *>(bm)[swz(c0 + j, s)] = make_uint4(wv[0], wv[1], wv[2], wv[3]);
+        }
+    }
+    if (tid == 0) {
+        s_clr[0] = s_clr[1] = 0;
+        *s_ms = 0;
+    }
+    uint32_t tot = 0;  // thread 0: survivors of the segment at the current level
+    {
+        uint32_t v = cnt0;
+#pragma unroll
+        for (int dd = 16; dd > 0; dd >>= 1) v += __shfl_down_sync(FULL, v, dd);
+        if (lane == 0) wsum[warp] = v;
+        __syncthreads();
+        if (tid == 0)
+            for (uint32_t k = 0; k < T / 32; k++) tot += wsum[k];
+        __syncthreads();
+    }
+
+    // survivors of the segment with n <= uu (uu in [lo, hi))
+    auto seg_count = [&](uint64_t uu) -> uint32_t {
+        const uint32_t kk = (uint32_t)((uu - lo + 1) >> 1);  // bits [0, kk)
+        if (!kk) return 0u;
+        const uint32_t jb = kk - 1, w = jb >> 5, ch = w >> 2, ow = ch >> s;
+        uint32_t cv = toff[ow];
+        for (uint32_t i = 0; i < (ow >> 5); i++) cv += wsum[i];
+        cv += counter_sum(cnt8 + (size_t)ow * CPT, ch - ow * CPT);
+        const uint4 v4 = reinterpret_cast<const uint4 *>(bm)[swz(ch, s)];
+        const uint32_t wi = w & 3, msk = (2u << (jb & 31)) - 1u;
+        if (wi == 0) cv += __popc(v4.x & msk);
+        else if (wi == 1) cv += __popc(v4.x) + __popc(v4.y & msk);
+        else if (wi == 2) cv += __popc(v4.x) + __popc(v4.y) + __popc(v4.z & msk);
+        else cv += __popc(v4.x) + __popc(v4.y) + __popc(v4.z) + __popc(v4.w & msk);
+        return cv;
+    };
+
+    int64_t S = 0;
+    for (uint32_t bb = c + 1; bb <= B; bb += T) {
+        const uint32_t nbat = min(T, B - bb + 1);
+        if (tid < nbat) {
+            const uint32_t b = bb + tid;
+            const uint64_t p = P[b - 1];
+            const XT xp = x / (XT)p;
+            uint64_t mlo = y / p;
+            const XT t1 = xp / (XT)hi;
+            if (t1 > (XT)mlo) mlo = (uint64_t)t1;
+            uint64_t mhi = y;
+            if (lo) {
+                const XT t2 = xp / (XT)lo;
+                if (t2 < (XT)mhi) mhi = (uint64_t)t2;
+            }
+            {
+                // hard leaves only: x/(p m) >= p^2, i.e. m <= x/p^3
+                const XT t3 = xp / (XT)(p * p);
+                if (t3 < (XT)mhi) mhi = (uint64_t)t3;
+            }
+            if (mhi < mlo) mhi = mlo;
+            s_p[tid] = (uint32_t)p;
+            s_xp[tid] = xp;
+            s_mlo[tid] = (uint32_t)mlo;
+            s_mhi[tid] = (uint32_t)mhi;
+            const uint64_t r0 = (lo + 1) % p;
+            s_r0[tid] = (uint32_t)r0;
+            uint64_t m = lo + 1 + (r0 ? p - r0 : 0);
+            if ((m & 1) == 0) m += p;
+            s_i0[tid] = (m < hi) ? (uint32_t)((m - lo - 1) >> 1) : 0xFFFFFFFFu;
+        }
+        __syncthreads();
+        for (uint32_t k = 0; k < nbat; k++) {
+            const uint32_t b = bb + k;
+            const uint32_t p = s_p[k];
+            const uint32_t mlo = s_mlo[k], mhi = s_mhi[k];
+            const uint64_t slot = off + (b - c - 1);
+            if (tid == 0) {
+                tot -= (uint32_t)s_clr[(b - 1) & 1];
+                s_clr[(b - 1) & 1] = 0;
+                out_cnt[slot] = tot;
+            }
+            if (mhi > mlo) {
+                // per-thread prefixes from the chunk counters
+                const uint32_t run = counter_sum(cnt8 + c0, CPT);
+                uint32_t inc = run;
+#pragma unroll
+                for (int oo = 1; oo < 32; oo <<= 1) {
+                    const uint32_t t = __shfl_up_sync(FULL, inc, oo);
+                    if (lane >= (uint32_t)oo) inc += t;
+                }
+                toff[tid] = inc - run;
+                if (lane == 31) wsum[warp] = inc;
+                __syncthreads();
+                const XT xp = s_xp[k];
+                int32_t msl = 0;
+                // a large candidate range goes to k_hard_leaves with a snapshot of the segment
+                const bool prime_lvl = (uint64_t)p * p > y;
+                const uint64_t qa = mlo > p ? mlo : p;
+                uint64_t work = 0;
+                if (prime_lvl) work = (mhi > qa) ? 8 * ((((uint64_t)mhi - 1) >> 7) - (qa >> 7) + 1) : 0;
+                else work = ((((uint64_t)mhi - 1) >> 1) - (((uint64_t)mlo + 1) >> 1) + 1);
+                bool offloaded = false;
+                if (max_jobs && work >= kOffloadMin) {
+                    if (tid == 0) {
+                        const unsigned int j = atomicAdd(njobs, 1u);
+                        *s_job = j < max_jobs ? j : 0xFFFFFFFFu;
+                    }
+                    __syncthreads();
+                    const unsigned int job = *s_job;
+                    if (job != 0xFFFFFFFFu) {
+                        offloaded = true;
+                        const size_t stride = snap_stride(lbits_max);
+                        uint4 *sb = reinterpret_cast<uint4 *>(snap + (size_t)job * stride);
+                        uint32_t *spre = reinterpret_cast<uint32_t *>(sb + (Lmax >> 7));
+                        uint32_t pre = toff[tid];
+                        for (uint32_t i = 0; i < warp; i++) pre += wsum[i];
+                        for (uint32_t j = 0; j < CPT; j++) {
+                            sb[c0 + j] = reinterpret_cast<const uint4 *>(bm)[swz(c0 + j, s)];
+                            spre[c0 + j] = pre;
+                            pre += cnt8[c0 + j];
+                        }
+                        if (tid == 0) {
+                            HardJob J;
+                            J.q = q;
+                            J.b = b;
+                            J.p = p;
+                            J.kind = prime_lvl ? 1u : 0u;
+                            J.mlo = prime_lvl ? qa : mlo;
+                            J.mhi = mhi;
+                            J.lo = lo;
+                            J.slot = slot;
+                            J.nunits = prime_lvl ? (work / 8 + kJobWords - 1) / kJobWords
+                                                 : (((((uint64_t)mhi - 1) >> 1) >> 2) -
+                                                    ((((uint64_t)mlo + 1) >> 1) >> 2) + kJobGroups) /
+                                                       kJobGroups;
+                            J.unit0 = 0;
+                            J.xp = (u128)xp;
+                            jobs[job] = J;
+                        }
+                    }
+                }
+                if (offloaded) {
+                    // the leaves of this level are counted by k_hard_leaves
+                } else if (prime_lvl) {
+                    // m must be a prime q > p: walk the pi-table bitmap of (max(mlo, p), mhi]
+                    if (mhi > qa) {
+                        const uint64_t w0q = qa >> 7, w1q = ((uint64_t)mhi - 1) >> 7;
+                        for (uint64_t wq = w0q + tid; wq <= w1q; wq += T) {
+                            const ulonglong2 e = __ldg(reinterpret_cast<const ulonglong2 *>(Tpi) + wq);
+                            uint64_t qb = e.x & range_mask(wq, qa, mhi);
+                            while (qb) {
+                                const int j = __ffsll((long long)qb) - 1;
+                                qb &= qb - 1;
+                                const uint64_t m = 128 * wq + 2 * j + 1;
+                                S += seg_count((uint64_t)(xp / (XT)m));  // mu(q) = -1
+                                msl += 1;
+                            }
+                        }
+                    }
+                } else {
+                    // any squarefree m with lpf(m) > p: 16-byte loads of packed mu*lpf
+                    const uint64_t i_lo = ((uint64_t)mlo + 1) >> 1, i_hi = ((uint64_t)mhi - 1) >> 1;  // m = 2i + 1
+                    for (uint64_t g = (i_lo >> 2) + tid; g <= (i_hi >> 2); g += T) {
+                        const int4 v4 = __ldg(reinterpret_cast<const int4 *>(MU) + g);
+                        const int32_t vals[4] = {v4.x, v4.y, v4.z, v4.w};
+#pragma unroll
+                        for (int kq = 0; kq < 4; kq++) {
+                            const uint64_t i = 4 * g + kq;
+                            const int32_t v = vals[kq];
+                            if (i < i_lo || i > i_hi || v == 0) continue;
+                            if ((uint32_t)(v > 0 ? v : -v) <= p) continue;
+                            const uint32_t cv = seg_count((uint64_t)(xp / (XT)(2 * i + 1)));
+                            if (v > 0) {
+                                S -= cv;
+                                msl -= 1;
+                            } else {
+                                S += cv;
+                                msl += 1;
+                            }
+                        }
+                    }
+                }
+#pragma unroll
+                for (int dd = 16; dd > 0; dd >>= 1) msl += __shfl_down_sync(FULL, msl, dd);
+                if (lane == 0 && msl) atomicAdd(s_ms, msl);
+                __syncthreads();
+                if (tid == 0) {
+                    out_ms[slot] = *s_ms;
+                    *s_ms = 0;
+                }
+            } else if (tid == 0) {
+                out_ms[slot] = 0;
+            }
+            // cross off p_b, counting bits that were still set and keeping the counters current
+            uint32_t cleared = 0;
+            if (p < 64) {
+                const uint32_t Mp = every_pth_bit(p);  // p < 32 has several multiples per word
+                const uint32_t st = 64u % p;
+                uint32_t r = (s_r0[k] + (64u * w0) % p) % p;
+                for (uint32_t j = 0; j < CPT; j++) {
+                    uint4 v = reinterpret_cast<const uint4 *>(bm)[swz(c0 + j, s)];
+                    uint32_t a4[4] = {v.x, v.y, v.z, v.w};
+                    uint32_t cj = 0;
+#pragma unroll
+                    for (int kk = 0; kk < 4; kk++) {
+                        const uint32_t mk = mult_mask(r, p, Mp);
+                        cj += __popc(a4[kk] & mk);
+                        a4[kk] &= ~mk;
+                        r += st;
+                        if (r >= p) r -= p;
+                    }
+                    if (cj) {
+                        cnt8[c0 + j] = (uint8_t)(cnt8[c0 + j] - cj);
+                        reinterpret_cast<uint4 *>(bm)[swz(c0 + j, s)] = make_uint4(a4[0], a4[1], a4[2], a4[3]);
+                    }
+                    cleared += cj;
+                }
+            } else {
+                const uint32_t i0 = s_i0[k];
+                if (i0 != 0xFFFFFFFFu) {
+                    for (uint64_t i = (uint64_t)i0 + (uint64_t)tid * p; i < L; i += (uint64_t)T * p) {
+                        const uint32_t w = (uint32_t)(i >> 5), bit = 1u << (i & 31);
+                        const uint32_t ch = w >> 2;
+                        const uint32_t pw = (swz(ch, s) << 2) | (w & 3);
+                        const uint32_t old = atomicAnd(&bm[pw], ~bit);
+                        if (old & bit) {
+                            cleared++;
+                            atomicSub(reinterpret_cast<unsigned int *>(cnt8) + (ch >> 2), 1u << (8 * (ch & 3)));
+                        }
+                    }
+                }
+            }
+#pragma unroll
+            for (int dd = 16; dd > 0; dd >>= 1) cleared += __shfl_down_sync(FULL, cleared, dd);
+            if (lane == 0 && cleared) atomicAdd(&s_clr[b & 1], (int)cleared);
+            __syncthreads();
+        }
+    }
+    const i128 Sb = cpx_block_sum_i128((i128)S, s_red);
+    if (tid == 0) acc_add(acc, q, ACC_HARD, Sb);
+}
+
+// Numbers the offloaded jobs' work units (exclusive scan of nunits in job
+// order); one CTA of 1024 threads.
+__global__ void __launch_bounds__(1024) k_hard_job_scan(HardJob *__restrict__ jobs, const unsigned int *njobs,
+                                                        uint32_t max_jobs, uint64_t *__restrict__ total_units)
+{
+    __shared__ uint64_t wsum[32];
+    const uint32_t n = min(*njobs, max_jobs);
+    const uint32_t t = threadIdx.x, per = (n + 1023) / 1024;
+    const uint32_t a = min(n, t * per), b = min(n, a + per);
+    uint64_t s = 0;
+    for (uint32_t i = a; i < b; i++) s += jobs[i].nunits;
+    uint64_t inc = s;
+    const uint32_t lane = t & 31, w = t >> 5;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const uint64_t v = __shfl_up_sync(FULL, inc, o);
+        if (lane >= (uint32_t)o) inc += v;
+    }
+    if (lane == 31) wsum[w] = inc;
+    __syncthreads();
+    uint64_t run = inc - s;
+    for (uint32_t i = 0; i < w; i++) run += wsum[i];
+    for (uint32_t i = a; i < b; i++) {
+        jobs[i].unit0 = run;
+        run += jobs[i].nunits;
+    }
+    if (t == 1023) *total_units = run;
+}
+
+// Leaves of the offloaded (segment, level) sets.  A warp takes one unit: 256
+// pi-table entries of prime m (prime-only levels) or 256 groups of 4 odd m
+// read as packed mu*lpf (other levels).  Each leaf's survivor count is the
+// snapshot's chunk prefix plus popcounts inside the 16-byte chunk; the sums go
+// to the query's hard-leaf accumulator and Sum(-mu) to the level's slot.
+template <class XT>
+__global__ void __launch_bounds__(kThreads) k_hard_leaves(const HardJob *__restrict__ jobs,
+                                                          const unsigned int *njobs, uint32_t max_jobs,
+                                                          const uint64_t *total_units,
+                                                          const unsigned char *__restrict__ snap,
+                                                          uint32_t lbits_max, const int32_t *__restrict__ MU,
+                                                          const cpx_pient *__restrict__ Tpi,
+                                                          int32_t *__restrict__ out_ms,
+                                                          unsigned long long *__restrict__ acc)
+{
+    const uint32_t n = min(*njobs, max_jobs);
+    const uint64_t total = *total_units;
+    const uint32_t lane = threadIdx.x & 31;
+    const uint64_t gw = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const uint64_t nw = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+    const size_t stride = snap_stride(lbits_max);
+    const size_t ncmax = (size_t(1) << lbits_max) >> 7;
+    for (uint64_t unit = gw; unit < total; unit += nw) {
+        uint32_t lo_j = 0, hi_j = n;  // jobs[lo_j].unit0 <= unit < jobs[hi_j].unit0
+        while (hi_j - lo_j > 1) {
+            const uint32_t mid = (lo_j + hi_j) >> 1;
+            if (jobs[mid].unit0 <= unit) lo_j = mid;
+            else hi_j = mid;
+        }
+        const HardJob &J = jobs[lo_j];
+        const uint64_t lu = unit - J.unit0;
+        const uint4 *sb = reinterpret_cast<const uint4 *>(snap + (size_t)lo_j * stride);
+        const uint32_t *spre = reinterpret_cast<const uint32_t *>(sb + ncmax);
+        const XT xp = (XT)J.xp;
+        const uint64_t lo = J.lo;
+        auto count = [&](uint64_t uu) -> uint32_t {
+            const uint32_t kk = (uint32_t)((uu - lo + 1) >> 1);
+            if (!kk) return 0u;
+            const uint32_t jb = kk - 1, w = jb >> 5, ch = w >> 2;
+            uint32_t cv = __ldg(spre + ch);
+            const uint4 v4 = __ldg(sb + ch);
+            const uint32_t wi = w & 3, msk = (2u << (jb & 31)) - 1u;
+            if (wi == 0) cv += __popc(v4.x & msk);
+            else if (wi == 1) cv += __popc(v4.x) + __popc(v4.y & msk);
+            else if (wi == 2) cv += __popc(v4.x) + __popc(v4.y) + __popc(v4.z & msk);
+            else cv += __popc(v4.x) + __popc(v4.y) + __popc(v4.z) + __popc(v4.w & msk);
+            return cv;
+        };
+        int64_t S = 0;
+        int32_t ms = 0;
+        if (J.kind == 1) {
+            const uint64_t qa = J.mlo, mhi = J.mhi;
+            const uint64_t w0 = (qa >> 7) + lu * kJobWords, wl = (mhi - 1) >> 7;
+            for (uint64_t k = 0; k < kJobWords / 32; k++) {
+                const uint64_t wq = w0 + 32 * k + lane;
+                if (wq > wl) break;
+                const ulonglong2 e = __ldg(reinterpret_cast<const ulonglong2 *>(Tpi) + wq);
+                uint64_t qb = e.x & range_mask(wq, qa, mhi);
+                while (qb) {
+                    const int j = __ffsll((long long)qb) - 1;
+                    qb &= qb - 1;
+                    S += count((uint64_t)(xp / (XT)(128 * wq + 2 * j + 1)));  // mu(q) = -1
+                    ms += 1;
+                }
+            }
+        } else {
+            const uint64_t i_lo = (J.mlo + 1) >> 1, i_hi = (J.mhi - 1) >> 1;
+            const uint64_t g0 = (i_lo >> 2) + lu * kJobGroups, gl = i_hi >> 2;
+            const uint32_t p = J.p;
+            for (uint64_t k = 0; k < kJobGroups / 32; k++) {
+                const uint64_t g = g0 + 32 * k + lane;
+                if (g > gl) break;
+                const int4 v4 = __ldg(reinterpret_cast<const int4 *>(MU) + g);
+                const int32_t vals[4] = {v4.x, v4.y, v4.z, v4.w};
+#pragma unroll
+                for (int kq = 0; kq < 4; kq++) {
+                    const uint64_t i = 4 * g + kq;
+                    const int32_t v = vals[kq];
+                    if (i < i_lo || i > i_hi || v == 0) continue;
+                    if ((uint32_t)(v > 0 ? v : -v) <= p) continue;
+                    const uint32_t cv = count((uint64_t)(xp / (XT)(2 * i + 1)));
+                    if (v > 0) {
+                        S -= cv;
+                        ms -= 1;
+                    } else {
+                        S += cv;
+                        ms += 1;
+                    }
+                }
+            }
+        }
+        const i128 Sw = cpx_warp_sum_i128((i128)S);
+#pragma unroll
+        for (int dd = 16; dd > 0; dd >>= 1) ms += __shfl_down_sync(FULL, ms, dd);
+        if (lane == 0) {
+            if (ms) atomicAdd(out_ms + J.slot, ms);
+            acc_add(acc, J.q, ACC_HARD, Sw);
+        }
+    }
+}
+
+// B(seg) = pi(min(r4, isqrt((x - 1) / lo), isqrt(hi - 1))): the levels b a
+// segment sieves.  p_b^2 * lo < x bounds the levels whose leaves can reach
+// the segment or a later one; p_b^2 < hi skips the levels whose leaves all lie
+// above the segment, because below p_b^2 the carry phi(v, b - 1) is
+// 1 + pi(v) - (b - 1) and k_hard_combine reads it from the pi table.
+// Levels per segment = max(0, B - c).
+template <class XT>
+__global__ void k_hard_plan(const QD *__restrict__ qd, uint32_t Q, const uint64_t *__restrict__ pre_seg,
+                            uint64_t total, const uint32_t *__restrict__ P, uint32_t np,
+                            uint32_t *__restrict__ seg_B, uint64_t *__restrict__ seg_lv)
+{
+    const uint64_t u = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (u >= total) return;
+    const uint32_t q = find_q(pre_seg, Q, u);
+    const QD &d = qd[q];
+    const uint64_t seg = u - pre_seg[q];
+    const uint64_t lo = seg * 2 * (1ull << d.lbits), hi = lo + 2 * (1ull << d.lbits);
+    const XT x = xload<XT>(d);
+    uint64_t v = d.r4;
+    if (lo) {
+        const uint64_t v1 = cpx_isqrt((u128)((x - 1) / (XT)lo));
+        if (v1 < v) v = v1;
+    }
+    const uint64_t v2 = cpx_isqrt((u128)(hi - 1));
+    if (v2 < v) v = v2;
+    uint32_t a = 0, bnd = np;  // count of P[i] <= v
+    while (a < bnd) {
+        const uint32_t mid = (a + bnd) >> 1;
+        if (P[mid] <= v) a = mid + 1;
+        else bnd = mid;
+    }
+    seg_B[u] = a;
+    seg_lv[u] = a > d.c ? a - d.c : 0;
+}
+
+// H += sum over segments of carry(seg, b) * msum(seg, b); carry = count of
+// survivors of level b-1 below the segment.  Level b is sieved from the first
+// segment reaching p_b^2; below p_b^2 the survivors of level b-1 are 1 and the
+// primes from p_b on, so the carry starts at 1 + max(0, pi(lo - 1) - (b - 1))
+// from the pi table and then adds the sieved segments' counts.  One thread per
+// (query, b).
+__global__ void k_hard_combine(const QD *__restrict__ qd, uint32_t Q, const uint64_t *__restrict__ pre_comb,
+                               uint64_t total, const uint64_t *__restrict__ pre_seg,
+                               const uint32_t *__restrict__ seg_B, const uint64_t *__restrict__ seg_off,
+                               const uint32_t *__restrict__ cnt, const int32_t *__restrict__ ms, uint64_t cap,
+                               const uint32_t *__restrict__ P, const cpx_pient *__restrict__ T,
+                               unsigned long long *__restrict__ acc)
+{
+    const uint64_t u = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    LaneAcc a;
+    if (u < total) {
+        const uint32_t q = find_q(pre_comb, Q, u);
+        const uint64_t lvl = u - pre_comb[q];
+        const QD &d = qd[q];
+        const uint32_t b = d.c + 1 + (uint32_t)lvl;
+        const uint64_t span = 2ull << d.lbits;
+        const uint64_t p = P[b - 1];
+        const uint64_t first = (p * p) / span;  // first segment with hi > p^2
+        const uint64_t s0 = pre_seg[q] + first, s1 = pre_seg[q + 1];
+        uint64_t carry = 0;
+        if (first > 0 && s0 < s1) {
+            const uint64_t lo = first * span;
+            const uint64_t pl = cpx_pi_dev(T, lo - 1);
+            carry = 1 + (pl > b - 1 ? pl - (b - 1) : 0);
+        }
+        i128 H = 0;
+        for (uint64_t sg = s0; sg < s1; sg++) {
+            if (seg_B[sg] < b) break;
+            const uint64_t idx = seg_off[sg] + lvl;
+            if (idx >= cap) break;
+            H += (i128)carry * (i128)ms[idx];
+            carry += cnt[idx];
+        }
+        a.q = q;
+        a.v = H;
+    }
+    warp_flush(a, acc, ACC_HARD);
+}
+
+// ------------------------------------------------------------------ launchers
+
+size_t hard_snapshot_stride(uint32_t lbits_max) { return snap_stride(lbits_max); }
+
+size_t hard_smem_bytes(uint32_t lbits, uint32_t threads, bool wide)
+{
+    return wide ? HardSmem<u128>::bytes(lbits, threads) : HardSmem<uint64_t>::bytes(lbits, threads);
+}
+
+template <class XT> static void hard_go(cpx_ctx *ctx, const Plan &pl)
+{
+    const Tables &tb = ctx->tab;
+    k_hard_plan<XT><<<(unsigned)((pl.n_seg + 255) / 256), 256, 0, ctx->stream>>>(
+        pl.qd, pl.Q, pl.pre_seg, pl.n_seg, tb.P, (uint32_t)tb.prm_n, pl.seg_B, pl.seg_off);
+    CPX_LAUNCH("k_hard_plan");
+    note_launch(ctx);
+    scan_u64(ctx, pl.seg_off, pl.n_seg);
+    const size_t smem = HardSmem<XT>::bytes(pl.lbits_max, pl.hard_threads);
+    CPX_CUDA(cudaFuncSetAttribute(k_hard<XT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    if (ctx->timing) CPX_CUDA(cudaEventRecord(ctx->ev_hard0, ctx->stream));
+    if (pl.max_jobs) CPX_CUDA(cudaMemsetAsync(pl.njobs, 0, sizeof(unsigned int), ctx->stream));
+    k_hard<XT><<<(unsigned)pl.n_seg, pl.hard_threads, smem, ctx->stream>>>(
+        pl.qd, pl.Q, pl.pre_seg, pl.n_seg, pl.seg_B, pl.seg_off, tb.P, tb.MU, tb.T, pl.hard_cnt, pl.hard_ms,
+        pl.hard_entries, pl.acc, pl.lbits_max, pl.jobs, pl.njobs, pl.snap, pl.max_jobs);
+    CPX_LAUNCH("k_hard");
+    note_launch(ctx);
+    if (pl.max_jobs) {
+        k_hard_job_scan<<<1, 1024, 0, ctx->stream>>>(pl.jobs, pl.njobs, pl.max_jobs, pl.job_units);
+        CPX_LAUNCH("k_hard_job_scan");
+        k_hard_leaves<XT><<<(unsigned)ctx->sm_count * 8, kThreads, 0, ctx->stream>>>(
+            pl.jobs, pl.njobs, pl.max_jobs, pl.job_units, pl.snap, pl.lbits_max, tb.MU, tb.T, pl.hard_ms, pl.acc);
+        CPX_LAUNCH("k_hard_leaves");
+        note_launch(ctx, 2);
+    }
+    if (ctx->timing) CPX_CUDA(cudaEventRecord(ctx->ev_hard1, ctx->stream));
+    if (pl.n_comb) {
+        k_hard_combine<<<(unsigned)((pl.n_comb + 255) / 256), 256, 0, ctx->stream>>>(
+            pl.qd, pl.Q, pl.pre_comb, pl.n_comb, pl.pre_seg, pl.seg_B, pl.seg_off, pl.hard_cnt, pl.hard_ms,
+            pl.hard_entries, tb.P, tb.T, pl.acc);
+        CPX_LAUNCH("k_hard_combine");
+        note_launch(ctx);
+    }
+}
+
+void launch_hard(cpx_ctx *ctx, const Plan &pl)
+{
+    if (!pl.n_seg) return;
+    if (pl.n_seg > 0x7FFFFFFFull) fail(CPX_ERANGE, "too many hard-leaf segments in one launch");
+    if (pl.wide) hard_go<u128>(ctx, pl);
+    else hard_go<uint64_t>(ctx, pl);
+}
+
+}  // namespace cpx

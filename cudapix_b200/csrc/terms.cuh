@@ -22,6 +22,17 @@ struct __align__(16) EasyLvl {
     uint64_t i_lo, i_hi, i_base, unit0;
 };
 
+// A heavy (segment, level) leaf set handed from k_hard to k_hard_leaves: the
+// segment's bitmap and per-chunk survivor prefixes at level b-1 sit in
+// snapshot slot `job`; the leaves are m in (mlo, mhi] (prime m only when
+// kind = 1).  unit0/nunits number its work units after the job scan.
+struct __align__(16) HardJob {
+    uint32_t q, b, p, kind;
+    uint64_t mlo, mhi, lo, slot;
+    uint64_t nunits, unit0;
+    u128 xp;
+};
+
 // accumulator slots per query (each a signed 128-bit value = 2 words)
 enum { ACC_P2 = 0, ACC_ORD, ACC_TRIV, ACC_EASY, ACC_HARD, ACC_PIY, ACC_PI, ACC_N };
 constexpr int kAccStride = 2 * ACC_N;  // u64 words per query
@@ -46,6 +57,12 @@ struct Plan {
     int32_t *hard_ms = nullptr;
     unsigned long long *acc = nullptr;
     unsigned int *ticket = nullptr;
+    // heavy hard-leaf sets offloaded from k_hard
+    HardJob *jobs = nullptr;
+    unsigned int *njobs = nullptr;   // device counter
+    uint64_t *job_units = nullptr;   // device: total work units after the scan
+    unsigned char *snap = nullptr;   // snapshot slots
+    uint32_t max_jobs = 0;
     // composite easy leaves
     const EasyLvl *elv = nullptr;
     uint32_t n_elv = 0;
@@ -60,5 +77,6 @@ void launch_easy_comp(cpx_ctx *ctx, const Plan &pl);
 void launch_hard(cpx_ctx *ctx, const Plan &pl);
 void launch_finalize(cpx_ctx *ctx, const Plan &pl, u128 *d_out_pi, bool full);
 size_t hard_smem_bytes(uint32_t lbits, uint32_t threads, bool wide);
+size_t hard_snapshot_stride(uint32_t lbits_max);
 
 }  // namespace cpx
