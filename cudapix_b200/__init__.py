@@ -106,6 +106,9 @@ class Context:
     def set_hard_params(self, log2_bits, threads):
         self.call("cpx_set_hard_params", log2_bits, threads)
 
+    def set_hard_offload(self, min_candidates):
+        self.call("cpx_set_hard_offload", min_candidates)
+
     def set_timing(self, on=True):
         self.call("cpx_set_timing", 1 if on else 0)
 

@@ -96,6 +96,7 @@ _SIGS = {
     "cpx_copy_to_device": (ctypes.c_int, [P, P, ctypes.c_size_t]),
     "cpx_device_count": (ctypes.c_int, []),
     "cpx_set_hard_params": (ctypes.c_int, [P, u32, u32]),
+    "cpx_set_hard_offload": (ctypes.c_int, [P, u32]),
     "cpx_last_hard_stats": (ctypes.c_int, [P, ctypes.POINTER(ctypes.c_float), ctypes.POINTER(ctypes.c_double)]),
     "cpx_set_timing": (ctypes.c_int, [P, ctypes.c_int]),
     "cpx_last_batch_ms": (ctypes.c_int, [P, ctypes.POINTER(ctypes.c_float)]),

@@ -162,6 +162,11 @@ int cpx_set_hard_params(cpx_ctx *ctx, uint32_t log2_bits, uint32_t threads)
     });
 }
 
+int cpx_set_hard_offload(cpx_ctx *ctx, uint32_t min_candidates)
+{
+    return guarded(ctx, [&] { ctx->hard_offload_min = min_candidates; });
+}
+
 int cpx_mem_info(cpx_ctx *ctx, uint64_t *free_bytes, uint64_t *total_bytes)
 {
     return guarded(ctx, [&] {

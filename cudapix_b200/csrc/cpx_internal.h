@@ -96,6 +96,7 @@ struct cpx_ctx {
     // tuning
     uint32_t hard_log2_bits = 18;  // hard-leaf segment size (odd numbers, bits)
     uint32_t hard_threads = 256;
+    uint32_t hard_offload_min = 1024;  // candidates of a (sub-segment, level) sent to k_hard_leaves
     // kernel timing (CUDA events around the hard-leaf sieve)
     bool timing = false;
     cudaEvent_t ev_hard0 = nullptr, ev_hard1 = nullptr;

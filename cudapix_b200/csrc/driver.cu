@@ -310,7 +310,7 @@ void run_batch(cpx_ctx *ctx, const BatchReq &rq)
         pl.hard_cnt = ctx->b_work[4].as<uint32_t>(hard_entries + 1);
         pl.hard_ms = ctx->b_work[5].as<int32_t>(hard_entries + 1);
         // snapshot pool for heavy (segment, level) leaf sets: at most 8192 slots and 512 MiB
-        const size_t stride = hard_snapshot_stride(lbits_max);
+        const size_t stride = hard_snapshot_stride(lbits_max - (uint32_t)(__builtin_ctz(threads) - 5));
         pl.max_jobs = (uint32_t)std::min<size_t>(8192, (size_t(512) << 20) / stride);
         pl.jobs = ctx->b_jobs.as<HardJob>(pl.max_jobs);
         uint64_t *ctl = ctx->b_jobctl.as<uint64_t>(4);

@@ -5,16 +5,23 @@
 // this library's exact leaf split: a leaf (b, m) is hard when
 // u = x/(p_b m) >= p_b^2, i.e. p_b <= iroot4(x) and m <= x/p_b^3; it
 // contributes -mu(m) phi(u, b-1), which the sieve answers from the bitmap of
-// the segment holding u plus the survivors of level b-1 below the segment.
+// the segment holding u plus the survivors of level b-1 below it.
 //
-// One CTA owns one segment of 2^lbits odd numbers n = lo + 2i + 1 as a bitmap
-// in shared memory, with one 8-bit survivor counter per 16-byte chunk
-// (128 numbers).  For each level b it (1) records the segment's survivor count
-// at level b-1, (2) if the segment holds leaves of p_b, scans the counters into
-// per-thread prefixes and answers each leaf as
-//     thread prefix + counters of the owner's earlier chunks + popcounts in the chunk,
-// (3) crosses off p_b, counting the bits it clears and keeping the chunk
-// counters current.  Carries between segments are added by k_hard_combine.
+// One CTA owns one segment of 2^lbits odd numbers n = lo + 2i + 1; each of its
+// warps owns a contiguous sub-segment as a bitmap in shared memory with one
+// 8-bit survivor counter per 16-byte chunk (128 numbers), and walks the levels
+// b = c+1 .. B(seg) on its own, synchronising only inside the warp.  Per
+// level a warp (1) records its survivor count at level b-1, (2) if its
+// sub-segment holds leaves of p_b, scans the counters into lane prefixes and
+// answers each leaf as lane prefix + earlier counters of the owning lane +
+// popcounts in the chunk -- or, for a large candidate range, hands the level
+// to k_hard_leaves with a snapshot of the sub-segment, (3) crosses off p_b,
+// counting cleared bits and keeping the counters current.  The level
+// parameters (x/p, candidate range, first multiple) are computed 32 levels at
+// a time, one level per lane, and broadcast by shuffles.  Every 32 levels the
+// CTA combines its warps: carries between sub-segments enter the hard sum and
+// the per-segment (count, Sum(-mu)) pairs go to k_hard_combine, which adds the
+// carries between segments.
 //
 // Bitmap layout: thread t owns chunks [CPT t, CPT (t+1)); chunk c is stored at
 // c ^ ((c >> log2 CPT) & 7) so the owners' 128-bit accesses are free of bank
@@ -58,36 +65,38 @@ __device__ __forceinline__ uint32_t counter_sum(const uint8_t *c8, uint32_t n)
     return s;
 }
 
-// A level whose candidate range in a segment holds at least kOffloadMin odd m
-// (8 per pi-table entry for prime-only levels) is answered by k_hard_leaves.
-constexpr uint64_t kOffloadMin = 4096;
+// A level whose candidate range in a warp's sub-segment holds at least
+// offload_min odd m (8 per pi-table entry for prime-only levels) is answered
+// by k_hard_leaves (cpx_set_hard_offload; 0 keeps every leaf in the sieve).
 constexpr uint64_t kJobWords = 256;   // pi-table entries per k_hard_leaves unit (prime levels)
 constexpr uint64_t kJobGroups = 256;  // 4-m groups per k_hard_leaves unit (other levels)
 
-// bytes of one snapshot slot: 16-byte bitmap chunks + 32-bit survivor prefixes
-__host__ __device__ __forceinline__ size_t snap_stride(uint32_t lbits_max)
+// bytes of one snapshot slot of a sub-segment of 2^lbits_sub numbers:
+// 16-byte bitmap chunks + 32-bit survivor prefixes
+__host__ __device__ __forceinline__ size_t snap_stride(uint32_t lbits_sub)
 {
-    const size_t nc = (size_t(1) << lbits_max) >> 7;
+    const size_t nc = (size_t(1) << lbits_sub) >> 7;
     return (nc * 20 + 255) & ~size_t(255);
 }
 
-template <class XT> struct HardSmem {
-    static __host__ __device__ size_t bytes(uint32_t lbits, uint32_t threads)
-    {
-        const size_t L = size_t(1) << lbits;
-        size_t o = L / 8;                        // bitmap
-        o += ((L / 128) + 15) & ~size_t(15);     // chunk counters
-        o += threads * 4;                        // toff
-        o += 32 * 4;                             // wsum
-        o += threads * (4 * 5);                  // s_p, s_mlo, s_mhi, s_i0, s_r0
-        o = (o + 15) & ~size_t(15);
-        o += threads * sizeof(XT);               // s_xp
-        o += 64;                                 // s_clr[2], s_ms
-        o = (o + 15) & ~size_t(15);
-        o += 32 * sizeof(i128);                  // reductions
-        return o;
-    }
+struct LvlOut {
+    uint32_t cnt;
+    int32_t ms;
+    uint32_t job;
+    uint32_t pad;
 };
+
+__host__ __device__ __forceinline__ size_t hard_smem(uint32_t lbits, uint32_t threads)
+{
+    const size_t L = size_t(1) << lbits;
+    size_t o = L / 8;                                 // bitmap
+    o += ((L / 128) + 15) & ~size_t(15);              // chunk counters
+    o += threads * 4;                                 // lane prefixes
+    o += 2 * (threads / 32) * 32 * sizeof(LvlOut);    // per-warp level outputs, double buffered
+    o = (o + 15) & ~size_t(15);
+    o += 32 * sizeof(i128);                           // reductions
+    return o;
+}
 
 template <class XT>
 __global__ void __launch_bounds__(512) k_hard(const QD *__restrict__ qd, uint32_t Q,
@@ -100,7 +109,7 @@ __global__ void __launch_bounds__(512) k_hard(const QD *__restrict__ qd, uint32_
                                               uint64_t cap, unsigned long long *__restrict__ acc,
                                               uint32_t lbits_max, HardJob *__restrict__ jobs,
                                               unsigned int *__restrict__ njobs, unsigned char *__restrict__ snap,
-                                              uint32_t max_jobs)
+                                              uint32_t max_jobs, uint32_t lbits_sub_max, uint32_t offload_min)
 {
     extern __shared__ uint4 smem4[];
     const uint64_t unit = blockIdx.x;
@@ -110,13 +119,15 @@ __global__ void __launch_bounds__(512) k_hard(const QD *__restrict__ qd, uint32_
     const QD &d = qd[q];
     const uint32_t c = d.c;
     if (B <= c) return;  // uniform over the CTA
-    const uint32_t T = blockDim.x, tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const uint32_t T = blockDim.x, tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, NW = T >> 5;
     const uint32_t L = 1u << d.lbits;
-    const uint32_t NC = L >> 7;    // chunks
-    const uint32_t CPT = NC / T;   // chunks per thread (>= 1)
+    const uint32_t NC = L >> 7;    // chunks of the segment
+    const uint32_t CPT = NC / T;   // chunks per lane (>= 1)
     const int s = __ffs(CPT) - 1;  // log2 CPT
+    const uint32_t Lw = L / NW;    // bits of a warp's sub-segment
     const uint64_t seg = unit - pre_seg[q];
-    const uint64_t lo = seg * 2 * (uint64_t)L, hi = lo + 2 * (uint64_t)L;
+    const uint64_t lo = seg * 2 * (uint64_t)L;
+    const uint64_t lo_w = lo + 2 * (uint64_t)Lw * warp, hi_w = lo_w + 2 * (uint64_t)Lw;
     const uint64_t off = seg_off[unit];
     if (off + (B - c) > cap) return;  // the host sized the ragged outputs exactly; never write past them
     const XT x = xload<XT>(d);
@@ -129,25 +140,17 @@ __global__ void __launch_bounds__(512) k_hard(const QD *__restrict__ qd, uint32_
     size_t o = Lmax / 8;
     uint8_t *cnt8 = reinterpret_cast<uint8_t *>(sp + o);
     o += ((Lmax / 128) + 15) & ~size_t(15);
-    uint32_t *toff = reinterpret_cast<uint32_t *>(sp + o);
+    uint32_t *loff = reinterpret_cast<uint32_t *>(sp + o);  // [NW][32] lane prefixes
     o += T * 4;
-    uint32_t *wsum = reinterpret_cast<uint32_t *>(sp + o);
-    o += 32 * 4;
-    uint32_t *s_p = reinterpret_cast<uint32_t *>(sp + o);
-    uint32_t *s_mlo = s_p + T, *s_mhi = s_mlo + T, *s_i0 = s_mhi + T, *s_r0 = s_i0 + T;
-    o += T * 20;
-    o = (o + 15) & ~size_t(15);
-    XT *s_xp = reinterpret_cast<XT *>(sp + o);
-    o += T * sizeof(XT);
-    int *s_clr = reinterpret_cast<int *>(sp + o);
-    int *s_ms = s_clr + 2;
-    unsigned int *s_job = reinterpret_cast<unsigned int *>(s_clr + 3);
-    o += 64;
+    LvlOut *area = reinterpret_cast<LvlOut *>(sp + o);      // [2][NW][32]
+    o += 2 * NW * 32 * sizeof(LvlOut);
     o = (o + 15) & ~size_t(15);
     i128 *s_red = reinterpret_cast<i128 *>(sp + o);
+    uint32_t *wl = loff + 32 * warp;  // this warp's lane prefixes
 
-    const uint32_t c0 = CPT * tid;  // first owned chunk
+    const uint32_t c0 = CPT * tid;  // first owned chunk (of the segment)
     const uint32_t w0 = 4 * c0;     // first owned word
+    const uint32_t cw0 = c0 - CPT * 32 * warp;  // first owned chunk of the sub-segment
     // ---- pre-sieve with p_2 .. p_c; chunk counters
     uint32_t cnt0 = 0;
     {
@@ -183,30 +186,17 @@ __global__ void __launch_bounds__(512) k_hard(const QD *__restrict__ qd, uint32_
             reinterpret_cast<uint4 *>(bm)[swz(c0 + j, s)] = make_uint4(wv[0], wv[1], wv[2], wv[3]);
         }
     }
-    if (tid == 0) {
-        s_clr[0] = s_clr[1] = 0;
-        *s_ms = 0;
-    }
-    uint32_t tot = 0;  // thread 0: survivors of the segment at the current level
-    {
-        uint32_t v = cnt0;
-#pragma unroll
-        for (int dd = 16; dd > 0; dd >>= 1) v += __shfl_down_sync(FULL, v, dd);
-        if (lane == 0) wsum[warp] = v;
-        __syncthreads();
-        if (tid == 0)
-            for (uint32_t k = 0; k < T / 32; k++) tot += wsum[k];
-        __syncthreads();
-    }
+    uint32_t tot = __reduce_add_sync(FULL, cnt0);  // survivors of this warp's sub-segment
+    __syncwarp();
 
-    // survivors of the segment with n <= uu (uu in [lo, hi))
-    auto seg_count = [&](uint64_t uu) -> uint32_t {
-        const uint32_t kk = (uint32_t)((uu - lo + 1) >> 1);  // bits [0, kk)
+    // survivors of the warp's sub-segment with n <= uu (uu in [lo_w, hi_w))
+    auto sub_count = [&](uint64_t uu) -> uint32_t {
+        const uint32_t kk = (uint32_t)((uu - lo_w + 1) >> 1);  // bits [0, kk) of the sub-segment
         if (!kk) return 0u;
-        const uint32_t jb = kk - 1, w = jb >> 5, ch = w >> 2, ow = ch >> s;
-        uint32_t cv = toff[ow];
-        for (uint32_t i = 0; i < (ow >> 5); i++) cv += wsum[i];
-        cv += counter_sum(cnt8 + (size_t)ow * CPT, ch - ow * CPT);
+        const uint32_t jb = kk - 1, w = jb >> 5;
+        const uint32_t chs = w >> 2, ow = chs >> s;      // chunk in the sub-segment, owning lane
+        const uint32_t ch = chs + CPT * 32 * warp;       // chunk in the segment
+        uint32_t cv = wl[ow] + counter_sum(cnt8 + ch - (chs - ow * CPT), chs - ow * CPT);
         const uint4 v4 = reinterpret_cast<const uint4 *>(bm)[swz(ch, s)];
         const uint32_t wi = w & 3, msk = (2u << (jb & 31)) - 1u;
         if (wi == 0) cv += __popc(v4.x & msk);
@@ -216,50 +206,56 @@ __global__ void __launch_bounds__(512) k_hard(const QD *__restrict__ qd, uint32_
         return cv;
     };
 
-    int64_t S = 0;
-    for (uint32_t bb = c + 1; bb <= B; bb += T) {
-        const uint32_t nbat = min(T, B - bb + 1);
-        if (tid < nbat) {
-            const uint32_t b = bb + tid;
-            const uint64_t p = P[b - 1];
+    int64_t S = 0;       // this lane's share of the hard sum (survivor counts within sub-segments)
+    i128 Sx = 0;         // warp 0: carries between the CTA's sub-segments
+    uint32_t grp = 0;
+    for (uint32_t gb = c + 1; gb <= B; gb += 32, grp++) {
+        const uint32_t nl = min(32u, B - gb + 1);
+        // ---- level parameters, one level per lane
+        uint32_t lp = 0, lmlo = 0, lmhi = 0, lr0 = 0, li0 = 0xFFFFFFFFu;
+        XT lxp = 0;
+        if (lane < nl) {
+            const uint64_t p = P[gb + lane - 1];
             const XT xp = x / (XT)p;
             uint64_t mlo = y / p;
-            const XT t1 = xp / (XT)hi;
+            const XT t1 = xp / (XT)hi_w;
             if (t1 > (XT)mlo) mlo = (uint64_t)t1;
             uint64_t mhi = y;
-            if (lo) {
-                const XT t2 = xp / (XT)lo;
+            if (lo_w) {
+                const XT t2 = xp / (XT)lo_w;
                 if (t2 < (XT)mhi) mhi = (uint64_t)t2;
             }
-            {
-                // hard leaves only: x/(p m) >= p^2, i.e. m <= x/p^3
-                const XT t3 = xp / (XT)(p * p);
-                if (t3 < (XT)mhi) mhi = (uint64_t)t3;
-            }
+            const XT t3 = xp / (XT)(p * p);  // hard leaves only: m <= x/p^3
+            if (t3 < (XT)mhi) mhi = (uint64_t)t3;
             if (mhi < mlo) mhi = mlo;
-            s_p[tid] = (uint32_t)p;
-            s_xp[tid] = xp;
-            s_mlo[tid] = (uint32_t)mlo;
-            s_mhi[tid] = (uint32_t)mhi;
-            const uint64_t r0 = (lo + 1) % p;
-            s_r0[tid] = (uint32_t)r0;
-            uint64_t m = lo + 1 + (r0 ? p - r0 : 0);
+            lp = (uint32_t)p;
+            lxp = xp;
+            lmlo = (uint32_t)mlo;
+            lmhi = (uint32_t)mhi;
+            const uint64_t r0 = (lo_w + 1) % p;
+            lr0 = (uint32_t)r0;
+            uint64_t m = lo_w + 1 + (r0 ? p - r0 : 0);
             if ((m & 1) == 0) m += p;
-            s_i0[tid] = (m < hi) ? (uint32_t)((m - lo - 1) >> 1) : 0xFFFFFFFFu;
+            li0 = (m < hi_w) ? (uint32_t)((m - lo_w - 1) >> 1) : 0xFFFFFFFFu;
         }
-        __syncthreads();
-        for (uint32_t k = 0; k < nbat; k++) {
-            const uint32_t b = bb + k;
-            const uint32_t p = s_p[k];
-            const uint32_t mlo = s_mlo[k], mhi = s_mhi[k];
-            const uint64_t slot = off + (b - c - 1);
-            if (tid == 0) {
-                tot -= (uint32_t)s_clr[(b - 1) & 1];
-                s_clr[(b - 1) & 1] = 0;
-                out_cnt[slot] = tot;
+        LvlOut mine = {0, 0, 0xFFFFFFFFu, 0};
+        for (uint32_t k = 0; k < nl; k++) {
+            const uint32_t b = gb + k;
+            const uint32_t p = __shfl_sync(FULL, lp, k);
+            const uint32_t mlo = __shfl_sync(FULL, lmlo, k), mhi = __shfl_sync(FULL, lmhi, k);
+            XT xp;
+            if (sizeof(XT) == 8) {
+                xp = (XT)__shfl_sync(FULL, (unsigned long long)lxp, k);
+            } else {
+                const unsigned long long a0 = __shfl_sync(FULL, (unsigned long long)lxp, k);
+                const unsigned long long a1 = __shfl_sync(FULL, (unsigned long long)((u128)lxp >> 64), k);
+                xp = (XT)(((u128)a1 << 64) | a0);
             }
+            const uint32_t cnt_b = tot;
+            int32_t ms_b = 0;
+            uint32_t job_b = 0xFFFFFFFFu;
             if (mhi > mlo) {
-                // per-thread prefixes from the chunk counters
+                // lane prefixes of the sub-segment from the chunk counters
                 const uint32_t run = counter_sum(cnt8 + c0, CPT);
                 uint32_t inc = run;
 #pragma unroll
@@ -267,38 +263,31 @@ __global__ void __launch_bounds__(512) k_hard(const QD *__restrict__ qd, uint32_
                     const uint32_t t = __shfl_up_sync(FULL, inc, oo);
                     if (lane >= (uint32_t)oo) inc += t;
                 }
-                toff[tid] = inc - run;
-                if (lane == 31) wsum[warp] = inc;
-                __syncthreads();
-                const XT xp = s_xp[k];
-                int32_t msl = 0;
-                // a large candidate range goes to k_hard_leaves with a snapshot of the segment
+                wl[lane] = inc - run;
+                __syncwarp();
                 const bool prime_lvl = (uint64_t)p * p > y;
                 const uint64_t qa = mlo > p ? mlo : p;
-                uint64_t work = 0;
+                uint64_t work;
                 if (prime_lvl) work = (mhi > qa) ? 8 * ((((uint64_t)mhi - 1) >> 7) - (qa >> 7) + 1) : 0;
                 else work = ((((uint64_t)mhi - 1) >> 1) - (((uint64_t)mlo + 1) >> 1) + 1);
                 bool offloaded = false;
-                if (max_jobs && work >= kOffloadMin) {
-                    if (tid == 0) {
-                        const unsigned int j = atomicAdd(njobs, 1u);
-                        *s_job = j < max_jobs ? j : 0xFFFFFFFFu;
-                    }
-                    __syncthreads();
-                    const unsigned int job = *s_job;
-                    if (job != 0xFFFFFFFFu) {
+                if (max_jobs && offload_min && work >= offload_min) {
+                    unsigned int j = 0;
+                    if (lane == 0) j = atomicAdd(njobs, 1u);
+                    j = __shfl_sync(FULL, j, 0);
+                    if (j < max_jobs) {
                         offloaded = true;
-                        const size_t stride = snap_stride(lbits_max);
-                        uint4 *sb = reinterpret_cast<uint4 *>(snap + (size_t)job * stride);
-                        uint32_t *spre = reinterpret_cast<uint32_t *>(sb + (Lmax >> 7));
-                        uint32_t pre = toff[tid];
-                        for (uint32_t i = 0; i < warp; i++) pre += wsum[i];
-                        for (uint32_t j = 0; j < CPT; j++) {
-                            sb[c0 + j] = reinterpret_cast<const uint4 *>(bm)[swz(c0 + j, s)];
-                            spre[c0 + j] = pre;
-                            pre += cnt8[c0 + j];
+                        job_b = j;
+                        const size_t stride = snap_stride(lbits_sub_max);
+                        uint4 *sb = reinterpret_cast<uint4 *>(snap + (size_t)j * stride);
+                        uint32_t *spre = reinterpret_cast<uint32_t *>(sb + ((size_t(1) << lbits_sub_max) >> 7));
+                        uint32_t pre = wl[lane];
+                        for (uint32_t jj = 0; jj < CPT; jj++) {
+                            sb[cw0 + jj] = reinterpret_cast<const uint4 *>(bm)[swz(c0 + jj, s)];
+                            spre[cw0 + jj] = pre;
+                            pre += cnt8[c0 + jj];
                         }
-                        if (tid == 0) {
+                        if (lane == 0) {
                             HardJob J;
                             J.q = q;
                             J.b = b;
@@ -306,76 +295,73 @@ __global__ void __launch_bounds__(512) k_hard(const QD *__restrict__ qd, uint32_
                             J.kind = prime_lvl ? 1u : 0u;
                             J.mlo = prime_lvl ? qa : mlo;
                             J.mhi = mhi;
-                            J.lo = lo;
-                            J.slot = slot;
+                            J.lo = lo_w;
+                            J.slot = off + (b - c - 1);
                             J.nunits = prime_lvl ? (work / 8 + kJobWords - 1) / kJobWords
                                                  : (((((uint64_t)mhi - 1) >> 1) >> 2) -
                                                     ((((uint64_t)mlo + 1) >> 1) >> 2) + kJobGroups) /
                                                        kJobGroups;
                             J.unit0 = 0;
+                            J.carry = 0;  // filled in by the group combine below
+                            J.pad = 0;
                             J.xp = (u128)xp;
-                            jobs[job] = J;
+                            jobs[j] = J;
                         }
                     }
                 }
-                if (offloaded) {
-                    // the leaves of this level are counted by k_hard_leaves
-                } else if (prime_lvl) {
-                    // m must be a prime q > p: walk the pi-table bitmap of (max(mlo, p), mhi]
-                    if (mhi > qa) {
-                        const uint64_t w0q = qa >> 7, w1q = ((uint64_t)mhi - 1) >> 7;
-                        for (uint64_t wq = w0q + tid; wq <= w1q; wq += T) {
-                            const ulonglong2 e = __ldg(reinterpret_cast<const ulonglong2 *>(Tpi) + wq);
-                            uint64_t qb = e.x & range_mask(wq, qa, mhi);
-                            while (qb) {
-                                const int j = __ffsll((long long)qb) - 1;
-                                qb &= qb - 1;
-                                const uint64_t m = 128 * wq + 2 * j + 1;
-                                S += seg_count((uint64_t)(xp / (XT)m));  // mu(q) = -1
-                                msl += 1;
+                if (!offloaded) {
+                    int32_t msl = 0;
+                    if (prime_lvl) {
+                        // m must be a prime q > p: walk the pi-table bitmap of (max(mlo, p), mhi]
+                        if (mhi > qa) {
+                            const uint64_t w0q = qa >> 7, w1q = ((uint64_t)mhi - 1) >> 7;
+                            for (uint64_t wq = w0q + lane; wq <= w1q; wq += 32) {
+                                const ulonglong2 e = __ldg(reinterpret_cast<const ulonglong2 *>(Tpi) + wq);
+                                uint64_t qb = e.x & range_mask(wq, qa, mhi);
+                                while (qb) {
+                                    const int j = __ffsll((long long)qb) - 1;
+                                    qb &= qb - 1;
+                                    const uint64_t m = 128 * wq + 2 * j + 1;
+                                    S += sub_count((uint64_t)(xp / (XT)m));  // mu(q) = -1
+                                    msl += 1;
+                                }
+                            }
+                        }
+                    } else {
+                        // any squarefree m with lpf(m) > p: 16-byte loads of packed mu*lpf
+                        const uint64_t i_lo = ((uint64_t)mlo + 1) >> 1, i_hi = ((uint64_t)mhi - 1) >> 1;
+                        for (uint64_t g = (i_lo >> 2) + lane; g <= (i_hi >> 2); g += 32) {
+                            const int4 v4 = __ldg(reinterpret_cast<const int4 *>(MU) + g);
+                            const int32_t vals[4] = {v4.x, v4.y, v4.z, v4.w};
+#pragma unroll
+                            for (int kq = 0; kq < 4; kq++) {
+                                const uint64_t i = 4 * g + kq;
+                                const int32_t v = vals[kq];
+                                if (i < i_lo || i > i_hi || v == 0) continue;
+                                if ((uint32_t)(v > 0 ? v : -v) <= p) continue;
+                                const uint32_t cv = sub_count((uint64_t)(xp / (XT)(2 * i + 1)));
+                                if (v > 0) {
+                                    S -= cv;
+                                    msl -= 1;
+                                } else {
+                                    S += cv;
+                                    msl += 1;
+                                }
                             }
                         }
                     }
-                } else {
-                    // any squarefree m with lpf(m) > p: 16-byte loads of packed mu*lpf
-                    const uint64_t i_lo = ((uint64_t)mlo + 1) >> 1, i_hi = ((uint64_t)mhi - 1) >> 1;  // m = 2i + 1
-                    for (uint64_t g = (i_lo >> 2) + tid; g <= (i_hi >> 2); g += T) {
-                        const int4 v4 = __ldg(reinterpret_cast<const int4 *>(MU) + g);
-                        const int32_t vals[4] = {v4.x, v4.y, v4.z, v4.w};
-#pragma unroll
-                        for (int kq = 0; kq < 4; kq++) {
-                            const uint64_t i = 4 * g + kq;
-                            const int32_t v = vals[kq];
-                            if (i < i_lo || i > i_hi || v == 0) continue;
-                            if ((uint32_t)(v > 0 ? v : -v) <= p) continue;
-                            const uint32_t cv = seg_count((uint64_t)(xp / (XT)(2 * i + 1)));
-                            if (v > 0) {
-                                S -= cv;
-                                msl -= 1;
-                            } else {
-                                S += cv;
-                                msl += 1;
-                            }
-                        }
-                    }
+                    ms_b = __reduce_add_sync(FULL, msl);
                 }
-#pragma unroll
-                for (int dd = 16; dd > 0; dd >>= 1) msl += __shfl_down_sync(FULL, msl, dd);
-                if (lane == 0 && msl) atomicAdd(s_ms, msl);
-                __syncthreads();
-                if (tid == 0) {
-                    out_ms[slot] = *s_ms;
-                    *s_ms = 0;
-                }
-            } else if (tid == 0) {
-                out_ms[slot] = 0;
+                __syncwarp();
             }
-            // cross off p_b, counting bits that were still set and keeping the counters current
+            // ---- cross off p_b in the sub-segment
             uint32_t cleared = 0;
-            if (p < 64) {
-                const uint32_t Mp = every_pth_bit(p);  // p < 32 has several multiples per word
-                const uint32_t st = 64u % p;
-                uint32_t r = (s_r0[k] + (64u * w0) % p) % p;
+            if (p < 128) {
+                // each lane masks its own words; p < 32 has several multiples per word
+                const uint32_t Mp = every_pth_bit(p);
+                const uint32_t stp = 64u % p;
+                const uint32_t r0 = __shfl_sync(FULL, lr0, k);
+                uint32_t r = (r0 + (64u * (cw0 * 4)) % p) % p;  // first owned word of the sub-segment
                 for (uint32_t j = 0; j < CPT; j++) {
                     uint4 v = reinterpret_cast<const uint4 *>(bm)[swz(c0 + j, s)];
                     uint32_t a4[4] = {v.x, v.y, v.z, v.w};
@@ -385,7 +371,7 @@ __global__ void __launch_bounds__(512) k_hard(const QD *__restrict__ qd, uint32_
                         const uint32_t mk = mult_mask(r, p, Mp);
                         cj += __popc(a4[kk] & mk);
                         a4[kk] &= ~mk;
-                        r += st;
+                        r += stp;
                         if (r >= p) r -= p;
                     }
                     if (cj) {
@@ -395,27 +381,52 @@ __global__ void __launch_bounds__(512) k_hard(const QD *__restrict__ qd, uint32_
                     cleared += cj;
                 }
             } else {
-                const uint32_t i0 = s_i0[k];
+                // p >= 128: the lanes of one step clear bits p apart, so they touch
+                // distinct words and distinct chunk counters (plain read-modify-write)
+                const uint32_t i0 = __shfl_sync(FULL, li0, k);
                 if (i0 != 0xFFFFFFFFu) {
-                    for (uint64_t i = (uint64_t)i0 + (uint64_t)tid * p; i < L; i += (uint64_t)T * p) {
+                    const uint32_t base_ch = CPT * 32 * warp;
+                    for (uint64_t i = (uint64_t)i0 + (uint64_t)lane * p; i < Lw; i += 32ull * p) {
                         const uint32_t w = (uint32_t)(i >> 5), bit = 1u << (i & 31);
-                        const uint32_t ch = w >> 2;
-                        const uint32_t pw = (swz(ch, s) << 2) | (w & 3);
-                        const uint32_t old = atomicAnd(&bm[pw], ~bit);
+                        const uint32_t ch = base_ch + (w >> 2);
+                        uint32_t *pw = bm + ((swz(ch, s) << 2) | (w & 3));
+                        const uint32_t old = *pw;
                         if (old & bit) {
+                            *pw = old & ~bit;
                             cleared++;
-                            atomicSub(reinterpret_cast<unsigned int *>(cnt8) + (ch >> 2), 1u << (8 * (ch & 3)));
+                            cnt8[ch] = (uint8_t)(cnt8[ch] - 1);
                         }
                     }
                 }
             }
-#pragma unroll
-            for (int dd = 16; dd > 0; dd >>= 1) cleared += __shfl_down_sync(FULL, cleared, dd);
-            if (lane == 0 && cleared) atomicAdd(&s_clr[b & 1], (int)cleared);
-            __syncthreads();
+            tot -= __reduce_add_sync(FULL, cleared);
+            __syncwarp();
+            if (lane == k) {
+                mine.cnt = cnt_b;
+                mine.ms = ms_b;
+                mine.job = job_b;
+            }
+        }
+        // ---- combine the warps of the CTA for these 32 levels
+        LvlOut *ar = area + (grp & 1) * NW * 32;
+        ar[warp * 32 + lane] = mine;
+        __syncthreads();
+        if (warp == 0 && lane < nl) {
+            const uint32_t b = gb + lane;
+            uint64_t carry = 0;
+            int32_t msum = 0;
+            for (uint32_t w = 0; w < NW; w++) {
+                const LvlOut e = ar[w * 32 + lane];
+                Sx += (i128)carry * e.ms;
+                if (e.job != 0xFFFFFFFFu) jobs[e.job].carry = carry;
+                carry += e.cnt;
+                msum += e.ms;
+            }
+            out_cnt[off + (b - c - 1)] = (uint32_t)carry;
+            out_ms[off + (b - c - 1)] = msum;
         }
     }
-    const i128 Sb = cpx_block_sum_i128((i128)S, s_red);
+    const i128 Sb = cpx_block_sum_i128((i128)S + Sx, s_red);
     if (tid == 0) acc_add(acc, q, ACC_HARD, Sb);
 }
 
@@ -458,7 +469,7 @@ __global__ void __launch_bounds__(kThreads) k_hard_leaves(const HardJob *__restr
                                                           const unsigned int *njobs, uint32_t max_jobs,
                                                           const uint64_t *total_units,
                                                           const unsigned char *__restrict__ snap,
-                                                          uint32_t lbits_max, const int32_t *__restrict__ MU,
+                                                          uint32_t lbits_sub, const int32_t *__restrict__ MU,
                                                           const cpx_pient *__restrict__ Tpi,
                                                           int32_t *__restrict__ out_ms,
                                                           unsigned long long *__restrict__ acc)
@@ -468,8 +479,8 @@ __global__ void __launch_bounds__(kThreads) k_hard_leaves(const HardJob *__restr
     const uint32_t lane = threadIdx.x & 31;
     const uint64_t gw = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const uint64_t nw = ((uint64_t)gridDim.x * blockDim.x) >> 5;
-    const size_t stride = snap_stride(lbits_max);
-    const size_t ncmax = (size_t(1) << lbits_max) >> 7;
+    const size_t stride = snap_stride(lbits_sub);
+    const size_t ncmax = (size_t(1) << lbits_sub) >> 7;
     for (uint64_t unit = gw; unit < total; unit += nw) {
         uint32_t lo_j = 0, hi_j = n;  // jobs[lo_j].unit0 <= unit < jobs[hi_j].unit0
         while (hi_j - lo_j > 1) {
@@ -485,9 +496,9 @@ __global__ void __launch_bounds__(kThreads) k_hard_leaves(const HardJob *__restr
         const uint64_t lo = J.lo;
         auto count = [&](uint64_t uu) -> uint32_t {
             const uint32_t kk = (uint32_t)((uu - lo + 1) >> 1);
-            if (!kk) return 0u;
+            if (!kk) return (uint32_t)J.carry;  // u = lo: no number of the sub-segment is <= u
             const uint32_t jb = kk - 1, w = jb >> 5, ch = w >> 2;
-            uint32_t cv = __ldg(spre + ch);
+            uint32_t cv = (uint32_t)J.carry + __ldg(spre + ch);
             const uint4 v4 = __ldg(sb + ch);
             const uint32_t wi = w & 3, msk = (2u << (jb & 31)) - 1u;
             if (wi == 0) cv += __popc(v4.x & msk);
@@ -630,11 +641,12 @@ __global__ void k_hard_combine(const QD *__restrict__ qd, uint32_t Q, const uint
 
 // ------------------------------------------------------------------ launchers
 
-size_t hard_snapshot_stride(uint32_t lbits_max) { return snap_stride(lbits_max); }
+size_t hard_snapshot_stride(uint32_t lbits_sub) { return snap_stride(lbits_sub); }
 
 size_t hard_smem_bytes(uint32_t lbits, uint32_t threads, bool wide)
 {
-    return wide ? HardSmem<u128>::bytes(lbits, threads) : HardSmem<uint64_t>::bytes(lbits, threads);
+    (void)wide;
+    return hard_smem(lbits, threads);
 }
 
 template <class XT> static void hard_go(cpx_ctx *ctx, const Plan &pl)
@@ -645,20 +657,22 @@ template <class XT> static void hard_go(cpx_ctx *ctx, const Plan &pl)
     CPX_LAUNCH("k_hard_plan");
     note_launch(ctx);
     scan_u64(ctx, pl.seg_off, pl.n_seg);
-    const size_t smem = HardSmem<XT>::bytes(pl.lbits_max, pl.hard_threads);
+    const size_t smem = hard_smem(pl.lbits_max, pl.hard_threads);
+    const uint32_t lbits_sub = pl.lbits_max - (uint32_t)(__builtin_ctz(pl.hard_threads) - 5);
     CPX_CUDA(cudaFuncSetAttribute(k_hard<XT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     if (ctx->timing) CPX_CUDA(cudaEventRecord(ctx->ev_hard0, ctx->stream));
     if (pl.max_jobs) CPX_CUDA(cudaMemsetAsync(pl.njobs, 0, sizeof(unsigned int), ctx->stream));
     k_hard<XT><<<(unsigned)pl.n_seg, pl.hard_threads, smem, ctx->stream>>>(
         pl.qd, pl.Q, pl.pre_seg, pl.n_seg, pl.seg_B, pl.seg_off, tb.P, tb.MU, tb.T, pl.hard_cnt, pl.hard_ms,
-        pl.hard_entries, pl.acc, pl.lbits_max, pl.jobs, pl.njobs, pl.snap, pl.max_jobs);
+        pl.hard_entries, pl.acc, pl.lbits_max, pl.jobs, pl.njobs, pl.snap, pl.max_jobs, lbits_sub,
+        ctx->hard_offload_min);
     CPX_LAUNCH("k_hard");
     note_launch(ctx);
     if (pl.max_jobs) {
         k_hard_job_scan<<<1, 1024, 0, ctx->stream>>>(pl.jobs, pl.njobs, pl.max_jobs, pl.job_units);
         CPX_LAUNCH("k_hard_job_scan");
         k_hard_leaves<XT><<<(unsigned)ctx->sm_count * 8, kThreads, 0, ctx->stream>>>(
-            pl.jobs, pl.njobs, pl.max_jobs, pl.job_units, pl.snap, pl.lbits_max, tb.MU, tb.T, pl.hard_ms, pl.acc);
+            pl.jobs, pl.njobs, pl.max_jobs, pl.job_units, pl.snap, lbits_sub, tb.MU, tb.T, pl.hard_ms, pl.acc);
         CPX_LAUNCH("k_hard_leaves");
         note_launch(ctx, 2);
     }

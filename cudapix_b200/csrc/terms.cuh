@@ -28,8 +28,9 @@ struct __align__(16) EasyLvl {
 // kind = 1).  unit0/nunits number its work units after the job scan.
 struct __align__(16) HardJob {
     uint32_t q, b, p, kind;
-    uint64_t mlo, mhi, lo, slot;
+    uint64_t mlo, mhi, lo, slot;  // lo: first number of the warp's sub-segment
     uint64_t nunits, unit0;
+    uint64_t carry, pad;          // survivors of level b-1 in the segment below the sub-segment
     u128 xp;
 };
 

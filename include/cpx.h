@@ -82,6 +82,10 @@ int cpx_mem_info(cpx_ctx *ctx, uint64_t *free_bytes, uint64_t *total_bytes);
 /* hard-leaf sieve tuning: segment = 2^log2_bits odd numbers (15..20),
  * threads per CTA in {128, 256, 512}. */
 int cpx_set_hard_params(cpx_ctx *ctx, uint32_t log2_bits, uint32_t threads);
+/* a (sub-segment, level) of the hard-leaf sieve with at least min_candidates
+ * candidate m is answered by a separate GPU-wide leaf kernel from a snapshot
+ * of the sub-segment; 0 answers every leaf inside the sieve (default 1024) */
+int cpx_set_hard_offload(cpx_ctx *ctx, uint32_t min_candidates);
 /* time of the last hard-leaf sieve (CUDA events on the context stream) and
  * its algorithmic byte count (one pass over the segment bitmap per active
  * prime per segment). */
