@@ -255,6 +255,7 @@ def main():
     ap.add_argument("--cpu-budget", type=float, default=15.0)
     ap.add_argument("--ref-step-s", type=float, default=20.0)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--graph", type=int, default=1, help="also time the batch as one CUDA graph launch")
     args = ap.parse_args()
     world, rank, local = dist_setup()
     if args.impl == "reference":
@@ -302,6 +303,23 @@ def main():
     nq = world * args.queries * args.steps
     value = nq / t_dev
 
+    # the same batch as one CUDA graph launch (CPX_BATCH_GRAPH), e2e through the C ABI
+    graph = None
+    if args.graph:
+        for _ in range(2):
+            assert cpx.pi_batch(xs, ctx=ctx, graph=True) == ref
+        g_e2e, g_dev = [], []
+        for _ in range(args.steps):
+            ctx.flush_l2()
+            ctx.timer_start()
+            out = cpx.pi_batch(xs, ctx=ctx, graph=True)
+            g_e2e.append(ctx.timer_stop())
+            g_dev.append(ctx.last_batch_ms())
+            assert out == ref
+        gt_dev = allmax(sum(g_dev) / 1000.0, world)
+        gt_e2e = allmax(sum(g_e2e) / 1000.0, world)
+        graph = {"value": nq / gt_dev, "e2e": nq / gt_e2e, "unit": UNIT}
+
     # plain path: one full launch sequence per query, on a fixed subsample
     plain = None
     if args.plain and rank == 0:
@@ -338,6 +356,7 @@ def main():
                    "parallelism": f"replicas x{world}"},
         "e2e": {"value": nq / t_e2e, "unit": UNIT, "h2d_bytes_per_step": io[0], "d2h_bytes_per_step": io[1]},
         "gpu_launches": int(launches),
+        "graph": graph,
         "plain": plain,
         "batched_over_plain": (value / plain["value"]) if plain else None,
         "e2e_over_plain": ((nq / t_e2e) / plain["value"]) if plain else None,

@@ -251,25 +251,55 @@ def pi(x, ctx=None):
     return pi_deleglise_rivat(x, 0, 6, ctx)
 
 
-def pi_batch(xs, alpha=None, c=6, hard_log2_bits=0, hard_threads=0, ctx=None):
-    """pi(x) for every x in xs in one batched device pass."""
+BATCH_WIDE = 1   # 128-bit kernels for every query (CPX_BATCH_WIDE)
+BATCH_GRAPH = 2  # the batch's kernels as one CUDA graph launch (CPX_BATCH_GRAPH)
+
+
+def _params(alpha, c, hard_log2_bits, hard_threads, wide, graph):
     from fractions import Fraction
 
-    ctx = ctx or context()
-    n = len(xs)
-    arr = (U128 * max(n, 1))()
-    for i, x in enumerate(xs):
-        arr[i] = U128.of(x)
-    out = (U128 * max(n, 1))()
     p = Params()
     if alpha is not None:
         f = Fraction(alpha).limit_denominator(1000)
         p.alpha_num, p.alpha_den = f.numerator, f.denominator
     p.c = c
+    p.flags = (BATCH_WIDE if wide else 0) | (BATCH_GRAPH if graph else 0)
     p.hard_log2_bits = hard_log2_bits
     p.hard_threads = hard_threads
+    return p
+
+
+def _u128_array(xs):
+    n = len(xs)
+    arr = (U128 * max(n, 1))()
+    for i, x in enumerate(xs):
+        arr[i] = U128.of(x)
+    return arr
+
+
+def pi_batch(xs, alpha=None, c=6, hard_log2_bits=0, hard_threads=0, wide=False, graph=False, ctx=None):
+    """pi(x) for every x in xs in one batched device pass."""
+    ctx = ctx or context()
+    n = len(xs)
+    arr = _u128_array(xs)
+    out = (U128 * max(n, 1))()
+    p = _params(alpha, c, hard_log2_bits, hard_threads, wide, graph)
     ctx.call("cpx_pi_batch", arr, n, ctypes.byref(p), out)
     return [out[i].value() for i in range(n)]
+
+
+def terms_batch(xs, ys=None, alpha=None, c=6, hard_log2_bits=0, hard_threads=0, wide=False, graph=False,
+                ctx=None):
+    """Every term (as pi_terms) for each x in xs, in one batched pass; ys[i] = 0
+    or ys = None selects the y rule (alpha)."""
+    ctx = ctx or context()
+    n = len(xs)
+    arr = _u128_array(xs)
+    yarr = (ctypes.c_uint64 * max(n, 1))(*(ys or [0] * n))
+    out = (Terms * max(n, 1))()
+    p = _params(alpha, c, hard_log2_bits, hard_threads, wide, graph)
+    ctx.call("cpx_terms_batch", arr, yarr, n, ctypes.byref(p), out)
+    return [out[i].as_dict() for i in range(n)]
 
 
 # ---------------------------------------------------------- sieves / tables

@@ -71,7 +71,7 @@ class Params(ctypes.Structure):
         ("alpha_num", ctypes.c_uint32),
         ("alpha_den", ctypes.c_uint32),
         ("c", ctypes.c_uint16),
-        ("pad", ctypes.c_uint16),
+        ("flags", ctypes.c_uint16),
         ("hard_log2_bits", ctypes.c_uint32),
         ("hard_threads", ctypes.c_uint32),
     ]
@@ -140,6 +140,7 @@ _SIGS = {
     "cpx_phisieve_update": (ctypes.c_int, [P]),
     "cpx_phisieve_counts": (ctypes.c_int, [P, PP, pu32]),
     "cpx_pi_batch": (ctypes.c_int, [P, pU, ctypes.c_size_t, ctypes.POINTER(Params), pU]),
+    "cpx_terms_batch": (ctypes.c_int, [P, pU, pu64, ctypes.c_size_t, ctypes.POINTER(Params), ctypes.POINTER(Terms)]),
     "cpx_mem_info": (ctypes.c_int, [P, pu64, pu64]),
 }
 

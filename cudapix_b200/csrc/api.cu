@@ -105,6 +105,7 @@ int cpx_destroy(cpx_ctx *ctx)
         ctx->b_jobs.release();
         ctx->b_jobctl.release();
         ctx->b_snap.release();
+        if (ctx->graph_exec) cudaGraphExecDestroy(ctx->graph_exec);
         if (ctx->ev_hard0) cudaEventDestroy(ctx->ev_hard0);
         if (ctx->ev_hard1) cudaEventDestroy(ctx->ev_hard1);
         for (cudaEvent_t ev : {ctx->ev_b0, ctx->ev_b1, ctx->ev_t0, ctx->ev_t1})
@@ -367,6 +368,19 @@ int cpx_pi_u128(cpx_ctx *ctx, cpx_u128 x, uint64_t y, uint16_t c, cpx_u128 *pi, 
     });
 }
 
+static void apply_params(BatchReq &rq, const cpx_params *params)
+{
+    if (!params) return;
+    if (params->flags & ~(CPX_BATCH_WIDE | CPX_BATCH_GRAPH)) fail(CPX_EINVAL, "unknown cpx_params flag");
+    rq.c = params->c ? params->c : 6;
+    rq.alpha_num = params->alpha_num;
+    rq.alpha_den = params->alpha_den;
+    rq.lbits = params->hard_log2_bits;
+    rq.threads = params->hard_threads;
+    rq.wide = (params->flags & CPX_BATCH_WIDE) != 0;
+    rq.graph = (params->flags & CPX_BATCH_GRAPH) != 0;
+}
+
 int cpx_pi_batch(cpx_ctx *ctx, const cpx_u128 *xs, size_t n, const cpx_params *params, cpx_u128 *out)
 {
     return guarded(ctx, [&] {
@@ -377,17 +391,36 @@ int cpx_pi_batch(cpx_ctx *ctx, const cpx_u128 *xs, size_t n, const cpx_params *p
         BatchReq rq;
         rq.xs = xv.data();
         rq.n = n;
-        if (params) {
-            rq.c = params->c ? params->c : 6;
-            rq.alpha_num = params->alpha_num;
-            rq.alpha_den = params->alpha_den;
-            rq.lbits = params->hard_log2_bits;
-            rq.threads = params->hard_threads;
-        }
+        apply_params(rq, params);
         rq.terms = TERM_PI;
         rq.out_pi = pv.data();
         run_batch(ctx, rq);
         for (size_t i = 0; i < n; i++) out[i] = C128(pv[i]);
+    });
+}
+
+int cpx_terms_batch(cpx_ctx *ctx, const cpx_u128 *xs, const uint64_t *ys, size_t n, const cpx_params *params,
+                    cpx_terms *out)
+{
+    return guarded(ctx, [&] {
+        if (!xs || !out) fail(CPX_EINVAL, "null buffer");
+        std::vector<u128> xv(n);
+        std::vector<uint64_t> yv(n, 0), yu(n, 0);
+        for (size_t i = 0; i < n; i++) {
+            xv[i] = U(xs[i]);
+            if (ys) yv[i] = ys[i];
+        }
+        std::vector<i128> t((size_t)n * 7);
+        BatchReq rq;
+        rq.xs = xv.data();
+        rq.ys = yv.data();
+        rq.n = n;
+        apply_params(rq, params);
+        rq.terms = TERM_PI;
+        rq.out_terms = t.data();
+        rq.out_y = yu.data();
+        run_batch(ctx, rq);
+        for (size_t i = 0; i < n; i++) fill_terms(out + i, xv[i], yu[i], rq.c, t.data() + 7 * i);
     });
 }
 

@@ -104,6 +104,8 @@ struct cpx_ctx {
     cudaEvent_t ev_b0 = nullptr, ev_b1 = nullptr;  // around a batch's kernels
     cudaEvent_t ev_t0 = nullptr, ev_t1 = nullptr;  // caller stopwatch
     float last_batch_ms = 0.f;
+    cudaGraphExec_t graph_exec = nullptr;  // the batch kernels of CPX_BATCH_GRAPH
+    uint64_t graph_builds = 0, graph_updates = 0;
     uint64_t last_h2d = 0, last_d2h = 0;  // bytes copied by the last batch
     double last_hard_bytes = 0.0;
     uint64_t launches = 0;  // kernels launched by this context
@@ -124,6 +126,8 @@ uint64_t build_pitable_window(cpx_ctx *ctx, uint64_t w0, uint64_t nwords, cpx_pi
 
 // exclusive scan of n uint64 values in place (device)
 void scan_u64(cpx_ctx *ctx, uint64_t *d, uint64_t n);
+// grows the scan's block-sum buffers for n values ahead of a graph capture
+void scan_reserve(cpx_ctx *ctx, uint64_t n);
 
 // Extract primes from table words [w0, w1) whose value is in [lo, hi).
 uint64_t extract_primes_u64(cpx_ctx *ctx, uint64_t lo, uint64_t hi, uint64_t *d_out, uint64_t cap);

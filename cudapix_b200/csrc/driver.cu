@@ -124,6 +124,50 @@ static void choose_lbits(cpx_ctx *ctx, std::vector<QD> &qd, uint32_t c, uint32_t
         if (nat[i]) qd[i].lbits = std::min(nat[i], cap);
 }
 
+// Captures the launches of one batch into a CUDA graph and runs it.  The
+// executable graph is kept in the context: a later batch with the same kernel
+// sequence only updates its nodes' parameters (grids, pointers) in place, a
+// different sequence rebuilds it.
+template <class F> static void launch_as_graph(cpx_ctx *ctx, F &&launches)
+{
+    CPX_CUDA(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
+    try {
+        launches();
+    } catch (...) {
+        cudaGraph_t g = nullptr;
+        cudaStreamEndCapture(ctx->stream, &g);
+        if (g) cudaGraphDestroy(g);
+        cudaGetLastError();
+        throw;
+    }
+    cudaGraph_t g = nullptr;
+    CPX_CUDA(cudaStreamEndCapture(ctx->stream, &g));
+    bool updated = false;
+    if (ctx->graph_exec) {
+        cudaGraphExecUpdateResultInfo info;
+        if (cudaGraphExecUpdate(ctx->graph_exec, g, &info) == cudaSuccess) {
+            updated = true;
+        } else {
+            cudaGetLastError();
+            cudaGraphExecDestroy(ctx->graph_exec);
+            ctx->graph_exec = nullptr;
+        }
+    }
+    if (!updated) {
+        const cudaError_t e = cudaGraphInstantiate(&ctx->graph_exec, g, 0);
+        if (e != cudaSuccess) {
+            cudaGraphDestroy(g);
+            ctx->graph_exec = nullptr;
+            check_cuda(e, "cudaGraphInstantiate");
+        }
+        ctx->graph_builds++;
+    } else {
+        ctx->graph_updates++;
+    }
+    cudaGraphDestroy(g);
+    CPX_CUDA(cudaGraphLaunch(ctx->graph_exec, ctx->stream));
+}
+
 void run_batch(cpx_ctx *ctx, const BatchReq &rq)
 {
     const uint32_t Q = (uint32_t)rq.n;
@@ -137,7 +181,7 @@ void run_batch(cpx_ctx *ctx, const BatchReq &rq)
     // ---- host planning: roots, y, validity, table bounds
     std::vector<QD> qd(Q);
     uint64_t N = 1 << 16, Y = 0, Pneed = 64;
-    bool wide = false;
+    bool wide = rq.wide;
     for (uint32_t i = 0; i < Q; i++) {
         QD &d = qd[i];
         memset(&d, 0, sizeof(d));
@@ -318,6 +362,12 @@ void run_batch(cpx_ctx *ctx, const BatchReq &rq)
         pl.job_units = ctl + 1;
         pl.snap = static_cast<unsigned char *>(ctx->b_snap.get(pl.max_jobs * stride));
     }
+    if (pl.n_easy) pl.easy_off = ctx->b_work[7].as<uint64_t>(pl.n_easy + 1);
+    // every buffer the launches touch exists before the first launch (no
+    // allocation between kernels, so the sequence can be captured in a graph)
+    scan_reserve(ctx, std::max<uint64_t>(pl.n_seg, pl.n_easy + 1));
+    pl.time_hard = ctx->timing && !rq.graph;
+    if (mask & TERM_HARD) prepare_hard(ctx, pl);
     u128 *d_out = ctx->b_work[6].as<u128>(Q);
 
     // one staging copy host -> device
@@ -329,16 +379,20 @@ void run_batch(cpx_ctx *ctx, const BatchReq &rq)
     CPX_CUDA(cudaMemsetAsync(d_acc, 0, acc_words * 8, ctx->stream));
 
     // ---- kernels
+    auto launch_all = [&] {
+        if (mask & TERM_ORD) launch_ordinary(ctx, pl);
+        if (mask & TERM_P2) launch_p2(ctx, pl);
+        if (mask & TERM_TRIV) launch_trivial(ctx, pl);
+        if (mask & TERM_EASY) {
+            launch_easy(ctx, pl);
+            launch_easy_comp(ctx, pl);
+        }
+        if (mask & TERM_HARD) launch_hard(ctx, pl);
+        launch_finalize(ctx, pl, d_out, mask == TERM_PI);
+    };
     if (ctx->timing) CPX_CUDA(cudaEventRecord(ctx->ev_b0, ctx->stream));
-    if (mask & TERM_ORD) launch_ordinary(ctx, pl);
-    if (mask & TERM_P2) launch_p2(ctx, pl);
-    if (mask & TERM_TRIV) launch_trivial(ctx, pl);
-    if (mask & TERM_EASY) {
-        launch_easy(ctx, pl);
-        launch_easy_comp(ctx, pl);
-    }
-    if (mask & TERM_HARD) launch_hard(ctx, pl);
-    launch_finalize(ctx, pl, d_out, mask == TERM_PI);
+    if (rq.graph) launch_as_graph(ctx, launch_all);
+    else launch_all();
     if (ctx->timing) CPX_CUDA(cudaEventRecord(ctx->ev_b1, ctx->stream));
 
     // ---- results
@@ -364,7 +418,7 @@ void run_batch(cpx_ctx *ctx, const BatchReq &rq)
         if (rq.out_y) rq.out_y[i] = qd[i].y;
     }
     if (ctx->timing) CPX_CUDA(cudaEventElapsedTime(&ctx->last_batch_ms, ctx->ev_b0, ctx->ev_b1));
-    if (ctx->timing && pl.n_seg) {
+    if (pl.time_hard && pl.n_seg) {
         float ms = 0.f;
         CPX_CUDA(cudaEventElapsedTime(&ms, ctx->ev_hard0, ctx->ev_hard1));
         ctx->last_hard_ms = ms;

@@ -25,6 +25,8 @@ struct BatchReq {
     u128 *out_pi = nullptr;                 // n entries
     i128 *out_terms = nullptr;              // 7 per query: P2 ord triv easy hard pi_y pi
     uint64_t *out_y = nullptr;
+    bool wide = false;   // 128-bit kernels even when every x < 2^64
+    bool graph = false;  // one CUDA graph launch for the batch's kernels
 };
 
 void run_batch(cpx_ctx *ctx, const BatchReq &rq);

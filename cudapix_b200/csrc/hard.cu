@@ -659,8 +659,7 @@ template <class XT> static void hard_go(cpx_ctx *ctx, const Plan &pl)
     scan_u64(ctx, pl.seg_off, pl.n_seg);
     const size_t smem = hard_smem(pl.lbits_max, pl.hard_threads);
     const uint32_t lbits_sub = pl.lbits_max - (uint32_t)(__builtin_ctz(pl.hard_threads) - 5);
-    CPX_CUDA(cudaFuncSetAttribute(k_hard<XT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    if (ctx->timing) CPX_CUDA(cudaEventRecord(ctx->ev_hard0, ctx->stream));
+    if (pl.time_hard) CPX_CUDA(cudaEventRecord(ctx->ev_hard0, ctx->stream));
     if (pl.max_jobs) CPX_CUDA(cudaMemsetAsync(pl.njobs, 0, sizeof(unsigned int), ctx->stream));
     k_hard<XT><<<(unsigned)pl.n_seg, pl.hard_threads, smem, ctx->stream>>>(
         pl.qd, pl.Q, pl.pre_seg, pl.n_seg, pl.seg_B, pl.seg_off, tb.P, tb.MU, tb.T, pl.hard_cnt, pl.hard_ms,
@@ -676,7 +675,7 @@ template <class XT> static void hard_go(cpx_ctx *ctx, const Plan &pl)
         CPX_LAUNCH("k_hard_leaves");
         note_launch(ctx, 2);
     }
-    if (ctx->timing) CPX_CUDA(cudaEventRecord(ctx->ev_hard1, ctx->stream));
+    if (pl.time_hard) CPX_CUDA(cudaEventRecord(ctx->ev_hard1, ctx->stream));
     if (pl.n_comb) {
         k_hard_combine<<<(unsigned)((pl.n_comb + 255) / 256), 256, 0, ctx->stream>>>(
             pl.qd, pl.Q, pl.pre_comb, pl.n_comb, pl.pre_seg, pl.seg_B, pl.seg_off, pl.hard_cnt, pl.hard_ms,
@@ -684,6 +683,15 @@ template <class XT> static void hard_go(cpx_ctx *ctx, const Plan &pl)
         CPX_LAUNCH("k_hard_combine");
         note_launch(ctx);
     }
+}
+
+void prepare_hard(cpx_ctx *ctx, const Plan &pl)
+{
+    (void)ctx;
+    if (!pl.n_seg) return;
+    const int smem = (int)hard_smem(pl.lbits_max, pl.hard_threads);
+    if (pl.wide) CPX_CUDA(cudaFuncSetAttribute(k_hard<u128>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    else CPX_CUDA(cudaFuncSetAttribute(k_hard<uint64_t>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
 }
 
 void launch_hard(cpx_ctx *ctx, const Plan &pl)

@@ -107,6 +107,16 @@ static void scan_u64_rec(cpx_ctx *ctx, uint64_t *d, uint64_t n, int depth)
 
 void scan_u64(cpx_ctx *ctx, uint64_t *d, uint64_t n) { scan_u64_rec(ctx, d, n, 0); }
 
+void scan_reserve(cpx_ctx *ctx, uint64_t n)
+{
+    for (int depth = 0; depth < 3 && n > 0; depth++) {
+        const uint64_t nb = (n + kScanBlock - 1) / kScanBlock;
+        ctx->b_scan[depth].as<uint64_t>(nb + 1);
+        if (nb <= 1) break;
+        n = nb;
+    }
+}
+
 // ---------------------------------------------------- bootstrap: trial division
 
 // Table entries for [0, 65536) by trial division (one entry per thread, one

@@ -441,7 +441,7 @@ void launch_trivial(cpx_ctx *ctx, const Plan &pl)
 void launch_easy(cpx_ctx *ctx, const Plan &pl)
 {
     if (!pl.n_easy) return;
-    uint64_t *off = ctx->b_work[7].as<uint64_t>(pl.n_easy + 1);
+    uint64_t *off = pl.easy_off;
     const unsigned gc = (unsigned)((pl.n_easy + 1 + 255) / 256);
     if (pl.wide)
         k_easy_count<u128><<<gc, 256, 0, ctx->stream>>>(pl.qd, pl.Q, pl.pre_easy, pl.n_easy, ctx->tab.T, off);

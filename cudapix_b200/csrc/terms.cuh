@@ -48,7 +48,8 @@ struct Plan {
     uint64_t n_ord = 0, n_p2 = 0, n_triv = 0, n_easy = 0, n_seg = 0, n_comb = 0;
     uint64_t hard_entries = 0;
     uint32_t c = 6;
-    bool wide = false;  // some x >= 2^64
+    bool wide = false;  // 128-bit kernels (some x >= 2^64, or requested)
+    bool time_hard = false;  // CUDA events around the hard-leaf kernels
     uint32_t hard_threads = 256;
     uint32_t lbits_max = 18;
     // device work arrays
@@ -68,6 +69,7 @@ struct Plan {
     const EasyLvl *elv = nullptr;
     uint32_t n_elv = 0;
     uint64_t n_ecomp = 0;
+    uint64_t *easy_off = nullptr;  // n_easy + 1 chunk offsets of the easy leaves
 };
 
 void launch_ordinary(cpx_ctx *ctx, const Plan &pl);
@@ -78,6 +80,9 @@ void launch_easy_comp(cpx_ctx *ctx, const Plan &pl);
 void launch_hard(cpx_ctx *ctx, const Plan &pl);
 void launch_finalize(cpx_ctx *ctx, const Plan &pl, u128 *d_out_pi, bool full);
 size_t hard_smem_bytes(uint32_t lbits, uint32_t threads, bool wide);
+// host-side set-up of the hard-leaf kernels (kernel attributes); called
+// before the launches so that they can be captured in a graph
+void prepare_hard(cpx_ctx *ctx, const Plan &pl);
 size_t hard_snapshot_stride(uint32_t lbits_max);
 
 }  // namespace cpx

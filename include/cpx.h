@@ -194,18 +194,30 @@ int cpx_phisieve_update(cpx_phisieve *ps);
 int cpx_phisieve_counts(cpx_phisieve *ps, uint32_t **d_counts, uint32_t *a_current);
 
 /* ---- batched and served evaluation -------------------------------------- */
+/* cpx_params.flags */
+#define CPX_BATCH_WIDE 1u  /* 128-bit kernels for every query, also when all x < 2^64 */
+#define CPX_BATCH_GRAPH 2u /* run the batch's kernels as one CUDA graph launch (the
+                              graph is kept in the context and updated in place) */
+
 typedef struct {
     uint32_t alpha_num, alpha_den; /* y rule; 0/0 = reference alpha(x) */
     uint16_t c;                    /* pre-sieve primes, default 6 */
-    uint16_t pad;
+    uint16_t flags;                /* CPX_BATCH_* */
     uint32_t hard_log2_bits;       /* 0 = context default */
     uint32_t hard_threads;         /* 0 = context default */
 } cpx_params;
 
 /* pi(x_i) for n queries in one batched device pass over shared tables sized
- * to the largest query.  out[i] = pi(x_i). */
+ * to the largest query.  out[i] = pi(x_i).  No reference counterpart: the
+ * reference evaluates one x per deleglise_rivat64/128 object
+ * (src/deleglise-rivat.cpp:13-80). */
 int cpx_pi_batch(cpx_ctx *ctx, const cpx_u128 *xs, size_t n, const cpx_params *params,
                  cpx_u128 *out);
+
+/* Every term for n queries in one batched pass; ys[i] = 0 (or ys = NULL)
+ * selects the y rule of params.  out[i] as filled by cpx_pi_u128. */
+int cpx_terms_batch(cpx_ctx *ctx, const cpx_u128 *xs, const uint64_t *ys, size_t n,
+                    const cpx_params *params, cpx_terms *out);
 
 #ifdef __cplusplus
 }

@@ -62,6 +62,23 @@ def test_segment_params_do_not_change_results(ctx, cpx, orc):
     ctx.set_hard_params(18, 256)
 
 
+@pytest.mark.parametrize("x,y", [(10**9, 10**4), (10**10, 30000), (10**11, 92830), (10**12, 10**5)])
+def test_hard_offload_threshold_does_not_change_results(ctx, cpx, orc, x, y):
+    """Leaf sets answered by k_hard_leaves from snapshots (threshold 1 sends
+    nearly every level there, 0 keeps every leaf in the sieve) give the same
+    hard sum, for every block size."""
+    ref = orc.hard(x, y)
+    try:
+        for off in (0, 1, 64, 1024):
+            ctx.set_hard_offload(off)
+            for th in (128, 256, 512):
+                ctx.set_hard_params(18, th)
+                assert cpx.S2hard(x, y, 6, ctx=ctx) == ref, (off, th)
+    finally:
+        ctx.set_hard_offload(1024)
+        ctx.set_hard_params(18, 256)
+
+
 def test_edge_y_bounds(ctx, cpx, orc):
     """y at the ends of the domain: y = icbrt(x) and y = isqrt(x) - 1."""
     for x in (10**10 + 1, 3 * 10**11, 2**36 - 1):
@@ -100,3 +117,39 @@ def test_invalid_arguments(ctx, cpx):
         cpx.pi_deleglise_rivat(10**12, 10**3, 6, ctx=ctx)  # y below cbrt(x)
     with pytest.raises(cpx.CpxError):
         ctx.set_hard_params(21, 256)
+
+
+def test_wide_kernels_match_oracle(ctx, cpx, orc):
+    """The 128-bit kernels (u128 quotients, 128-bit accumulators) on x < 2^64,
+    every term against the oracle, in one batch with per-query y."""
+    cases = CASES + [(10**14, 600000), (3 * 10**13 + 7, 250001)]
+    got = cpx.terms_batch([x for x, _ in cases], [y for _, y in cases], wide=True, ctx=ctx)
+    for (x, y), t in zip(cases, got):
+        o = orc.pi_dr(x, y, 6)
+        for k in ("P2", "ordinary", "trivial", "easy", "hard", "pi_y", "pi"):
+            assert t[k] == o[k], (k, x, y, t[k], o[k])
+
+
+def test_wide_batch_equals_narrow(ctx, cpx):
+    rng = np.random.default_rng(11)
+    xs = [int(10**e) for e in rng.uniform(6, 13, 200)]
+    assert cpx.pi_batch(xs, ctx=ctx, wide=True) == cpx.pi_batch(xs, ctx=ctx)
+
+
+def test_terms_batch_equals_single(ctx, cpx):
+    xs = [10**9 + 7, 10**11, 2**40 + 15, 10**12]
+    ys = [0, 46415 * 2, 10**5 + 3, 0]
+    got = cpx.terms_batch(xs, ys, ctx=ctx)
+    for x, y, t in zip(xs, ys, got):
+        assert t == cpx.pi_terms(x, y, 6, ctx=ctx), x
+
+
+def test_graph_batches_equal_direct_launches(ctx, cpx, golden):
+    """CUDA-graph batches: the first builds the graph, later ones of other
+    sizes update it in place; every result equals the direct launches'."""
+    rng = np.random.default_rng(3)
+    for n, hi in ((300, 12), (57, 13.5), (300, 11), (1, 9)):
+        xs = [int(10**e) for e in rng.uniform(6, hi, n)]
+        assert cpx.pi_batch(xs, ctx=ctx, graph=True) == cpx.pi_batch(xs, ctx=ctx), (n, hi)
+    pw = [10**k for k in range(1, 16)]
+    assert cpx.pi_batch(pw, ctx=ctx, graph=True) == [golden["pi_pow10"][str(k)] for k in range(1, 16)]
