@@ -91,6 +91,32 @@ __device__ __forceinline__ uint64_t cpx_pi_dev(const cpx_pient *__restrict__ T, 
     return cpx_pi_from_entry(e, n);
 }
 
+// ------------------------------------------------ leaf quotients floor(n / d)
+// Leaves divide a fixed x/p by many m < 2^32 with quotients below 2^44.  The
+// quotient is taken from the double product n * (1/d) and made exact by one
+// integer correction, instead of the general 64-bit division routine:
+//   r0 = 1/d rounded to float, then one Newton-Raphson step in double
+//   rd = r0 + r0 (1 - d r0), relative error < 2^-45;
+//   v = n * rd is within 0.15 of n/d when n/d < 2^44, so trunc(v) is
+//   floor(n/d) - 1, floor(n/d) or floor(n/d) + 1, and the sign of
+//   n - trunc(v) d settles which.  Other operands use the hardware path.
+__device__ __forceinline__ uint64_t cpx_udiv_leaf(uint64_t n, uint64_t d)
+{
+    if ((d >> 32) || (n >> 44) >= d) return n / d;
+    const uint32_t d32 = (uint32_t)d;
+    const double r = (double)__frcp_rn(__uint2float_rn(d32));
+    const double dd = (double)d32;
+    const double e = __fma_rn(-dd, r, 1.0);
+    const double rd = __fma_rn(r, e, r);
+    uint64_t u = __double2ull_rz(__dmul_rn(__ull2double_rn(n), rd));
+    const int64_t rem = (int64_t)(n - u * d);
+    if (rem < 0) u--;
+    else if (rem >= (int64_t)d) u++;
+    return u;
+}
+__device__ __forceinline__ uint64_t cpx_qdiv(uint64_t n, uint64_t d) { return cpx_udiv_leaf(n, d); }
+__device__ __forceinline__ u128 cpx_qdiv(u128 n, uint64_t d) { return n / (u128)d; }
+
 // ------------------------------------------------ 128-bit atomic accumulate
 // Two 64-bit atomics; the carry out of the low word is added to the high word
 // by the same thread, which makes the final 128-bit total exact in any order.

@@ -88,6 +88,63 @@ static uint64_t segments_at_level(u128 x, uint64_t span, uint64_t p, uint64_t ns
     return hi >= first ? (uint64_t)(hi - first + 1) : 0;
 }
 
+// Number of (sub-segment, level) leaf sets of one query that k_hard hands to
+// k_hard_leaves at threshold thr: the same candidate bounds as k_hard's warps
+// (m in (max(y/p, xp/hi_w), min(y, xp/lo_w, x/p^3)], prime m only when
+// p^2 > y).  Along a level the candidate count rises while the sub-segments
+// reach into the leaves' smallest u and falls once xp/lo_w is the upper
+// bound, so each level is scanned from its first sub-segment with leaves to
+// the first light one past that point.  Stops counting at `limit`.
+template <class XT>
+static uint64_t heavy_leaf_sets(const QD &d, const std::vector<uint32_t> &hP, uint32_t threads, uint64_t thr,
+                                uint64_t limit)
+{
+    const uint64_t NW = threads / 32, Lw = (1ull << d.lbits) / NW, span_w = 2 * Lw;
+    const uint64_t nsub = d.nseg * NW, L2 = 2ull << d.lbits;
+    const XT x = (XT)d.x;
+    const uint64_t y = d.y;
+    uint64_t jobs = 0;
+    for (uint32_t b = d.c + 1; b <= d.nb && jobs < limit; b++) {
+        const uint64_t p = hP[b - 1];
+        const XT xp = x / (XT)p;
+        const XT x3 = xp / (XT)(p * p);
+        const uint64_t mtop = x3 < (XT)y ? (uint64_t)x3 : y;
+        if (mtop <= y / p) continue;
+        const bool prime_lvl = p * p > y;
+        for (uint64_t w = (uint64_t)(xp / (XT)mtop) / span_w; w < nsub; w++) {
+            const uint64_t lo_w = w * span_w, hi_w = lo_w + span_w;
+            const uint64_t lo = (w / NW) * L2;
+            if ((u128)p * p > (u128)(lo + L2 - 1) || (lo && (u128)p * p > (u128)((x - 1) / (XT)lo))) continue;
+            uint64_t mlo = y / p;
+            const XT t1 = xp / (XT)hi_w;
+            if (t1 > (XT)mlo) mlo = (uint64_t)t1;
+            uint64_t mhi = mtop;
+            bool interior = false;
+            if (lo_w) {
+                const XT t2 = xp / (XT)lo_w;
+                if (t2 < (XT)mhi) {
+                    mhi = (uint64_t)t2;
+                    interior = true;
+                }
+            }
+            if (mhi <= mlo) {
+                if (interior) break;
+                continue;
+            }
+            uint64_t work;
+            const uint64_t qa = mlo > p ? mlo : p;
+            if (prime_lvl) work = (mhi > qa) ? 8 * (((mhi - 1) >> 7) - (qa >> 7) + 1) : 0;
+            else work = ((mhi - 1) >> 1) - ((mlo + 1) >> 1) + 1;
+            if (work >= thr) {
+                if (++jobs >= limit) break;
+            } else if (interior) {
+                break;
+            }
+        }
+    }
+    return jobs;
+}
+
 // Hard-leaf segment sizes for a batch.  A query never gets a segment longer
 // than needed to cover [0, z]; below the context default the sizes of the
 // largest queries shrink (one cap for all) until the whole batch has about
@@ -353,14 +410,29 @@ void run_batch(cpx_ctx *ctx, const BatchReq &rq)
         pl.seg_off = ctx->b_work[3].as<uint64_t>(pl.n_seg + 1);
         pl.hard_cnt = ctx->b_work[4].as<uint32_t>(hard_entries + 1);
         pl.hard_ms = ctx->b_work[5].as<int32_t>(hard_entries + 1);
-        // snapshot pool for heavy (segment, level) leaf sets: at most 8192 slots and 512 MiB
+        // snapshot pool for the heavy (sub-segment, level) leaf sets, counted on
+        // the host; the threshold doubles until the pool fits the budget
         const size_t stride = hard_snapshot_stride(lbits_max - (uint32_t)(__builtin_ctz(threads) - 5));
-        pl.max_jobs = (uint32_t)std::min<size_t>(8192, (size_t(512) << 20) / stride);
-        pl.jobs = ctx->b_jobs.as<HardJob>(pl.max_jobs);
+        const uint64_t budget = std::max<uint64_t>(1, ctx->hard_offload_bytes / (stride + sizeof(HardJob)));
+        uint64_t thr = ctx->hard_offload_min, njobs = 0;
+        while (thr) {
+            njobs = 0;
+            for (const QD &d : qd) {
+                if (d.direct || d.nb <= c) continue;
+                njobs += wide ? heavy_leaf_sets<u128>(d, hP, threads, thr, budget + 1 - njobs)
+                              : heavy_leaf_sets<uint64_t>(d, hP, threads, thr, budget + 1 - njobs);
+                if (njobs > budget) break;
+            }
+            if (njobs <= budget) break;
+            thr = (thr >= (1ull << 40)) ? 0 : 2 * thr;
+        }
+        pl.offload_min = thr;
+        pl.max_jobs = thr ? (uint32_t)std::min<uint64_t>(njobs + 64, 0xFFFFFFF0ull) : 0;
+        pl.jobs = ctx->b_jobs.as<HardJob>(pl.max_jobs + 1);
         uint64_t *ctl = ctx->b_jobctl.as<uint64_t>(4);
         pl.njobs = reinterpret_cast<unsigned int *>(ctl);
         pl.job_units = ctl + 1;
-        pl.snap = static_cast<unsigned char *>(ctx->b_snap.get(pl.max_jobs * stride));
+        pl.snap = static_cast<unsigned char *>(ctx->b_snap.get((pl.max_jobs + 1) * stride));
     }
     if (pl.n_easy) pl.easy_off = ctx->b_work[7].as<uint64_t>(pl.n_easy + 1);
     // every buffer the launches touch exists before the first launch (no

@@ -99,7 +99,7 @@ __host__ __device__ __forceinline__ size_t hard_smem(uint32_t lbits, uint32_t th
 }
 
 template <class XT>
-__global__ void __launch_bounds__(512) k_hard(const QD *__restrict__ qd, uint32_t Q,
+__global__ void __launch_bounds__(512, 2) k_hard(const QD *__restrict__ qd, uint32_t Q,
                                               const uint64_t *__restrict__ pre_seg, uint64_t total,
                                               const uint32_t *__restrict__ seg_B,
                                               const uint64_t *__restrict__ seg_off,
@@ -322,7 +322,7 @@ __global__ void __launch_bounds__(512) k_hard(const QD *__restrict__ qd, uint32_
                                     const int j = __ffsll((long long)qb) - 1;
                                     qb &= qb - 1;
                                     const uint64_t m = 128 * wq + 2 * j + 1;
-                                    S += sub_count((uint64_t)(xp / (XT)m));  // mu(q) = -1
+                                    S += sub_count((uint64_t)cpx_qdiv(xp, m));  // mu(q) = -1
                                     msl += 1;
                                 }
                             }
@@ -339,7 +339,7 @@ __global__ void __launch_bounds__(512) k_hard(const QD *__restrict__ qd, uint32_
                                 const int32_t v = vals[kq];
                                 if (i < i_lo || i > i_hi || v == 0) continue;
                                 if ((uint32_t)(v > 0 ? v : -v) <= p) continue;
-                                const uint32_t cv = sub_count((uint64_t)(xp / (XT)(2 * i + 1)));
+                                const uint32_t cv = sub_count((uint64_t)cpx_qdiv(xp, 2 * i + 1));
                                 if (v > 0) {
                                     S -= cv;
                                     msl -= 1;
@@ -520,7 +520,7 @@ __global__ void __launch_bounds__(kThreads) k_hard_leaves(const HardJob *__restr
                 while (qb) {
                     const int j = __ffsll((long long)qb) - 1;
                     qb &= qb - 1;
-                    S += count((uint64_t)(xp / (XT)(128 * wq + 2 * j + 1)));  // mu(q) = -1
+                    S += count((uint64_t)cpx_qdiv(xp, 128 * wq + 2 * j + 1));  // mu(q) = -1
                     ms += 1;
                 }
             }
@@ -539,7 +539,7 @@ __global__ void __launch_bounds__(kThreads) k_hard_leaves(const HardJob *__restr
                     const int32_t v = vals[kq];
                     if (i < i_lo || i > i_hi || v == 0) continue;
                     if ((uint32_t)(v > 0 ? v : -v) <= p) continue;
-                    const uint32_t cv = count((uint64_t)(xp / (XT)(2 * i + 1)));
+                    const uint32_t cv = count((uint64_t)cpx_qdiv(xp, 2 * i + 1));
                     if (v > 0) {
                         S -= cv;
                         ms -= 1;
@@ -664,7 +664,7 @@ template <class XT> static void hard_go(cpx_ctx *ctx, const Plan &pl)
     k_hard<XT><<<(unsigned)pl.n_seg, pl.hard_threads, smem, ctx->stream>>>(
         pl.qd, pl.Q, pl.pre_seg, pl.n_seg, pl.seg_B, pl.seg_off, tb.P, tb.MU, tb.T, pl.hard_cnt, pl.hard_ms,
         pl.hard_entries, pl.acc, pl.lbits_max, pl.jobs, pl.njobs, pl.snap, pl.max_jobs, lbits_sub,
-        ctx->hard_offload_min);
+        (uint32_t)std::min<uint64_t>(pl.offload_min, 0xFFFFFFFFull));
     CPX_LAUNCH("k_hard");
     note_launch(ctx);
     if (pl.max_jobs) {

@@ -107,7 +107,7 @@ __global__ void __launch_bounds__(kThreads) k_p2(const QD *__restrict__ qd, uint
                 bits &= bits - 1;
                 const uint64_t p = 128 * w + 2 * j + 1;
                 const uint64_t i = 1 + e.y + __popcll(e.x & ((2ull << j) - 1));  // pi(p)
-                const uint64_t xp = (uint64_t)(x / (XT)p);
+                const uint64_t xp = (uint64_t)cpx_qdiv(x, p);
                 s += (int64_t)cpx_pi_dev(T, xp) - (int64_t)i + 1;
             }
             a.v += s;
@@ -282,7 +282,7 @@ __global__ void __launch_bounds__(kThreads) k_easy(const QD *__restrict__ qd, ui
             while (qb) {
                 const int j2 = __ffsll((long long)qb) - 1;
                 qb &= qb - 1;
-                const uint64_t uu = (uint64_t)(xp / (XT)(128 * wq + 2 * j2 + 1));
+                const uint64_t uu = (uint64_t)cpx_qdiv(xp, 128 * wq + 2 * j2 + 1);
                 ps += cpx_pi_dev(T, uu);
                 cnt++;
             }
@@ -331,7 +331,7 @@ __global__ void __launch_bounds__(kThreads) k_easy_comp(const QD *__restrict__ q
                 const uint64_t m = 2 * i + 1;
                 const uint32_t av = (uint32_t)(v > 0 ? v : -v);
                 if (v == 0 || av <= r.p || (uint64_t)av >= m) continue;  // mu = 0, lpf <= p, or m prime
-                const uint64_t uu = (uint64_t)(xp / (XT)m);
+                const uint64_t uu = (uint64_t)cpx_qdiv(xp, m);
                 const int64_t val = (int64_t)cpx_pi_dev(T, uu) - (int64_t)r.b + 2;
                 s += (v > 0) ? -val : val;
             }

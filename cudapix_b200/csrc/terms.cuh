@@ -65,6 +65,7 @@ struct Plan {
     uint64_t *job_units = nullptr;   // device: total work units after the scan
     unsigned char *snap = nullptr;   // snapshot slots
     uint32_t max_jobs = 0;
+    uint64_t offload_min = 0;        // candidate threshold of an offloaded leaf set (0: none)
     // composite easy leaves
     const EasyLvl *elv = nullptr;
     uint32_t n_elv = 0;
