@@ -79,6 +79,15 @@ bool dr_domain_ok(u128 x, uint64_t y, uint32_t c)
 
 // Segments (of `span` integers) that sieve level b, p = p_b: those with
 // hi > p^2 and (lo = 0 or p^2 lo < x); the same rule as k_hard_plan.
+// An upper bound of x^(2/5), at most 2^31: the u primes an easy leaf's
+// clustered part needs (the kernels fall back to single leaves above the
+// resident prime list, so the bound only has to be close).
+static uint64_t easy_u_bound(u128 x)
+{
+    const long double v = powl((long double)x, 0.4L) * 1.001L + 16.0L;
+    return v >= 2147483648.0L ? 2147483648ull : (uint64_t)v;
+}
+
 static uint64_t segments_at_level(u128 x, uint64_t span, uint64_t p, uint64_t nseg)
 {
     const u128 p2 = (u128)p * p;
@@ -280,7 +289,9 @@ void run_batch(cpx_ctx *ctx, const BatchReq &rq)
             N = std::max<uint64_t>(N, std::max<uint64_t>(r4 * r4 + 2, y + 1));
         }
         if (mask & TERM_EASY) {
-            Pneed = std::max<uint64_t>(Pneed, r4 + 1);  // composite easy leaves: p_b <= iroot4(x)
+            // the p of the easy leaves (p <= icbrt(x)) and the u primes of their
+            // clustered parts (u <= min(p^2, sqrt(x/p)) <= x^(2/5))
+            Pneed = std::max<uint64_t>(Pneed, std::max<uint64_t>(cx + 1, easy_u_bound(x)));
             Y = std::max(Y, y);
         }
         if (mask == TERM_PI) N = std::max<uint64_t>(N, y + 1);
@@ -320,7 +331,7 @@ void run_batch(cpx_ctx *ctx, const BatchReq &rq)
             if (mask & TERM_ORD) n_ord = ((d.y + 1) / 2 + 3) / 4;
             if ((mask & TERM_P2) && d.sx > d.y) n_p2 = ((d.sx - 1) >> 7) - (d.y >> 7) + 1;
             if (mask & TERM_TRIV) n_triv = (d.cx > d.tx) ? ((d.cx - 1) >> 7) - (d.tx >> 7) + 1 : 1;
-            if ((mask & TERM_EASY) && d.cx > pc) n_easy = ((d.cx - 1) >> 7) - (pc >> 7) + 1;
+            if ((mask & TERM_EASY) && d.cx > pc) n_easy = host_pi(hP, d.cx) - c;  // primes p_c < p <= icbrt(x)
             if (mask & TERM_EASY) {
                 // composite easy leaves: levels b with p_b <= iroot4(x), p_b^2 < y and
                 // max(y/p_b, x/p_b^3) < y
@@ -429,15 +440,15 @@ void run_batch(cpx_ctx *ctx, const BatchReq &rq)
         pl.offload_min = thr;
         pl.max_jobs = thr ? (uint32_t)std::min<uint64_t>(njobs + 64, 0xFFFFFFF0ull) : 0;
         pl.jobs = ctx->b_jobs.as<HardJob>(pl.max_jobs + 1);
-        uint64_t *ctl = ctx->b_jobctl.as<uint64_t>(4);
+        uint64_t *ctl = ctx->b_jobctl.as<uint64_t>(pl.max_jobs + 4);
         pl.njobs = reinterpret_cast<unsigned int *>(ctl);
-        pl.job_units = ctl + 1;
+        pl.job_units = ctl + 2;
         pl.snap = static_cast<unsigned char *>(ctx->b_snap.get((pl.max_jobs + 1) * stride));
     }
     if (pl.n_easy) pl.easy_off = ctx->b_work[7].as<uint64_t>(pl.n_easy + 1);
     // every buffer the launches touch exists before the first launch (no
     // allocation between kernels, so the sequence can be captured in a graph)
-    scan_reserve(ctx, std::max<uint64_t>(pl.n_seg, pl.n_easy + 1));
+    scan_reserve(ctx, std::max<uint64_t>(std::max<uint64_t>(pl.n_seg, pl.n_easy + 1), (uint64_t)pl.max_jobs + 1));
     pl.time_hard = ctx->timing && !rq.graph;
     if (mask & TERM_HARD) prepare_hard(ctx, pl);
     u128 *d_out = ctx->b_work[6].as<u128>(Q);

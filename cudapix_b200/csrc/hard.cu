@@ -108,8 +108,9 @@ __global__ void __launch_bounds__(512, 2) k_hard(const QD *__restrict__ qd, uint
                                               uint32_t *__restrict__ out_cnt, int32_t *__restrict__ out_ms,
                                               uint64_t cap, unsigned long long *__restrict__ acc,
                                               uint32_t lbits_max, HardJob *__restrict__ jobs,
-                                              unsigned int *__restrict__ njobs, unsigned char *__restrict__ snap,
-                                              uint32_t max_jobs, uint32_t lbits_sub_max, uint32_t offload_min)
+                                              unsigned int *__restrict__ njobs, uint64_t *__restrict__ job_units,
+                                              unsigned char *__restrict__ snap, uint32_t max_jobs,
+                                              uint32_t lbits_sub_max, uint32_t offload_min)
 {
     extern __shared__ uint4 smem4[];
     const uint64_t unit = blockIdx.x;
@@ -301,9 +302,8 @@ __global__ void __launch_bounds__(512, 2) k_hard(const QD *__restrict__ qd, uint
                                                  : (((((uint64_t)mhi - 1) >> 1) >> 2) -
                                                     ((((uint64_t)mlo + 1) >> 1) >> 2) + kJobGroups) /
                                                        kJobGroups;
-                            J.unit0 = 0;
                             J.carry = 0;  // filled in by the group combine below
-                            J.pad = 0;
+                            job_units[j] = J.nunits;
                             J.xp = (u128)xp;
                             jobs[j] = J;
                         }
@@ -430,35 +430,6 @@ __global__ void __launch_bounds__(512, 2) k_hard(const QD *__restrict__ qd, uint
     if (tid == 0) acc_add(acc, q, ACC_HARD, Sb);
 }
 
-// Numbers the offloaded jobs' work units (exclusive scan of nunits in job
-// order); one CTA of 1024 threads.
-__global__ void __launch_bounds__(1024) k_hard_job_scan(HardJob *__restrict__ jobs, const unsigned int *njobs,
-                                                        uint32_t max_jobs, uint64_t *__restrict__ total_units)
-{
-    __shared__ uint64_t wsum[32];
-    const uint32_t n = min(*njobs, max_jobs);
-    const uint32_t t = threadIdx.x, per = (n + 1023) / 1024;
-    const uint32_t a = min(n, t * per), b = min(n, a + per);
-    uint64_t s = 0;
-    for (uint32_t i = a; i < b; i++) s += jobs[i].nunits;
-    uint64_t inc = s;
-    const uint32_t lane = t & 31, w = t >> 5;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-        const uint64_t v = __shfl_up_sync(FULL, inc, o);
-        if (lane >= (uint32_t)o) inc += v;
-    }
-    if (lane == 31) wsum[w] = inc;
-    __syncthreads();
-    uint64_t run = inc - s;
-    for (uint32_t i = 0; i < w; i++) run += wsum[i];
-    for (uint32_t i = a; i < b; i++) {
-        jobs[i].unit0 = run;
-        run += jobs[i].nunits;
-    }
-    if (t == 1023) *total_units = run;
-}
-
 // Leaves of the offloaded (segment, level) sets.  A warp takes one unit: 256
 // pi-table entries of prime m (prime-only levels) or 256 groups of 4 odd m
 // read as packed mu*lpf (other levels).  Each leaf's survivor count is the
@@ -467,7 +438,7 @@ __global__ void __launch_bounds__(1024) k_hard_job_scan(HardJob *__restrict__ jo
 template <class XT>
 __global__ void __launch_bounds__(kThreads) k_hard_leaves(const HardJob *__restrict__ jobs,
                                                           const unsigned int *njobs, uint32_t max_jobs,
-                                                          const uint64_t *total_units,
+                                                          const uint64_t *__restrict__ unit0,
                                                           const unsigned char *__restrict__ snap,
                                                           uint32_t lbits_sub, const int32_t *__restrict__ MU,
                                                           const cpx_pient *__restrict__ Tpi,
@@ -475,21 +446,21 @@ __global__ void __launch_bounds__(kThreads) k_hard_leaves(const HardJob *__restr
                                                           unsigned long long *__restrict__ acc)
 {
     const uint32_t n = min(*njobs, max_jobs);
-    const uint64_t total = *total_units;
+    const uint64_t total = unit0[max_jobs];  // exclusive scan of the units; slots past n hold 0
     const uint32_t lane = threadIdx.x & 31;
     const uint64_t gw = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const uint64_t nw = ((uint64_t)gridDim.x * blockDim.x) >> 5;
     const size_t stride = snap_stride(lbits_sub);
     const size_t ncmax = (size_t(1) << lbits_sub) >> 7;
     for (uint64_t unit = gw; unit < total; unit += nw) {
-        uint32_t lo_j = 0, hi_j = n;  // jobs[lo_j].unit0 <= unit < jobs[hi_j].unit0
+        uint32_t lo_j = 0, hi_j = n;  // unit0[lo_j] <= unit < unit0[hi_j]
         while (hi_j - lo_j > 1) {
             const uint32_t mid = (lo_j + hi_j) >> 1;
-            if (jobs[mid].unit0 <= unit) lo_j = mid;
+            if (__ldg(unit0 + mid) <= unit) lo_j = mid;
             else hi_j = mid;
         }
         const HardJob &J = jobs[lo_j];
-        const uint64_t lu = unit - J.unit0;
+        const uint64_t lu = unit - __ldg(unit0 + lo_j);
         const uint4 *sb = reinterpret_cast<const uint4 *>(snap + (size_t)lo_j * stride);
         const uint32_t *spre = reinterpret_cast<const uint32_t *>(sb + ncmax);
         const XT xp = (XT)J.xp;
@@ -599,8 +570,10 @@ __global__ void k_hard_plan(const QD *__restrict__ qd, uint32_t Q, const uint64_
 // survivors of level b-1 below the segment.  Level b is sieved from the first
 // segment reaching p_b^2; below p_b^2 the survivors of level b-1 are 1 and the
 // primes from p_b on, so the carry starts at 1 + max(0, pi(lo - 1) - (b - 1))
-// from the pi table and then adds the sieved segments' counts.  One thread per
-// (query, b).
+// from the pi table and then adds the sieved segments' counts.  One warp per
+// (query, b): its lanes take 32 consecutive segments at a time and a warp
+// scan of their counts gives each segment its carry.  The segments sieving
+// level b are contiguous from the first one.
 __global__ void k_hard_combine(const QD *__restrict__ qd, uint32_t Q, const uint64_t *__restrict__ pre_comb,
                                uint64_t total, const uint64_t *__restrict__ pre_seg,
                                const uint32_t *__restrict__ seg_B, const uint64_t *__restrict__ seg_off,
@@ -608,35 +581,54 @@ __global__ void k_hard_combine(const QD *__restrict__ qd, uint32_t Q, const uint
                                const uint32_t *__restrict__ P, const cpx_pient *__restrict__ T,
                                unsigned long long *__restrict__ acc)
 {
-    const uint64_t u = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    LaneAcc a;
-    if (u < total) {
-        const uint32_t q = find_q(pre_comb, Q, u);
-        const uint64_t lvl = u - pre_comb[q];
-        const QD &d = qd[q];
-        const uint32_t b = d.c + 1 + (uint32_t)lvl;
-        const uint64_t span = 2ull << d.lbits;
-        const uint64_t p = P[b - 1];
-        const uint64_t first = (p * p) / span;  // first segment with hi > p^2
-        const uint64_t s0 = pre_seg[q] + first, s1 = pre_seg[q + 1];
-        uint64_t carry = 0;
-        if (first > 0 && s0 < s1) {
-            const uint64_t lo = first * span;
-            const uint64_t pl = cpx_pi_dev(T, lo - 1);
-            carry = 1 + (pl > b - 1 ? pl - (b - 1) : 0);
-        }
-        i128 H = 0;
-        for (uint64_t sg = s0; sg < s1; sg++) {
-            if (seg_B[sg] < b) break;
-            const uint64_t idx = seg_off[sg] + lvl;
-            if (idx >= cap) break;
-            H += (i128)carry * (i128)ms[idx];
-            carry += cnt[idx];
-        }
-        a.q = q;
-        a.v = H;
+    const uint64_t u = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const uint32_t lane = threadIdx.x & 31;
+    if (u >= total) return;  // uniform over the warp
+    const uint32_t q = find_q(pre_comb, Q, u);
+    const uint64_t lvl = u - pre_comb[q];
+    const QD &d = qd[q];
+    const uint32_t b = d.c + 1 + (uint32_t)lvl;
+    const uint64_t span = 2ull << d.lbits;
+    const uint64_t p = P[b - 1];
+    const uint64_t first = (p * p) / span;  // first segment with hi > p^2
+    const uint64_t s0 = pre_seg[q] + first, s1 = pre_seg[q + 1];
+    uint64_t carry = 0;
+    if (first > 0 && s0 < s1) {
+        const uint64_t pl = cpx_pi_dev(T, first * span - 1);
+        carry = 1 + (pl > b - 1 ? pl - (b - 1) : 0);
     }
-    warp_flush(a, acc, ACC_HARD);
+    i128 H = 0;
+    for (uint64_t base = s0; base < s1; base += 32) {
+        const uint64_t sg = base + lane;
+        uint32_t cv = 0;
+        int32_t mv = 0;
+        bool act = false;
+        if (sg < s1 && __ldg(seg_B + sg) >= b) {
+            const uint64_t idx = __ldg(seg_off + sg) + lvl;
+            if (idx < cap) {
+                cv = __ldg(cnt + idx);
+                mv = __ldg(ms + idx);
+                act = true;
+            }
+        }
+        const unsigned bal = __ballot_sync(FULL, act);
+        const int stop = __ffs(~bal) - 1;  // first segment past the level's range (-1: none here)
+        if (stop >= 0 && (int)lane >= stop) {
+            cv = 0;
+            mv = 0;
+        }
+        uint64_t inc = cv;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint64_t t = __shfl_up_sync(FULL, inc, o);
+            if (lane >= (uint32_t)o) inc += t;
+        }
+        H += (i128)(carry + inc - cv) * (i128)mv;
+        carry += __shfl_sync(FULL, inc, 31);
+        if (stop >= 0) break;
+    }
+    H = cpx_warp_sum_i128(H);
+    if (lane == 0) acc_add(acc, q, ACC_HARD, H);
 }
 
 // ------------------------------------------------------------------ launchers
@@ -660,24 +652,26 @@ template <class XT> static void hard_go(cpx_ctx *ctx, const Plan &pl)
     const size_t smem = hard_smem(pl.lbits_max, pl.hard_threads);
     const uint32_t lbits_sub = pl.lbits_max - (uint32_t)(__builtin_ctz(pl.hard_threads) - 5);
     if (pl.time_hard) CPX_CUDA(cudaEventRecord(ctx->ev_hard0, ctx->stream));
-    if (pl.max_jobs) CPX_CUDA(cudaMemsetAsync(pl.njobs, 0, sizeof(unsigned int), ctx->stream));
+    if (pl.max_jobs) {
+        CPX_CUDA(cudaMemsetAsync(pl.njobs, 0, sizeof(unsigned int), ctx->stream));
+        CPX_CUDA(cudaMemsetAsync(pl.job_units, 0, (pl.max_jobs + 1) * sizeof(uint64_t), ctx->stream));
+    }
     k_hard<XT><<<(unsigned)pl.n_seg, pl.hard_threads, smem, ctx->stream>>>(
         pl.qd, pl.Q, pl.pre_seg, pl.n_seg, pl.seg_B, pl.seg_off, tb.P, tb.MU, tb.T, pl.hard_cnt, pl.hard_ms,
-        pl.hard_entries, pl.acc, pl.lbits_max, pl.jobs, pl.njobs, pl.snap, pl.max_jobs, lbits_sub,
+        pl.hard_entries, pl.acc, pl.lbits_max, pl.jobs, pl.njobs, pl.job_units, pl.snap, pl.max_jobs, lbits_sub,
         (uint32_t)std::min<uint64_t>(pl.offload_min, 0xFFFFFFFFull));
     CPX_LAUNCH("k_hard");
     note_launch(ctx);
     if (pl.max_jobs) {
-        k_hard_job_scan<<<1, 1024, 0, ctx->stream>>>(pl.jobs, pl.njobs, pl.max_jobs, pl.job_units);
-        CPX_LAUNCH("k_hard_job_scan");
+        scan_u64(ctx, pl.job_units, pl.max_jobs + 1);
         k_hard_leaves<XT><<<(unsigned)ctx->sm_count * 8, kThreads, 0, ctx->stream>>>(
             pl.jobs, pl.njobs, pl.max_jobs, pl.job_units, pl.snap, lbits_sub, tb.MU, tb.T, pl.hard_ms, pl.acc);
         CPX_LAUNCH("k_hard_leaves");
-        note_launch(ctx, 2);
+        note_launch(ctx);
     }
     if (pl.time_hard) CPX_CUDA(cudaEventRecord(ctx->ev_hard1, ctx->stream));
     if (pl.n_comb) {
-        k_hard_combine<<<(unsigned)((pl.n_comb + 255) / 256), 256, 0, ctx->stream>>>(
+        k_hard_combine<<<(unsigned)((pl.n_comb * 32 + 255) / 256), 256, 0, ctx->stream>>>(
             pl.qd, pl.Q, pl.pre_comb, pl.n_comb, pl.pre_seg, pl.seg_B, pl.seg_off, pl.hard_cnt, pl.hard_ms,
             pl.hard_entries, tb.P, tb.T, pl.acc);
         CPX_LAUNCH("k_hard_combine");

@@ -170,31 +170,66 @@ __global__ void __launch_bounds__(kThreads) k_trivial(const QD *__restrict__ qd,
 // Easy leaves are the non-trivial leaves with u = x/(p_b m) < p_b^2, where
 // phi(u, b - 1) = pi(u) - b + 2 is one pi-table lookup.  k_easy takes the
 // prime m = q: p_c < p <= icbrt(x), max(p, y/p, x/p^3) < q <= min(y, x/p^2)
-// (for p > iroot4(x) the bound x/p^3 is below p).  A warp takes one table
-// entry of p candidates at a time (ticket counter); its lanes stride over the
-// table entries of the q range.  k_easy_comp takes the composite m.
-// q range of the prime easy leaves of p: (qlo, qhi], with xp = x / p
+// (for p > iroot4(x) the bound x/p^3 is below p); k_easy_comp takes the
+// composite m.
+//
+// Per p the q range (qlo, qhi] is split at q1 ~ sqrt(x/p).  Below q1 every q
+// gives its own u and the leaves are taken one by one (sparse part).  Above
+// q1 runs of consecutive primes q share pi(x/(pq)) (clustered part): with
+// G(k) = pi(clamp(x/(p p_k), q1, qhi)) the primes q of the run with
+// pi(x/(pq)) = k number G(k) - G(k+1), and summation by parts turns
+//   Sum_{q in (q1, qhi]} (pi(x/(pq)) - b + 2)
+// into (klo - b + 2) pi(qhi) - (khi - b + 2) pi(q1) + Sum_{klo < k <= khi} G(k)
+// with klo = pi(x/(p qhi)), khi = pi(x/(p (q1 + 1))): one quotient and one
+// table lookup per prime u instead of per leaf.  The u primes come from the
+// resident prime list, so q1 is raised until x/(p (q1 + 1)) <= prm_max.
+
+constexpr uint64_t kEasyChunk = 64;   // pi-table entries of q per sparse work chunk
+constexpr uint64_t kEasyClu = 512;    // u primes per clustered work chunk
+
+struct EasyP {
+    uint64_t qlo, qhi, q1;  // sparse q in (qlo, q1], clustered q in (q1, qhi]
+    uint64_t klo, khi;      // pi(x / (p qhi)), pi(x / (p (q1 + 1)))
+    uint64_t nsp, ncl;      // work chunks of the two parts
+};
+
 template <class XT>
-__device__ __forceinline__ bool easy_q_range(XT x, uint64_t y, uint64_t p, XT &xp, uint64_t &qlo, uint64_t &qhi)
+__device__ __forceinline__ bool easy_plan(XT x, uint64_t y, uint64_t p, uint64_t prm_max,
+                                          const cpx_pient *__restrict__ T, XT &xp, EasyP &e)
 {
     xp = x / (XT)p;
-    qlo = y / p;
+    uint64_t qlo = y / p;
     if (qlo < p) qlo = p;
     const XT xpp = xp / (XT)p;
     const XT x3 = xpp / (XT)p;  // p <= iroot4(x): only q > x/p^3 (x/(pq) < p^2) are easy
     if (x3 > (XT)qlo) qlo = (x3 >= (XT)y) ? y : (uint64_t)x3;
-    qhi = (xpp < (XT)y) ? (uint64_t)xpp : y;
-    return qhi > qlo;
+    const uint64_t qhi = (xpp < (XT)y) ? (uint64_t)xpp : y;
+    if (qhi <= qlo) return false;
+    uint64_t q1 = cpx_isqrt((u128)xp);
+    const XT lim = xp / (XT)prm_max;
+    if (lim > (XT)q1) q1 = (lim >= (XT)qhi) ? qhi : (uint64_t)lim;
+    q1 = q1 < qlo ? qlo : (q1 > qhi ? qhi : q1);
+    e.qlo = qlo;
+    e.qhi = qhi;
+    e.q1 = q1;
+    e.nsp = (q1 > qlo) ? (((q1 - 1) >> 7) - (qlo >> 7) + kEasyChunk) / kEasyChunk : 0;
+    if (qhi > q1) {
+        e.klo = cpx_pi_dev(T, (uint64_t)cpx_qdiv(xp, qhi));
+        e.khi = cpx_pi_dev(T, (uint64_t)cpx_qdiv(xp, q1 + 1));
+        e.ncl = e.khi > e.klo ? (e.khi - e.klo + kEasyClu - 1) / kEasyClu : 1;
+    } else {
+        e.klo = e.khi = 0;
+        e.ncl = 0;
+    }
+    return true;
 }
 
-constexpr uint64_t kEasyChunk = 64;  // pi-table entries of q per work chunk
-
-// Pass 1: chunks of kEasyChunk q entries needed by each entry of p candidates
-// (one thread per entry); cnt[total] is left 0 so that the exclusive scan of
-// cnt ends with the grand total.
+// Pass 1: work chunks of each p (one thread per p = P[c + i]); cnt[total] is
+// left 0 so that the exclusive scan of cnt ends with the grand total.
 template <class XT>
 __global__ void k_easy_count(const QD *__restrict__ qd, uint32_t Q, const uint64_t *__restrict__ pre, uint64_t total,
-                             const cpx_pient *__restrict__ T, uint64_t *__restrict__ cnt)
+                             const uint32_t *__restrict__ P, uint64_t prm_max, const cpx_pient *__restrict__ T,
+                             uint64_t *__restrict__ cnt)
 {
     const uint64_t unit = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (unit > total) return;
@@ -204,41 +239,33 @@ __global__ void k_easy_count(const QD *__restrict__ qd, uint32_t Q, const uint64
     }
     const uint32_t q = find_q(pre, Q, unit);
     const QD &d = qd[q];
-    const XT x = xload<XT>(d);
-    const uint64_t pc = c_pc[d.c];
-    const uint64_t w = (pc >> 7) + (unit - pre[q]);
-    const ulonglong2 e = __ldg(reinterpret_cast<const ulonglong2 *>(T) + w);
-    uint64_t pb = e.x & range_mask(w, pc, d.cx), n = 0;
-    while (pb) {
-        const int j = __ffsll((long long)pb) - 1;
-        pb &= pb - 1;
-        XT xp;
-        uint64_t qlo, qhi;
-        if (!easy_q_range<XT>(x, d.y, 128 * w + 2 * j + 1, xp, qlo, qhi)) continue;
-        n += (((qhi - 1) >> 7) - (qlo >> 7) + kEasyChunk) / kEasyChunk;
-    }
-    cnt[unit] = n;
+    const uint64_t p = __ldg(P + d.c + (unit - pre[q]));
+    XT xp;
+    EasyP e;
+    cnt[unit] = easy_plan<XT>(xload<XT>(d), d.y, p, prm_max, T, xp, e) ? e.nsp + e.ncl : 0;
 }
 
-// Pass 2: each warp owns a contiguous slice of chunks; a chunk is one prime p
-// and kEasyChunk table entries of its q range, two entries per lane.
+// Pass 2: each warp owns a contiguous slice of chunks.  A sparse chunk is
+// kEasyChunk table entries of the q range of one p (two entries per lane); a
+// clustered chunk is kEasyClu consecutive u primes of one p.
 template <class XT>
 __global__ void __launch_bounds__(kThreads) k_easy(const QD *__restrict__ qd, uint32_t Q,
                                                    const uint64_t *__restrict__ pre, uint64_t total_units,
                                                    const uint64_t *__restrict__ off,
+                                                   const uint32_t *__restrict__ P, uint64_t prm_max,
                                                    const cpx_pient *__restrict__ T,
                                                    unsigned long long *__restrict__ acc)
 {
     const int lane = threadIdx.x & 31;
     const WarpSlice sl = warp_slice(off[total_units]);
     LaneAcc a;
-    // decoded chunk state, kept across consecutive chunks of the same p
-    uint64_t c_unit = ~0ull, c_first = 0, c_last = 0, qlo = 0, qhi = 0, wq0 = 0, b = 0;
+    // decoded state of the current p, kept across its consecutive chunks
+    uint64_t c_unit = ~0ull, c_first = 0, c_last = 0, b = 0;
     uint32_t q = 0;
     XT xp = 0;
+    EasyP e = {};
     for (uint64_t ch = sl.u0; ch < sl.u1; ch++) {
         if (ch < c_first || ch > c_last || c_unit == ~0ull) {
-            // locate the entry of p candidates holding chunk ch, then the prime
             uint64_t lo = 0, hi = total_units;  // off[lo] <= ch < off[hi]
             while (hi - lo > 1) {
                 const uint64_t mid = (lo + hi) >> 1;
@@ -248,46 +275,47 @@ __global__ void __launch_bounds__(kThreads) k_easy(const QD *__restrict__ qd, ui
             c_unit = lo;
             q = find_q(pre, Q, c_unit);
             const QD &d = qd[q];
-            const XT x = xload<XT>(d);
-            const uint64_t pc = c_pc[d.c];
-            const uint64_t w = (pc >> 7) + (c_unit - __ldg(pre + q));
-            const ulonglong2 e = __ldg(reinterpret_cast<const ulonglong2 *>(T) + w);
-            uint64_t pb = e.x & range_mask(w, pc, d.cx), base = __ldg(off + c_unit);
-            while (pb) {
-                const int j = __ffsll((long long)pb) - 1;
-                pb &= pb - 1;
-                const uint64_t p = 128 * w + 2 * j + 1;
-                if (!easy_q_range<XT>(x, d.y, p, xp, qlo, qhi)) continue;
-                wq0 = qlo >> 7;
-                const uint64_t n = (((qhi - 1) >> 7) - wq0 + kEasyChunk) / kEasyChunk;
-                if (ch < base + n) {
-                    c_first = base;
-                    c_last = base + n - 1;
-                    b = 1 + e.y + __popcll(e.x & ((2ull << j) - 1));
-                    break;
-                }
-                base += n;
-            }
+            const uint64_t i = c_unit - __ldg(pre + q);
+            b = d.c + 1 + i;  // p = p_b
+            easy_plan<XT>(xload<XT>(d), d.y, __ldg(P + d.c + i), prm_max, T, xp, e);
+            c_first = __ldg(off + c_unit);
+            c_last = c_first + e.nsp + e.ncl - 1;
         }
         if (q != a.q) {  // q is the same on every lane of the warp
             warp_flush(a, acc, ACC_EASY);
             a.q = q;
         }
-        const uint64_t w_beg = wq0 + (ch - c_first) * kEasyChunk;
-        const uint64_t w_end = min(w_beg + kEasyChunk, ((qhi - 1) >> 7) + 1);
-        uint64_t ps = 0, cnt = 0;
-        for (uint64_t wq = w_beg + lane; wq < w_end; wq += 32) {
-            const ulonglong2 e2 = __ldg(reinterpret_cast<const ulonglong2 *>(T) + wq);
-            uint64_t qb = e2.x & range_mask(wq, qlo, qhi);
-            while (qb) {
-                const int j2 = __ffsll((long long)qb) - 1;
-                qb &= qb - 1;
-                const uint64_t uu = (uint64_t)cpx_qdiv(xp, 128 * wq + 2 * j2 + 1);
-                ps += cpx_pi_dev(T, uu);
-                cnt++;
+        const uint64_t r = ch - c_first;
+        if (r < e.nsp) {
+            const uint64_t w_beg = (e.qlo >> 7) + r * kEasyChunk;
+            const uint64_t w_end = min(w_beg + kEasyChunk, ((e.q1 - 1) >> 7) + 1);
+            uint64_t ps = 0, cnt = 0;
+            for (uint64_t wq = w_beg + lane; wq < w_end; wq += 32) {
+                const ulonglong2 e2 = __ldg(reinterpret_cast<const ulonglong2 *>(T) + wq);
+                uint64_t qb = e2.x & range_mask(wq, e.qlo, e.q1);
+                while (qb) {
+                    const int j2 = __ffsll((long long)qb) - 1;
+                    qb &= qb - 1;
+                    ps += cpx_pi_dev(T, (uint64_t)cpx_qdiv(xp, 128 * wq + 2 * j2 + 1));
+                    cnt++;
+                }
             }
+            a.v += (i128)ps + (i128)cnt * (2 - (i128)b);
+        } else {
+            const uint64_t j = r - e.nsp;
+            const uint64_t k0 = e.klo + 1 + j * kEasyClu, k1 = min(e.khi, e.klo + (j + 1) * kEasyClu);
+            uint64_t ps = 0;
+            for (uint64_t k = k0 + lane; k <= k1; k += 32) {
+                uint64_t v = (uint64_t)cpx_qdiv(xp, (uint64_t)__ldg(P + k - 1));
+                v = v < e.q1 ? e.q1 : (v > e.qhi ? e.qhi : v);
+                ps += cpx_pi_dev(T, v);
+            }
+            i128 add = (i128)ps;
+            if (j == 0 && lane == 0)
+                add += ((i128)e.klo - (i128)b + 2) * (i128)cpx_pi_dev(T, e.qhi) -
+                       ((i128)e.khi - (i128)b + 2) * (i128)cpx_pi_dev(T, e.q1);
+            a.v += add;
         }
-        a.v += (i128)ps + (i128)cnt * (2 - (i128)b);
     }
     warp_flush(a, acc, ACC_EASY);
 }
@@ -443,20 +471,23 @@ void launch_easy(cpx_ctx *ctx, const Plan &pl)
     if (!pl.n_easy) return;
     uint64_t *off = pl.easy_off;
     const unsigned gc = (unsigned)((pl.n_easy + 1 + 255) / 256);
+    const Tables &tb = ctx->tab;
     if (pl.wide)
-        k_easy_count<u128><<<gc, 256, 0, ctx->stream>>>(pl.qd, pl.Q, pl.pre_easy, pl.n_easy, ctx->tab.T, off);
+        k_easy_count<u128><<<gc, 256, 0, ctx->stream>>>(pl.qd, pl.Q, pl.pre_easy, pl.n_easy, tb.P, tb.prm_max,
+                                                         tb.T, off);
     else
-        k_easy_count<uint64_t><<<gc, 256, 0, ctx->stream>>>(pl.qd, pl.Q, pl.pre_easy, pl.n_easy, ctx->tab.T, off);
+        k_easy_count<uint64_t><<<gc, 256, 0, ctx->stream>>>(pl.qd, pl.Q, pl.pre_easy, pl.n_easy, tb.P, tb.prm_max,
+                                                             tb.T, off);
     CPX_LAUNCH("k_easy_count");
     note_launch(ctx);
     scan_u64(ctx, off, pl.n_easy + 1);
     const unsigned grid = (unsigned)ctx->sm_count * 8;
     if (pl.wide)
-        k_easy<u128><<<grid, kThreads, 0, ctx->stream>>>(pl.qd, pl.Q, pl.pre_easy, pl.n_easy, off, ctx->tab.T,
-                                                         pl.acc);
+        k_easy<u128><<<grid, kThreads, 0, ctx->stream>>>(pl.qd, pl.Q, pl.pre_easy, pl.n_easy, off, tb.P, tb.prm_max,
+                                                         tb.T, pl.acc);
     else
-        k_easy<uint64_t><<<grid, kThreads, 0, ctx->stream>>>(pl.qd, pl.Q, pl.pre_easy, pl.n_easy, off, ctx->tab.T,
-                                                             pl.acc);
+        k_easy<uint64_t><<<grid, kThreads, 0, ctx->stream>>>(pl.qd, pl.Q, pl.pre_easy, pl.n_easy, off, tb.P,
+                                                             tb.prm_max, tb.T, pl.acc);
     CPX_LAUNCH("k_easy");
     note_launch(ctx);
 }

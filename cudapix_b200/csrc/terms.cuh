@@ -29,8 +29,8 @@ struct __align__(16) EasyLvl {
 struct __align__(16) HardJob {
     uint32_t q, b, p, kind;
     uint64_t mlo, mhi, lo, slot;  // lo: first number of the warp's sub-segment
-    uint64_t nunits, unit0;
-    uint64_t carry, pad;          // survivors of level b-1 in the segment below the sub-segment
+    uint64_t nunits;              // k_hard_leaves work units
+    uint64_t carry;               // survivors of level b-1 in the segment below the sub-segment
     u128 xp;
 };
 
@@ -62,7 +62,7 @@ struct Plan {
     // heavy hard-leaf sets offloaded from k_hard
     HardJob *jobs = nullptr;
     unsigned int *njobs = nullptr;   // device counter
-    uint64_t *job_units = nullptr;   // device: total work units after the scan
+    uint64_t *job_units = nullptr;   // max_jobs + 1 work-unit counts, scanned into offsets
     unsigned char *snap = nullptr;   // snapshot slots
     uint32_t max_jobs = 0;
     uint64_t offload_min = 0;        // candidate threshold of an offloaded leaf set (0: none)
