@@ -278,7 +278,7 @@ def main():
         assert out == ref, "batch results changed between runs"
 
     launches0 = ctx.launches
-    dev_ms, e2e_ms, hard_ms, hard_bytes = [], [], [], []
+    dev_ms, e2e_ms, hard_ms, hard_bytes, host_stats = [], [], [], [], []
     barrier(world)
     with Clocks(local) as clk:
         for _ in range(args.steps):
@@ -290,6 +290,7 @@ def main():
             hm, hb = ctx.last_hard_stats()
             hard_ms.append(hm)
             hard_bytes.append(hb)
+            host_stats.append(ctx.last_batch_stats())
             assert out == ref
     barrier(world)
     import ctypes
@@ -356,6 +357,8 @@ def main():
                    "parallelism": f"replicas x{world}"},
         "e2e": {"value": nq / t_e2e, "unit": UNIT, "h2d_bytes_per_step": io[0], "d2h_bytes_per_step": io[1]},
         "gpu_launches": int(launches),
+        "host_ms": {k: round(statistics.median(h[k] for h in host_stats), 3)
+                    for k in ("roots_ms", "tables_ms", "plan_ms", "launch_ms", "wait_ms")},
         "graph": graph,
         "plain": plain,
         "batched_over_plain": (value / plain["value"]) if plain else None,

@@ -22,7 +22,7 @@ Python int; 64- and 128-bit overloads are chosen by the size of x.
 """
 import ctypes
 
-from ._lib import CpxError, ExtensionMissing, Params, Terms, U128, header_symbols, load  # noqa: F401
+from ._lib import BatchStats, CpxError, ExtensionMissing, Params, Terms, U128, header_symbols, load  # noqa: F401
 
 __all__ = [
     "Context", "context", "P2", "S2_trivial", "Ordinary", "S2_easy", "S2hard", "pi_deleglise_rivat",
@@ -121,6 +121,12 @@ class Context:
         ms = ctypes.c_float()
         self.call("cpx_last_batch_ms", ctypes.byref(ms))
         return ms.value
+
+    def last_batch_stats(self):
+        """Host phases (ms) and hard-leaf work shape of the last batch."""
+        st = BatchStats()
+        self.call("cpx_last_batch_stats", ctypes.byref(st))
+        return st.as_dict()
 
     def timer_start(self):
         self.call("cpx_timer_start")

@@ -66,6 +66,23 @@ class Terms(ctypes.Structure):
         return d
 
 
+class BatchStats(ctypes.Structure):
+    _fields_ = [
+        ("roots_ms", ctypes.c_double),
+        ("tables_ms", ctypes.c_double),
+        ("plan_ms", ctypes.c_double),
+        ("launch_ms", ctypes.c_double),
+        ("wait_ms", ctypes.c_double),
+        ("queries", ctypes.c_uint64),
+        ("segments", ctypes.c_uint64),
+        ("hard_jobs", ctypes.c_uint64),
+        ("offload_min", ctypes.c_uint64),
+    ]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
 class Params(ctypes.Structure):
     _fields_ = [
         ("alpha_num", ctypes.c_uint32),
@@ -104,6 +121,7 @@ _SIGS = {
     "cpx_timer_stop": (ctypes.c_int, [P, ctypes.POINTER(ctypes.c_float)]),
     "cpx_flush_l2": (ctypes.c_int, [P]),
     "cpx_last_batch_io": (ctypes.c_int, [P, pu64, pu64]),
+    "cpx_last_batch_stats": (ctypes.c_int, [P, ctypes.POINTER(BatchStats)]),
     "cpx_iroots": (ctypes.c_int, [U128, pu64, pu64, pu64]),
     "cpx_default_y": (ctypes.c_int, [U128, u32, u32, pu64]),
     "cpx_alpha_milli": (u32, [U128]),

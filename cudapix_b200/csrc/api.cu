@@ -206,6 +206,14 @@ int cpx_last_batch_io(cpx_ctx *ctx, uint64_t *h2d_bytes, uint64_t *d2h_bytes)
     });
 }
 
+int cpx_last_batch_stats(cpx_ctx *ctx, cpx_batch_stats *out)
+{
+    return guarded(ctx, [&] {
+        if (!out) fail(CPX_EINVAL, "null output");
+        *out = ctx->last_stats;
+    });
+}
+
 int cpx_timer_start(cpx_ctx *ctx)
 {
     return guarded(ctx, [&] { CPX_CUDA(cudaEventRecord(ctx->ev_t0, ctx->stream)); });

@@ -6,6 +6,7 @@
 // src/main.cpp:61,165).  Every root here is an exact floor root computed in
 // integers; no floating point value ever reaches a count.
 #pragma once
+#include <cmath>
 #include <cstdint>
 
 #if defined(__CUDACC__)
@@ -18,7 +19,9 @@ typedef unsigned __int128 u128;
 typedef __int128 i128;
 
 // ------------------------------------------------------------------ roots
-// Integer Newton iteration from an over-estimate (a power of two above the
+// x < 2^64: a double estimate of the root corrected to the exact floor root
+// by integer comparisons (the estimate is within 2 of the root).  Wider x:
+// integer Newton iteration from an over-estimate (a power of two above the
 // root), which decreases monotonically to the floor root.
 
 CPX_HD int cpx_bitlen128(u128 x)
@@ -36,6 +39,13 @@ CPX_HD int cpx_bitlen128(u128 x)
 CPX_HD uint64_t cpx_isqrt(u128 x)
 {
     if (x < 2) return (uint64_t)x;
+    if (!(x >> 64)) {
+        const uint64_t v = (uint64_t)x;
+        uint64_t r = (uint64_t)sqrt((double)v);
+        while ((u128)r * r > v) r--;
+        while ((u128)(r + 1) * (r + 1) <= v) r++;
+        return r;
+    }
     int b = cpx_bitlen128(x);
     u128 r = (u128)1 << ((b + 1) / 2); // r >= sqrt(x)
     for (;;) {
@@ -49,6 +59,13 @@ CPX_HD uint64_t cpx_isqrt(u128 x)
 CPX_HD uint64_t cpx_icbrt(u128 x)
 {
     if (x < 8) return x ? 1 : 0;
+    if (!(x >> 64)) {
+        const uint64_t v = (uint64_t)x;
+        uint64_t r = (uint64_t)cbrt((double)v);
+        while ((u128)r * r * r > v) r--;
+        while ((u128)(r + 1) * (r + 1) * (r + 1) <= v) r++;
+        return r;
+    }
     int b = cpx_bitlen128(x);
     u128 r = (u128)1 << ((b + 2) / 3); // r >= cbrt(x)
     for (;;) {

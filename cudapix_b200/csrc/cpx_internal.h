@@ -108,6 +108,7 @@ struct cpx_ctx {
     cudaGraphExec_t graph_exec = nullptr;  // the batch kernels of CPX_BATCH_GRAPH
     uint64_t graph_builds = 0, graph_updates = 0;
     uint64_t last_h2d = 0, last_d2h = 0;  // bytes copied by the last batch
+    cpx_batch_stats last_stats = {};      // host phases of the last batch
     double last_hard_bytes = 0.0;
     uint64_t launches = 0;  // kernels launched by this context
 };

@@ -6,7 +6,12 @@
 // roots, and replaces its one-term-at-a-time, synchronise-after-every-launch
 // flow with one pass of a handful of kernels over every query of a batch.
 #include <algorithm>
+#include <atomic>
+#include <chrono>
 #include <cmath>
+#include <exception>
+#include <mutex>
+#include <thread>
 
 #include "driver.h"
 #include "terms.cuh"
@@ -77,8 +82,6 @@ bool dr_domain_ok(u128 x, uint64_t y, uint32_t c)
     return true;
 }
 
-// Segments (of `span` integers) that sieve level b, p = p_b: those with
-// hi > p^2 and (lo = 0 or p^2 lo < x); the same rule as k_hard_plan.
 // An upper bound of x^(2/5), at most 2^31: the u primes an easy leaf's
 // clustered part needs (the kernels fall back to single leaves above the
 // resident prime list, so the bound only has to be close).
@@ -88,13 +91,18 @@ static uint64_t easy_u_bound(u128 x)
     return v >= 2147483648.0L ? 2147483648ull : (uint64_t)v;
 }
 
+// Segments (of `span` integers) that sieve level b, p = p_b: those with
+// hi > p^2 and (lo = 0 or p^2 lo < x); the same rule as k_hard_plan.
 static uint64_t segments_at_level(u128 x, uint64_t span, uint64_t p, uint64_t nseg)
 {
-    const u128 p2 = (u128)p * p;
-    const u128 first = p2 / span;
-    const u128 last = (x - 1) / (p2 * span);  // largest s >= 0 with s * span * p^2 < x
-    const u128 hi = std::min<u128>(last, (u128)nseg - 1);
-    return hi >= first ? (uint64_t)(hi - first + 1) : 0;
+    const uint64_t p2 = p * p;  // p <= iroot4(x) < 2^32
+    const uint64_t first = p2 / span;
+    // largest s >= 0 with s * span * p^2 < x (p^2 span < 2^64 for the segment sizes used)
+    const u128 d = (u128)p2 * span;
+    const uint64_t last = (x >> 64) || (d >> 64) ? (uint64_t)std::min<u128>((x - 1) / d, (u128)nseg)
+                                                 : ((uint64_t)x - 1) / (uint64_t)d;
+    const uint64_t hi = std::min<uint64_t>(last, nseg - 1);
+    return hi >= first ? hi - first + 1 : 0;
 }
 
 // Number of (sub-segment, level) leaf sets of one query that k_hard hands to
@@ -119,6 +127,12 @@ static uint64_t heavy_leaf_sets(const QD &d, const std::vector<uint32_t> &hP, ui
         const XT x3 = xp / (XT)(p * p);
         const uint64_t mtop = x3 < (XT)y ? (uint64_t)x3 : y;
         if (mtop <= y / p) continue;
+        // No sub-segment holds more than mtop^2 span_w / (xp + span_w mtop) + 2
+        // candidate m (the densest one starts at u = xp / mtop), and a set's
+        // count is at most half its m range + 16: skip levels below thr.
+        const double dm = (double)mtop, dsw = (double)span_w;
+        const double most = 1.001 * dm * dm * dsw / ((double)xp + dsw * dm) + 2.0;
+        if (0.5 * most + 17.0 < (double)thr) continue;
         const bool prime_lvl = p * p > y;
         for (uint64_t w = (uint64_t)(xp / (XT)mtop) / span_w; w < nsub; w++) {
             const uint64_t lo_w = w * span_w, hi_w = lo_w + span_w;
@@ -234,10 +248,55 @@ template <class F> static void launch_as_graph(cpx_ctx *ctx, F &&launches)
     CPX_CUDA(cudaGraphLaunch(ctx->graph_exec, ctx->stream));
 }
 
+// Runs f(0) .. f(n - 1) on up to 16 host threads (the calling thread
+// included); the first exception thrown by any f is rethrown here.
+constexpr size_t kPlanBlock = 64;  // queries per planning block
+template <class F> static void parallel_blocks(size_t n, F &&f)
+{
+    const size_t hw = std::max<size_t>(1, std::thread::hardware_concurrency());
+    const size_t nt = std::min<size_t>(std::min<size_t>(hw, 16), n);
+    if (nt <= 1) {
+        for (size_t k = 0; k < n; k++) f(k);
+        return;
+    }
+    std::atomic<size_t> next(0);
+    std::exception_ptr err;
+    std::mutex em;
+    auto worker = [&] {
+        try {
+            for (;;) {
+                const size_t k = next.fetch_add(1);
+                if (k >= n) break;
+                f(k);
+            }
+        } catch (...) {
+            std::lock_guard<std::mutex> g(em);
+            if (!err) err = std::current_exception();
+        }
+    };
+    std::vector<std::thread> th;
+    th.reserve(nt - 1);
+    for (size_t t = 1; t < nt; t++) th.emplace_back(worker);
+    worker();
+    for (auto &t : th) t.join();
+    if (err) std::rethrow_exception(err);
+}
+
+static double ms_since(std::chrono::steady_clock::time_point &t)
+{
+    const auto now = std::chrono::steady_clock::now();
+    const double ms = std::chrono::duration<double, std::milli>(now - t).count();
+    t = now;
+    return ms;
+}
+
 void run_batch(cpx_ctx *ctx, const BatchReq &rq)
 {
     const uint32_t Q = (uint32_t)rq.n;
     if (Q == 0) return;
+    cpx_batch_stats st = {};
+    st.queries = Q;
+    auto clk = std::chrono::steady_clock::now();
     const uint32_t c = rq.c;
     if (c < 1 || c > 8) fail(CPX_EINVAL, "c must be in 1..8");
     const uint32_t threads = rq.threads ? rq.threads : ctx->hard_threads;
@@ -298,6 +357,7 @@ void run_batch(cpx_ctx *ctx, const BatchReq &rq)
     }
     if (N > rq.max_table_n) fail(CPX_ERANGE, "pi table bound exceeds the configured limit");
 
+    st.roots_ms = ms_since(clk);
     // ---- tables
     ensure_primes(ctx, std::max<uint64_t>(Pneed, cpx_isqrt(Y + 1) + 2));
     bool any_direct = false;
@@ -307,6 +367,7 @@ void run_batch(cpx_ctx *ctx, const BatchReq &rq)
     if (Y) ensure_mulpf(ctx, Y + 8);
     if (mask & TERM_ORD) ensure_wheel(ctx, c);
     const std::vector<uint32_t> &hP = host_primes(ctx);
+    st.tables_ms = ms_since(clk);
 
     if (mask & TERM_HARD) {
         for (QD &d : qd)
@@ -314,69 +375,94 @@ void run_batch(cpx_ctx *ctx, const BatchReq &rq)
         choose_lbits(ctx, qd, c, threads, rq.lbits);
     }
 
-    // ---- units per kernel family
+    // ---- units per kernel family (queries planned in parallel blocks)
     std::vector<uint64_t> pre(6 * (size_t)(Q + 1), 0);
     uint64_t *p_ord = pre.data(), *p_p2 = p_ord + (Q + 1), *p_triv = p_p2 + (Q + 1), *p_easy = p_triv + (Q + 1),
              *p_seg = p_easy + (Q + 1), *p_comb = p_seg + (Q + 1);
-    uint64_t hard_entries = 0;
-    uint32_t lbits_max = 0;
-    std::vector<EasyLvl> elv;
-    uint64_t n_ecomp = 0;
-    for (uint32_t i = 0; i < Q; i++) {
-        QD &d = qd[i];
-        uint64_t n_ord = 0, n_p2 = 0, n_triv = 0, n_easy = 0, n_seg = 0, n_comb = 0;
-        if (!d.direct) {
-            const u128 x = d.x;
-            const uint64_t pc = kSmallPrimes[c];
-            if (mask & TERM_ORD) n_ord = ((d.y + 1) / 2 + 3) / 4;
-            if ((mask & TERM_P2) && d.sx > d.y) n_p2 = ((d.sx - 1) >> 7) - (d.y >> 7) + 1;
-            if (mask & TERM_TRIV) n_triv = (d.cx > d.tx) ? ((d.cx - 1) >> 7) - (d.tx >> 7) + 1 : 1;
-            if ((mask & TERM_EASY) && d.cx > pc) n_easy = host_pi(hP, d.cx) - c;  // primes p_c < p <= icbrt(x)
-            if (mask & TERM_EASY) {
-                // composite easy leaves: levels b with p_b <= iroot4(x), p_b^2 < y and
-                // max(y/p_b, x/p_b^3) < y
-                const uint64_t nb4 = host_pi(hP, d.r4);
-                for (uint64_t b = c + 1; b <= nb4; b++) {
-                    const uint64_t p = hP[b - 1];
-                    if (p * p >= d.y) break;
-                    const u128 x3 = x / ((u128)p * p * p);
-                    uint64_t mlo = d.y / p;
-                    if (x3 > (u128)mlo) mlo = x3 >= (u128)d.y ? d.y : (uint64_t)x3;
-                    if (mlo >= d.y) continue;
-                    const uint64_t mfirst = (mlo + 1) | 1;
-                    EasyLvl r;
-                    r.q = i;
-                    r.b = (uint32_t)b;
-                    r.p = (uint32_t)p;
-                    r.pad = 0;
-                    r.i_lo = (mfirst - 1) / 2;
-                    r.i_hi = (d.y - 1) / 2 + 1;
-                    if (r.i_lo >= r.i_hi) continue;
-                    r.i_base = r.i_lo & ~uint64_t(3);
-                    r.unit0 = n_ecomp;
-                    n_ecomp += (r.i_hi - r.i_base + 1023) / 1024;
-                    elv.push_back(r);
+    std::vector<uint64_t> q_ent(Q, 0);
+    const size_t nblk = (Q + kPlanBlock - 1) / kPlanBlock;
+    std::vector<std::vector<EasyLvl>> blk_elv(nblk);
+    std::vector<uint64_t> blk_ecomp(nblk, 0);
+    parallel_blocks(nblk, [&](size_t k) {
+        const uint32_t i0 = (uint32_t)(k * kPlanBlock), i1 = (uint32_t)std::min<size_t>(Q, (k + 1) * kPlanBlock);
+        std::vector<EasyLvl> &elv = blk_elv[k];
+        uint64_t n_ecomp = 0;  // relative to the block
+        for (uint32_t i = i0; i < i1; i++) {
+            QD &d = qd[i];
+            uint64_t n_ord = 0, n_p2 = 0, n_triv = 0, n_easy = 0, n_seg = 0, n_comb = 0;
+            if (!d.direct) {
+                const u128 x = d.x;
+                const uint64_t pc = kSmallPrimes[c];
+                if (mask & TERM_ORD) n_ord = ((d.y + 1) / 2 + 3) / 4;
+                if ((mask & TERM_P2) && d.sx > d.y) n_p2 = ((d.sx - 1) >> 7) - (d.y >> 7) + 1;
+                if (mask & TERM_TRIV) n_triv = (d.cx > d.tx) ? ((d.cx - 1) >> 7) - (d.tx >> 7) + 1 : 1;
+                if ((mask & TERM_EASY) && d.cx > pc) n_easy = host_pi(hP, d.cx) - c;  // primes p_c < p <= icbrt(x)
+                if (mask & TERM_EASY) {
+                    // composite easy leaves: levels b with p_b <= iroot4(x), p_b^2 < y and
+                    // max(y/p_b, x/p_b^3) < y
+                    const uint64_t nb4 = host_pi(hP, d.r4);
+                    for (uint64_t b = c + 1; b <= nb4; b++) {
+                        const uint64_t p = hP[b - 1];
+                        if (p * p >= d.y) break;
+                        const u128 x3 = (x >> 64) ? x / ((u128)p * p * p) : (u128)((uint64_t)x / (p * p * p));
+                        uint64_t mlo = d.y / p;
+                        if (x3 > (u128)mlo) mlo = x3 >= (u128)d.y ? d.y : (uint64_t)x3;
+                        if (mlo >= d.y) continue;
+                        const uint64_t mfirst = (mlo + 1) | 1;
+                        EasyLvl r;
+                        r.q = i;
+                        r.b = (uint32_t)b;
+                        r.p = (uint32_t)p;
+                        r.pad = 0;
+                        r.i_lo = (mfirst - 1) / 2;
+                        r.i_hi = (d.y - 1) / 2 + 1;
+                        if (r.i_lo >= r.i_hi) continue;
+                        r.i_base = r.i_lo & ~uint64_t(3);
+                        r.unit0 = n_ecomp;
+                        n_ecomp += (r.i_hi - r.i_base + 1023) / 1024;
+                        elv.push_back(r);
+                    }
                 }
-            }
-            if (mask & TERM_HARD) {
-                if (d.nb > c) {
-                    lbits_max = std::max(lbits_max, d.lbits);
+                if ((mask & TERM_HARD) && d.nb > c) {
                     const uint64_t span = 2ull << d.lbits;
                     d.nseg = (d.z + 1 + span - 1) / span;
                     n_seg = d.nseg;
                     n_comb = d.nb - c;
-                    for (uint32_t b = c + 1; b <= d.nb; b++) {
-                        hard_entries += segments_at_level(x, span, hP[b - 1], d.nseg);
-                    }
+                    uint64_t ent = 0;
+                    for (uint32_t b = c + 1; b <= d.nb; b++) ent += segments_at_level(x, span, hP[b - 1], d.nseg);
+                    q_ent[i] = ent;
                 }
             }
+            p_ord[i + 1] = n_ord;
+            p_p2[i + 1] = n_p2;
+            p_triv[i + 1] = n_triv;
+            p_easy[i + 1] = n_easy;
+            p_seg[i + 1] = n_seg;
+            p_comb[i + 1] = n_comb;
         }
-        p_ord[i + 1] = p_ord[i] + n_ord;
-        p_p2[i + 1] = p_p2[i] + n_p2;
-        p_triv[i + 1] = p_triv[i] + n_triv;
-        p_easy[i + 1] = p_easy[i] + n_easy;
-        p_seg[i + 1] = p_seg[i] + n_seg;
-        p_comb[i + 1] = p_comb[i] + n_comb;
+        blk_ecomp[k] = n_ecomp;
+    });
+    for (int f = 0; f < 6; f++) {
+        uint64_t *a = pre.data() + (size_t)f * (Q + 1);
+        for (uint32_t i = 0; i < Q; i++) a[i + 1] += a[i];
+    }
+    uint64_t hard_entries = 0;
+    double hard_bytes = 0.0;  // one pass over the segment bitmap per (segment, level)
+    uint32_t lbits_max = 0;
+    for (uint32_t i = 0; i < Q; i++) {
+        if (!q_ent[i]) continue;
+        hard_entries += q_ent[i];
+        hard_bytes += (double)q_ent[i] * (double)(1u << qd[i].lbits) / 8.0;
+        lbits_max = std::max(lbits_max, qd[i].lbits);
+    }
+    std::vector<EasyLvl> elv;
+    uint64_t n_ecomp = 0;
+    for (size_t k = 0; k < nblk; k++) {
+        for (EasyLvl r : blk_elv[k]) {
+            r.unit0 += n_ecomp;
+            elv.push_back(r);
+        }
+        n_ecomp += blk_ecomp[k];
     }
     if (!lbits_max) lbits_max = 15;
 
@@ -427,13 +513,17 @@ void run_batch(cpx_ctx *ctx, const BatchReq &rq)
         const uint64_t budget = std::max<uint64_t>(1, ctx->hard_offload_bytes / (stride + sizeof(HardJob)));
         uint64_t thr = ctx->hard_offload_min, njobs = 0;
         while (thr) {
-            njobs = 0;
-            for (const QD &d : qd) {
-                if (d.direct || d.nb <= c) continue;
-                njobs += wide ? heavy_leaf_sets<u128>(d, hP, threads, thr, budget + 1 - njobs)
-                              : heavy_leaf_sets<uint64_t>(d, hP, threads, thr, budget + 1 - njobs);
-                if (njobs > budget) break;
-            }
+            std::atomic<uint64_t> total(0);
+            parallel_blocks(nblk, [&](size_t k) {
+                const size_t i1 = std::min<size_t>(Q, (k + 1) * kPlanBlock);
+                for (size_t i = k * kPlanBlock; i < i1 && total.load() <= budget; i++) {
+                    const QD &d = qd[i];
+                    if (d.direct || d.nb <= c) continue;
+                    total += wide ? heavy_leaf_sets<u128>(d, hP, threads, thr, budget + 1)
+                                  : heavy_leaf_sets<uint64_t>(d, hP, threads, thr, budget + 1);
+                }
+            });
+            njobs = total.load();
             if (njobs <= budget) break;
             thr = (thr >= (1ull << 40)) ? 0 : 2 * thr;
         }
@@ -453,6 +543,10 @@ void run_batch(cpx_ctx *ctx, const BatchReq &rq)
     if (mask & TERM_HARD) prepare_hard(ctx, pl);
     u128 *d_out = ctx->b_work[6].as<u128>(Q);
 
+    st.plan_ms = ms_since(clk);
+    st.segments = pl.n_seg;
+    st.hard_jobs = pl.max_jobs;
+    st.offload_min = pl.offload_min;
     // one staging copy host -> device
     std::vector<unsigned char> stage(qd_bytes + pre_bytes + elv_bytes);
     memcpy(stage.data(), qd.data(), qd_bytes);
@@ -478,12 +572,15 @@ void run_batch(cpx_ctx *ctx, const BatchReq &rq)
     else launch_all();
     if (ctx->timing) CPX_CUDA(cudaEventRecord(ctx->ev_b1, ctx->stream));
 
+    st.launch_ms = ms_since(clk);
     // ---- results
     std::vector<unsigned long long> acc(acc_words);
     CPX_CUDA(cudaMemcpyAsync(acc.data(), d_acc, acc_words * 8, cudaMemcpyDeviceToHost, ctx->stream));
     CPX_CUDA(cudaStreamSynchronize(ctx->stream));
     ctx->last_h2d = stage.size();
     ctx->last_d2h = acc_words * 8;
+    st.wait_ms = ms_since(clk);
+    ctx->last_stats = st;
     for (uint32_t i = 0; i < Q; i++) {
         const unsigned long long *A = acc.data() + (size_t)i * kAccStride;
         auto rd = [&](int t) { return (i128)(((u128)A[2 * t + 1] << 64) | A[2 * t]); };
@@ -505,17 +602,7 @@ void run_batch(cpx_ctx *ctx, const BatchReq &rq)
         float ms = 0.f;
         CPX_CUDA(cudaEventElapsedTime(&ms, ctx->ev_hard0, ctx->ev_hard1));
         ctx->last_hard_ms = ms;
-        // algorithmic bytes: one pass over the segment bitmap per active level
-        double bytes = 0.0;
-        for (uint32_t i = 0; i < Q; i++) {
-            const QD &d = qd[i];
-            if (d.direct || d.nb <= c) continue;
-            const uint64_t span = 2ull << d.lbits;
-            for (uint32_t b = c + 1; b <= d.nb; b++) {
-                bytes += (double)segments_at_level(d.x, span, hP[b - 1], d.nseg) * (double)(1u << d.lbits) / 8.0;
-            }
-        }
-        ctx->last_hard_bytes = bytes;
+        ctx->last_hard_bytes = hard_bytes;
     }
 }
 

@@ -96,6 +96,21 @@ int cpx_set_timing(cpx_ctx *ctx, int enable);
 int cpx_last_batch_ms(cpx_ctx *ctx, float *ms);
 /* bytes the last batch copied host->device and device->host */
 int cpx_last_batch_io(cpx_ctx *ctx, uint64_t *h2d_bytes, uint64_t *d2h_bytes);
+
+/* Host-side profile of the last batch (wall clock, milliseconds) and the
+ * shape of its hard-leaf work.  No reference counterpart. */
+typedef struct {
+    double roots_ms;      /* per-query roots, y, validity, table bounds */
+    double tables_ms;     /* growing the resident tables (0 when they suffice) */
+    double plan_ms;       /* segment sizes, work-unit prefixes, leaf-set count */
+    double launch_ms;     /* staging copy and kernel launches (enqueue only) */
+    double wait_ms;       /* waiting for the device and reading the results */
+    uint64_t queries;
+    uint64_t segments;    /* hard-leaf segments */
+    uint64_t hard_jobs;   /* leaf-set slots reserved for k_hard_leaves */
+    uint64_t offload_min; /* candidate threshold of an offloaded leaf set */
+} cpx_batch_stats;
+int cpx_last_batch_stats(cpx_ctx *ctx, cpx_batch_stats *out);
 /* CUDA-event stopwatch on the context stream: start records an event; stop
  * records another, synchronises and returns the elapsed milliseconds */
 int cpx_timer_start(cpx_ctx *ctx);
