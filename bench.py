@@ -140,6 +140,67 @@ def alpha_frac(x):
     return _lib.load().cpx_alpha_milli(_lib.U128.of(x)), 1000
 
 
+def target_ratio(cpx, ctx, args):
+    """Batched vs plain queries/s for x log-uniform in [1e10, 1e15] (1024
+    queries, numpy default_rng(0)); the plain path on the first 128."""
+    xs = workload(1024, seed=0, lo=10.0, hi=15.0)
+    ref = cpx.pi_batch(xs, ctx=ctx)
+    dev = []
+    for _ in range(3):
+        ctx.flush_l2()
+        ctx.timer_start()
+        assert cpx.pi_batch(xs, ctx=ctx) == ref
+        dev.append(ctx.timer_stop())
+    lat = []
+    for x, r in zip(xs[:128], ref):
+        ctx.timer_start()
+        assert cpx.pi_deleglise_rivat(x, 0, 6, ctx=ctx) == r
+        lat.append(ctx.timer_stop())
+    b = len(xs) / (statistics.median(dev) / 1000.0)
+    p = len(lat) / (sum(lat) / 1000.0)
+    return {"workload": "1024 x = floor(10^e), e ~ U[10,15], default_rng(0); plain on the first 128",
+            "batch_e2e_qps": b, "plain_qps": p, "ratio": b / p}
+
+
+def serve_sweep(cpx, ctx, args):
+    """Continuous batching (cpx_serve_*) under Poisson arrivals: x = floor(10^e),
+    e ~ U[10, 17], gaps ~ Exp(1/lambda), both from numpy default_rng(1).  Per
+    rate: p50/p99 latency from arrival to result and completed queries/s; the
+    plain path's service rate on the same x mix beside it.  Every answer is
+    checked against the same x answered alone."""
+    rng = np.random.default_rng(1)
+    pool = [int(10.0**e) for e in rng.uniform(10, 17, 400)]
+    truth = dict(zip(pool, cpx.pi_batch(pool, ctx=ctx)))
+    # plain per-query path on the same distribution
+    lat = []
+    for x in pool[:48]:
+        ctx.timer_start()
+        assert cpx.pi_deleglise_rivat(x, 0, 6, ctx=ctx) == truth[x]
+        lat.append(ctx.timer_stop())
+    lat.sort()
+    plain = {"qps": len(lat) / (sum(lat) / 1000.0), "p50_ms": lat[len(lat) // 2], "p99_ms": lat[-1],
+             "queries": len(lat)}
+    rows = []
+    own = cpx.Context(ctx.device)
+    with cpx.Server(own, lanes=args.serve_lanes, reserve_x=10**17) as srv:
+        for lam in (10.0, 100.0, 1000.0, 10000.0):
+            n = int(min(len(pool), max(30, 3 * lam)))
+            gaps = rng.exponential(1.0 / lam, n)
+            xs = pool[:n]
+            t0 = time.perf_counter()
+            got, ls = srv.replay(xs, np.cumsum(gaps).tolist())
+            wall = time.perf_counter() - t0
+            assert got == [truth[x] for x in xs], "served answer differs from the standalone answer"
+            ls = sorted(ls)
+            rows.append({"lambda": lam, "requests": n, "p50_ms": ls[len(ls) // 2],
+                         "p99_ms": ls[min(len(ls) - 1, int(0.99 * len(ls)))], "qps": n / wall})
+        st = srv.stats()
+    own.close()
+    return {"workload": "x = floor(10^e), e ~ U[10,17]; Poisson arrivals; default_rng(1)",
+            "lanes": args.serve_lanes, "rates": rows, "plain": plain,
+            "batches": st["batches"], "max_batch_seen": st["max_batch_seen"]}
+
+
 def dist_setup():
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -256,6 +317,8 @@ def main():
     ap.add_argument("--ref-step-s", type=float, default=20.0)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--graph", type=int, default=1, help="also time the batch as one CUDA graph launch")
+    ap.add_argument("--serve", type=int, default=1, help="serving sweep and the [1e10,1e15] target check")
+    ap.add_argument("--serve-lanes", type=int, default=4)
     args = ap.parse_args()
     world, rank, local = dist_setup()
     if args.impl == "reference":
@@ -335,6 +398,11 @@ def main():
         plain = {"value": len(sub) / (sum(lat) / 1000.0), "unit": UNIT, "queries": len(sub),
                  "p50_ms": lat[len(lat) // 2], "p99_ms": lat[min(len(lat) - 1, int(len(lat) * 0.99))]}
 
+    target = None
+    serving = None
+    if rank == 0 and args.serve:
+        target = target_ratio(cpx, ctx, args)
+        serving = serve_sweep(cpx, ctx, args)
     if rank != 0:
         return
     hbm, kind = peaks()
@@ -360,6 +428,8 @@ def main():
         "host_ms": {k: round(statistics.median(h[k] for h in host_stats), 3)
                     for k in ("roots_ms", "tables_ms", "plan_ms", "launch_ms", "wait_ms")},
         "graph": graph,
+        "target_1e10_1e15": target,
+        "serving": serving,
         "plain": plain,
         "batched_over_plain": (value / plain["value"]) if plain else None,
         "e2e_over_plain": ((nq / t_e2e) / plain["value"]) if plain else None,

@@ -22,7 +22,8 @@ Python int; 64- and 128-bit overloads are chosen by the size of x.
 """
 import ctypes
 
-from ._lib import BatchStats, CpxError, ExtensionMissing, Params, Terms, U128, header_symbols, load  # noqa: F401
+from ._lib import (BatchStats, CpxError, ExtensionMissing, Params, ServeConfig, ServeCounters, Terms, U128,  # noqa: F401
+                   header_symbols, load)
 
 __all__ = [
     "Context", "context", "P2", "S2_trivial", "Ordinary", "S2_easy", "S2hard", "pi_deleglise_rivat",
@@ -292,6 +293,75 @@ def pi_batch(xs, alpha=None, c=6, hard_log2_bits=0, hard_threads=0, wide=False, 
     p = _params(alpha, c, hard_log2_bits, hard_threads, wide, graph)
     ctx.call("cpx_pi_batch", arr, n, ctypes.byref(p), out)
     return [out[i].value() for i in range(n)]
+
+
+class Server:
+    """Continuous batching of pi(x) requests (cpx_serve_*): `lanes` worker
+    streams share the context's resident tables; while the server exists the
+    context answers no other call."""
+
+    def __init__(self, ctx, lanes=4, max_batch=4096, admit_fraction=0.5, reserve_x=0, alpha=None, c=6,
+                 hard_log2_bits=0, hard_threads=0, graph=False):
+        self.ctx = ctx
+        self.L = ctx.L
+        cfg = ServeConfig()
+        cfg.lanes = lanes
+        cfg.max_batch = max_batch
+        cfg.admit_fraction = admit_fraction
+        cfg.reserve_x = U128.of(reserve_x)
+        cfg.params = _params(alpha, c, hard_log2_bits, hard_threads, False, graph)
+        h = ctypes.c_void_p()
+        rc = self.L.cpx_serve_create(ctx.h, ctypes.byref(cfg), ctypes.byref(h))
+        if rc != 0:
+            raise CpxError(rc, self.L.cpx_last_error(ctx.h).decode())
+        self.h = h
+
+    def _check(self, rc):
+        if rc != 0:
+            raise CpxError(rc, self.L.cpx_serve_last_error(self.h).decode())
+
+    def submit(self, x):
+        t = ctypes.c_uint64()
+        self._check(self.L.cpx_serve_submit(self.h, U128.of(x), ctypes.byref(t)))
+        return t.value
+
+    def wait(self, ticket):
+        """(pi, latency_ms) of a submitted request."""
+        o, ms = U128(), ctypes.c_double()
+        self._check(self.L.cpx_serve_wait(self.h, ticket, ctypes.byref(o), ctypes.byref(ms)))
+        return o.value(), ms.value
+
+    def replay(self, xs, arrival_s):
+        """Submits xs[i] at arrival_s[i] seconds from now; returns (pis, latencies_ms)."""
+        n = len(xs)
+        arr = _u128_array(xs)
+        ts = (ctypes.c_double * max(n, 1))(*arrival_s)
+        out = (U128 * max(n, 1))()
+        lat = (ctypes.c_double * max(n, 1))()
+        self._check(self.L.cpx_serve_replay(self.h, arr, ts, n, out, lat))
+        return [out[i].value() for i in range(n)], [lat[i] for i in range(n)]
+
+    def stats(self):
+        st = ServeCounters()
+        self._check(self.L.cpx_serve_stats(self.h, ctypes.byref(st)))
+        return st.as_dict()
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.L.cpx_serve_destroy(self.h)
+            self.h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 def terms_batch(xs, ys=None, alpha=None, c=6, hard_log2_bits=0, hard_threads=0, wide=False, graph=False,

@@ -94,6 +94,32 @@ class Params(ctypes.Structure):
     ]
 
 
+class ServeConfig(ctypes.Structure):
+    _fields_ = [
+        ("lanes", ctypes.c_uint32),
+        ("max_batch", ctypes.c_uint32),
+        ("admit_fraction", ctypes.c_double),
+        ("reserve_x", U128),
+        ("params", Params),
+    ]
+
+
+class ServeCounters(ctypes.Structure):
+    _fields_ = [
+        ("submitted", ctypes.c_uint64),
+        ("completed", ctypes.c_uint64),
+        ("failed", ctypes.c_uint64),
+        ("pending", ctypes.c_uint64),
+        ("batches", ctypes.c_uint64),
+        ("max_batch_seen", ctypes.c_uint64),
+        ("table_growths", ctypes.c_uint64),
+        ("busy_ms", ctypes.c_double),
+    ]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
 P = ctypes.c_void_p
 PP = ctypes.POINTER(ctypes.c_void_p)
 u16, u32, u64, i32, i64 = ctypes.c_uint16, ctypes.c_uint32, ctypes.c_uint64, ctypes.c_int32, ctypes.c_int64
@@ -160,6 +186,14 @@ _SIGS = {
     "cpx_pi_batch": (ctypes.c_int, [P, pU, ctypes.c_size_t, ctypes.POINTER(Params), pU]),
     "cpx_terms_batch": (ctypes.c_int, [P, pU, pu64, ctypes.c_size_t, ctypes.POINTER(Params), ctypes.POINTER(Terms)]),
     "cpx_mem_info": (ctypes.c_int, [P, pu64, pu64]),
+    "cpx_serve_create": (ctypes.c_int, [P, ctypes.POINTER(ServeConfig), PP]),
+    "cpx_serve_destroy": (ctypes.c_int, [P]),
+    "cpx_serve_submit": (ctypes.c_int, [P, U128, pu64]),
+    "cpx_serve_wait": (ctypes.c_int, [P, u64, pU, ctypes.POINTER(ctypes.c_double)]),
+    "cpx_serve_replay": (ctypes.c_int, [P, pU, ctypes.POINTER(ctypes.c_double), ctypes.c_size_t, pU,
+                                        ctypes.POINTER(ctypes.c_double)]),
+    "cpx_serve_stats": (ctypes.c_int, [P, ctypes.POINTER(ServeCounters)]),
+    "cpx_serve_last_error": (ctypes.c_char_p, [P]),
 }
 
 _lib = None

@@ -17,6 +17,10 @@ template <class F> int guarded(cpx_ctx *ctx, F &&f)
 {
     if (!ctx) return CPX_EINVAL;
     std::lock_guard<std::recursive_mutex> lk(ctx->mu);
+    if (ctx->server_attached) {
+        ctx->last_error = "the context serves a cpx_server; destroy the server first";
+        return CPX_ESTATE;
+    }
     try {
         cudaError_t e = cudaSetDevice(ctx->device);
         if (e != cudaSuccess) fail(CPX_ECUDA, std::string("cudaSetDevice: ") + cudaGetErrorString(e));
@@ -51,6 +55,62 @@ void one(cpx_ctx *ctx, u128 x, uint64_t y, uint32_t c, unsigned terms, i128 *t7,
 
 }  // namespace
 
+namespace cpx {
+
+int init_context(cpx_ctx *ctx, int device)
+{
+    ctx->device = device;
+    cudaError_t e = cudaSetDevice(device);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&ctx->sm_count, cudaDevAttrMultiProcessorCount, device);
+    int optin = 0;
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device);
+    for (cudaEvent_t *ev : {&ctx->ev_hard0, &ctx->ev_hard1, &ctx->ev_b0, &ctx->ev_b1, &ctx->ev_t0, &ctx->ev_t1})
+        if (e == cudaSuccess) e = cudaEventCreate(ev);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return CPX_ECUDA;
+    }
+    ctx->smem_optin = (size_t)optin;
+    return CPX_OK;
+}
+
+void release_context(cpx_ctx *ctx)
+{
+    std::lock_guard<std::recursive_mutex> lk(ctx->mu);
+    cudaSetDevice(ctx->device);
+    if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+    Tables &tb = ctx->tab;
+    if (!ctx->tables_borrowed) {
+        if (tb.T) cudaFree(tb.T);
+        if (tb.P) cudaFree(tb.P);
+        if (tb.MU) cudaFree(tb.MU);
+        if (tb.WH) cudaFree(tb.WH);
+    }
+    tb = Tables{};
+    for (auto &b : ctx->b_scan) b.release();
+    ctx->b_segtot.release();
+    ctx->b_small.release();
+    ctx->b_tmp.release();
+    ctx->b_win.release();
+    ctx->b_win2.release();
+    for (auto &b : ctx->b_work) b.release();
+    ctx->b_flush.release();
+    ctx->b_jobs.release();
+    ctx->b_jobctl.release();
+    ctx->b_snap.release();
+    if (ctx->graph_exec) cudaGraphExecDestroy(ctx->graph_exec);
+    ctx->graph_exec = nullptr;
+    for (cudaEvent_t *ev : {&ctx->ev_hard0, &ctx->ev_hard1, &ctx->ev_b0, &ctx->ev_b1, &ctx->ev_t0, &ctx->ev_t1}) {
+        if (*ev) cudaEventDestroy(*ev);
+        *ev = nullptr;
+    }
+    if (ctx->stream) cudaStreamDestroy(ctx->stream);
+    ctx->stream = nullptr;
+}
+
+}  // namespace cpx
+
 extern "C" {
 
 const char *cpx_version(void) { return "cudapix_b200 0.1 (sm_100a)"; }
@@ -61,23 +121,12 @@ int cpx_create(int device, cpx_ctx **out)
     *out = nullptr;
     cpx_ctx *ctx = new (std::nothrow) cpx_ctx();
     if (!ctx) return CPX_EOOM;
-    ctx->device = device;
-    cudaError_t e = cudaSetDevice(device);
-    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking);
-    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&ctx->sm_count, cudaDevAttrMultiProcessorCount, device);
-    int optin = 0;
-    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device);
-    if (e == cudaSuccess) e = cudaEventCreate(&ctx->ev_hard0);
-    if (e == cudaSuccess) e = cudaEventCreate(&ctx->ev_hard1);
-    if (e == cudaSuccess) e = cudaEventCreate(&ctx->ev_b0);
-    if (e == cudaSuccess) e = cudaEventCreate(&ctx->ev_b1);
-    if (e == cudaSuccess) e = cudaEventCreate(&ctx->ev_t0);
-    if (e == cudaSuccess) e = cudaEventCreate(&ctx->ev_t1);
-    if (e != cudaSuccess) {
+    const int rc = init_context(ctx, device);
+    if (rc != CPX_OK) {
+        release_context(ctx);
         delete ctx;
-        return (e == cudaErrorNoDevice || e == cudaErrorInsufficientDriver) ? CPX_ECUDA : CPX_ECUDA;
+        return rc;
     }
-    ctx->smem_optin = (size_t)optin;
     *out = ctx;
     return CPX_OK;
 }
@@ -85,33 +134,8 @@ int cpx_create(int device, cpx_ctx **out)
 int cpx_destroy(cpx_ctx *ctx)
 {
     if (!ctx) return CPX_EINVAL;
-    {
-        std::lock_guard<std::recursive_mutex> lk(ctx->mu);
-        cudaSetDevice(ctx->device);
-        if (ctx->stream) cudaStreamSynchronize(ctx->stream);
-        Tables &tb = ctx->tab;
-        if (tb.T) cudaFree(tb.T);
-        if (tb.P) cudaFree(tb.P);
-        if (tb.MU) cudaFree(tb.MU);
-        if (tb.WH) cudaFree(tb.WH);
-        for (auto &b : ctx->b_scan) b.release();
-        ctx->b_segtot.release();
-        ctx->b_small.release();
-        ctx->b_tmp.release();
-        ctx->b_win.release();
-        ctx->b_win2.release();
-        for (auto &b : ctx->b_work) b.release();
-        ctx->b_flush.release();
-        ctx->b_jobs.release();
-        ctx->b_jobctl.release();
-        ctx->b_snap.release();
-        if (ctx->graph_exec) cudaGraphExecDestroy(ctx->graph_exec);
-        if (ctx->ev_hard0) cudaEventDestroy(ctx->ev_hard0);
-        if (ctx->ev_hard1) cudaEventDestroy(ctx->ev_hard1);
-        for (cudaEvent_t ev : {ctx->ev_b0, ctx->ev_b1, ctx->ev_t0, ctx->ev_t1})
-            if (ev) cudaEventDestroy(ev);
-        if (ctx->stream) cudaStreamDestroy(ctx->stream);
-    }
+    if (ctx->server_attached) return CPX_ESTATE;
+    release_context(ctx);
     delete ctx;
     return CPX_OK;
 }

@@ -117,9 +117,13 @@ __device__ __forceinline__ uint64_t cpx_pi_dev(const cpx_pient *__restrict__ T, 
 //   v = n * rd is within 0.15 of n/d when n/d < 2^44, so trunc(v) is
 //   floor(n/d) - 1, floor(n/d) or floor(n/d) + 1, and the sign of
 //   n - trunc(v) d settles which.  Other operands use the hardware path.
+// the hardware-path 64-bit quotient, kept out of line: every inlined copy of
+// it would cost the calling loops instruction-cache space
+static __device__ __noinline__ uint64_t cpx_udiv_slow(uint64_t n, uint64_t d) { return n / d; }
+
 __device__ __forceinline__ uint64_t cpx_udiv_leaf(uint64_t n, uint64_t d)
 {
-    if ((d >> 32) || (n >> 44) >= d) return n / d;
+    if ((d >> 32) || (n >> 44) >= d) return cpx_udiv_slow(n, d);
     const uint32_t d32 = (uint32_t)d;
     const double r = (double)__frcp_rn(__uint2float_rn(d32));
     const double dd = (double)d32;

@@ -91,6 +91,8 @@ struct cpx_ctx {
     std::recursive_mutex mu;
     std::vector<uint32_t> hP;  // host mirror of tab.P (launch planning only)
     uint64_t hP_version = 0;
+    bool tables_borrowed = false;  // a serving lane: tab points at the server's tables, never grown here
+    bool server_attached = false;  // the context's tables serve a cpx_server
     int sm_count = 148;
     size_t smem_optin = 0;
     // tuning
@@ -137,6 +139,11 @@ uint64_t extract_primes_u64(cpx_ctx *ctx, uint64_t lo, uint64_t hi, uint64_t *d_
 // mu / lpf sieve over odd n in [lo, hi), lo even; any of the outputs may be null.
 void mulpf_sieve(cpx_ctx *ctx, uint64_t lo, uint64_t hi, int8_t *mu, uint32_t *lpf32,
                  uint64_t *lpf64, int32_t *packed);
+
+// context set-up and tear-down shared by cpx_create/cpx_destroy and the
+// serving lanes (a lane with tables_borrowed leaves the tables alone)
+int init_context(cpx_ctx *ctx, int device);
+void release_context(cpx_ctx *ctx);
 
 // counts launched kernels for the gpu_launches report
 inline void note_launch(cpx_ctx *ctx, uint64_t n = 1) { ctx->launches += n; }

@@ -248,6 +248,92 @@ template <class F> static void launch_as_graph(cpx_ctx *ctx, F &&launches)
     CPX_CUDA(cudaGraphLaunch(ctx->graph_exec, ctx->stream));
 }
 
+// Roots, y and validity of every query of a request, and the table bounds
+// the batch needs (pi table to N, mu/lpf to Y, primes to P, wheel for c).
+void compute_needs(const BatchReq &rq, std::vector<QD> &qd, TableNeed &need, bool &wide)
+{
+    const uint32_t Q = (uint32_t)rq.n;
+    const uint32_t c = rq.c;
+    const unsigned mask = rq.terms;
+    if (c < 1 || c > 8) fail(CPX_EINVAL, "c must be in 1..8");
+    qd.assign(Q, QD{});
+    uint64_t N = 1 << 16, Y = 0, Pneed = 64;
+    wide = rq.wide;
+    bool any_direct = false;
+    for (uint32_t i = 0; i < Q; i++) {
+        QD &d = qd[i];
+        memset(&d, 0, sizeof(d));
+        const u128 x = rq.xs[i];
+        d.x = x;
+        d.c = c;
+        if (x >> 64) wide = true;
+        const uint64_t sx = cpx_isqrt(x), cx = cpx_icbrt(x), r4 = cpx_iroot4(x);
+        uint64_t y = rq.ys ? rq.ys[i] : 0;
+        if (mask == TERM_PI) {
+            if (!y) y = default_y(x, rq.alpha_num, rq.alpha_den);
+            if (!dr_domain_ok(x, y, c)) {
+                if (x >= ((u128)1 << 32)) fail(CPX_EINVAL, "y outside the Deleglise-Rivat domain for this x");
+                d.direct = 1;
+                d.y = 0;
+                any_direct = true;
+                N = std::max<uint64_t>(N, (uint64_t)x + 1);
+                continue;
+            }
+        } else if (y == 0) {
+            fail(CPX_EINVAL, "y must be >= 1");
+        }
+        if (y >= 0x7FFFFFF0ull && (mask & (TERM_ORD | TERM_HARD)))
+            fail(CPX_ERANGE, "y must be below 2^31 for the mu/lpf table");
+        const u128 z128 = x / y;
+        if (z128 >> 63) fail(CPX_ERANGE, "x / y must be below 2^63");
+        d.y = y;
+        d.z = (uint64_t)z128;
+        d.sx = sx;
+        d.cx = cx;
+        d.r4 = r4;
+        d.tx = cpx_isqrt(z128);
+        if (mask & TERM_P2) N = std::max<uint64_t>(N, std::max(d.z, sx) + 1);
+        if (mask & TERM_TRIV) N = std::max<uint64_t>(N, std::max(y, cx) + 1);
+        if (mask & TERM_EASY) N = std::max<uint64_t>(N, std::max(sx, y) + 1);
+        if (mask & (TERM_ORD | TERM_HARD)) Y = std::max(Y, y);
+        if (mask & TERM_HARD) {
+            Pneed = std::max<uint64_t>(Pneed, r4 + 1);
+            // carries below p_b^2 come from the pi table; prime m of the sparse levels from its bitmap
+            N = std::max<uint64_t>(N, std::max<uint64_t>(r4 * r4 + 2, y + 1));
+        }
+        if (mask & TERM_EASY) {
+            // the p of the easy leaves (p <= icbrt(x)) and the u primes of their
+            // clustered parts (u <= min(p^2, sqrt(x/p)) <= x^(2/5))
+            Pneed = std::max<uint64_t>(Pneed, std::max<uint64_t>(cx + 1, easy_u_bound(x)));
+            Y = std::max(Y, y);
+        }
+        if (mask == TERM_PI) N = std::max<uint64_t>(N, y + 1);
+    }
+    if (N > rq.max_table_n) fail(CPX_ERANGE, "pi table bound exceeds the configured limit");
+    need.P = std::max<uint64_t>(Pneed, cpx_isqrt(Y + 1) + 2);
+    need.N = ((mask & (TERM_P2 | TERM_TRIV | TERM_EASY | TERM_HARD)) || mask == TERM_PI || any_direct) ? N : 0;
+    need.Y = Y ? Y + 8 : 0;
+    need.c = (mask & TERM_ORD) ? c : 0;
+}
+
+bool tables_cover(const cpx_ctx *ctx, const TableNeed &need)
+{
+    const Tables &tb = ctx->tab;
+    if (!tb.P || tb.prm_max < need.P) return false;
+    if (need.N && (!tb.T || tb.tab_n < need.N)) return false;
+    if (need.Y && (!tb.MU || tb.mu_n < need.Y)) return false;
+    if (need.c && (!tb.WH || tb.wh_c != need.c)) return false;
+    return true;
+}
+
+void grow_tables(cpx_ctx *ctx, const TableNeed &need)
+{
+    ensure_primes(ctx, need.P);
+    if (need.N) ensure_pitable(ctx, need.N);
+    if (need.Y) ensure_mulpf(ctx, need.Y);
+    if (need.c) ensure_wheel(ctx, need.c);
+}
+
 // Runs f(0) .. f(n - 1) on up to 16 host threads (the calling thread
 // included); the first exception thrown by any f is rethrown here.
 constexpr size_t kPlanBlock = 64;  // queries per planning block
@@ -304,68 +390,17 @@ void run_batch(cpx_ctx *ctx, const BatchReq &rq)
     const unsigned mask = rq.terms;
 
     // ---- host planning: roots, y, validity, table bounds
-    std::vector<QD> qd(Q);
-    uint64_t N = 1 << 16, Y = 0, Pneed = 64;
-    bool wide = rq.wide;
-    for (uint32_t i = 0; i < Q; i++) {
-        QD &d = qd[i];
-        memset(&d, 0, sizeof(d));
-        const u128 x = rq.xs[i];
-        d.x = x;
-        d.c = c;
-        if (x >> 64) wide = true;
-        const uint64_t sx = cpx_isqrt(x), cx = cpx_icbrt(x), r4 = cpx_iroot4(x);
-        uint64_t y = rq.ys ? rq.ys[i] : 0;
-        if (mask == TERM_PI) {
-            if (!y) y = default_y(x, rq.alpha_num, rq.alpha_den);
-            if (!dr_domain_ok(x, y, c)) {
-                if (x >= ((u128)1 << 32)) fail(CPX_EINVAL, "y outside the Deleglise-Rivat domain for this x");
-                d.direct = 1;
-                d.y = 0;
-                N = std::max<uint64_t>(N, (uint64_t)x + 1);
-                continue;
-            }
-        } else if (y == 0) {
-            fail(CPX_EINVAL, "y must be >= 1");
-        }
-        if (y >= 0x7FFFFFF0ull && (mask & (TERM_ORD | TERM_HARD)))
-            fail(CPX_ERANGE, "y must be below 2^31 for the mu/lpf table");
-        const u128 z128 = x / y;
-        if (z128 >> 63) fail(CPX_ERANGE, "x / y must be below 2^63");
-        d.y = y;
-        d.z = (uint64_t)z128;
-        d.sx = sx;
-        d.cx = cx;
-        d.r4 = r4;
-        d.tx = cpx_isqrt(z128);
-        if (mask & TERM_P2) N = std::max<uint64_t>(N, std::max(d.z, sx) + 1);
-        if (mask & TERM_TRIV) N = std::max<uint64_t>(N, std::max(y, cx) + 1);
-        if (mask & TERM_EASY) N = std::max<uint64_t>(N, std::max(sx, y) + 1);
-        if (mask & (TERM_ORD | TERM_HARD)) Y = std::max(Y, y);
-        if (mask & TERM_HARD) {
-            Pneed = std::max<uint64_t>(Pneed, r4 + 1);
-            // carries below p_b^2 come from the pi table; prime m of the sparse levels from its bitmap
-            N = std::max<uint64_t>(N, std::max<uint64_t>(r4 * r4 + 2, y + 1));
-        }
-        if (mask & TERM_EASY) {
-            // the p of the easy leaves (p <= icbrt(x)) and the u primes of their
-            // clustered parts (u <= min(p^2, sqrt(x/p)) <= x^(2/5))
-            Pneed = std::max<uint64_t>(Pneed, std::max<uint64_t>(cx + 1, easy_u_bound(x)));
-            Y = std::max(Y, y);
-        }
-        if (mask == TERM_PI) N = std::max<uint64_t>(N, y + 1);
-    }
-    if (N > rq.max_table_n) fail(CPX_ERANGE, "pi table bound exceeds the configured limit");
-
+    std::vector<QD> qd;
+    TableNeed need;
+    bool wide = false;
+    compute_needs(rq, qd, need, wide);
     st.roots_ms = ms_since(clk);
     // ---- tables
-    ensure_primes(ctx, std::max<uint64_t>(Pneed, cpx_isqrt(Y + 1) + 2));
-    bool any_direct = false;
-    for (const QD &d : qd) any_direct |= d.direct != 0;
-    const bool need_tab = (mask & (TERM_P2 | TERM_TRIV | TERM_EASY | TERM_HARD)) || mask == TERM_PI || any_direct;
-    if (need_tab) ensure_pitable(ctx, N);
-    if (Y) ensure_mulpf(ctx, Y + 8);
-    if (mask & TERM_ORD) ensure_wheel(ctx, c);
+    if (ctx->tables_borrowed) {
+        if (!tables_cover(ctx, need)) fail(CPX_ESTATE, "the shared tables do not cover this batch");
+    } else {
+        grow_tables(ctx, need);
+    }
     const std::vector<uint32_t> &hP = host_primes(ctx);
     st.tables_ms = ms_since(clk);
 

@@ -1,6 +1,7 @@
 // driver.h -- batch execution entry point shared by the C-ABI layer.
 #pragma once
 #include "cpx_internal.h"
+#include "terms.cuh"
 
 namespace cpx {
 
@@ -29,7 +30,16 @@ struct BatchReq {
     bool graph = false;  // one CUDA graph launch for the batch's kernels
 };
 
+// table bounds of a batch: pi table to N, mu/lpf to Y, primes to P, wheel for c (0 = not needed)
+struct TableNeed {
+    uint64_t N = 0, Y = 0, P = 0;
+    uint32_t c = 0;
+};
+
 void run_batch(cpx_ctx *ctx, const BatchReq &rq);
+void compute_needs(const BatchReq &rq, std::vector<QD> &qd, TableNeed &need, bool &wide);
+bool tables_cover(const cpx_ctx *ctx, const TableNeed &need);
+void grow_tables(cpx_ctx *ctx, const TableNeed &need);
 uint64_t default_y(u128 x, uint32_t num, uint32_t den);
 uint32_t alpha_milli(u128 x);
 bool dr_domain_ok(u128 x, uint64_t y, uint32_t c);

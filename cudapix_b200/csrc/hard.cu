@@ -27,6 +27,7 @@
 // c ^ ((c >> log2 CPT) & 7) so the owners' 128-bit accesses are free of bank
 // conflicts.  Counters are indexed by the unswizzled chunk.
 #include <algorithm>
+#include <mutex>
 
 #include "kern_common.cuh"
 
@@ -98,6 +99,119 @@ __host__ __device__ __forceinline__ size_t hard_smem(uint32_t lbits, uint32_t th
     return o;
 }
 
+// Pre-sieve of one lane's chunks [c0, c0 + CPT) of the segment starting at lo
+// with p_2 .. p_c (residue masks per 32-bit word); writes the bitmap and the
+// chunk counters and returns the lane's survivors.  Runs once per segment, so
+// it is kept out of line (instruction-cache footprint of the level loop).
+__device__ __noinline__ uint32_t presieve(uint32_t *bm, uint8_t *cnt8, const uint32_t *__restrict__ P, uint32_t c,
+                                          uint64_t lo, uint32_t c0, uint32_t CPT, int s)
+{
+    uint32_t pr[8], rr[8], st[8], Mp[8];
+    const uint32_t np = c - 1;
+    const uint32_t w0 = 4 * c0;
+#pragma unroll
+    for (uint32_t i = 0; i < 8; i++) {
+        if (i < np) {
+            pr[i] = P[i + 1];
+            rr[i] = (uint32_t)(((lo + 1) % pr[i] + (64ull * w0) % pr[i]) % pr[i]);
+            st[i] = 64u % pr[i];
+            Mp[i] = every_pth_bit(pr[i]);
+        }
+    }
+    uint32_t cnt0 = 0;
+    for (uint32_t j = 0; j < CPT; j++) {
+        uint32_t wv[4];
+#pragma unroll
+        for (int k = 0; k < 4; k++) {
+            uint32_t m = 0;
+#pragma unroll
+            for (uint32_t i = 0; i < 8; i++) {
+                if (i < np) {
+                    m |= mult_mask(rr[i], pr[i], Mp[i]);
+                    rr[i] += st[i];
+                    if (rr[i] >= pr[i]) rr[i] -= pr[i];
+                }
+            }
+            wv[k] = ~m;
+        }
+        const uint32_t cc = __popc(wv[0]) + __popc(wv[1]) + __popc(wv[2]) + __popc(wv[3]);
+        cnt0 += cc;
+        cnt8[c0 + j] = (uint8_t)cc;
+        reinterpret_cast<uint4 *>(bm)[swz(c0 + j, s)] = make_uint4(wv[0], wv[1], wv[2], wv[3]);
+    }
+    return cnt0;
+}
+
+// Writes one lane's share of a leaf-set snapshot: its chunks of the
+// sub-segment bitmap and the survivor prefix of each chunk (pre = survivors of
+// the sub-segment before the lane's first chunk).  Out of line: rare path.
+__device__ __noinline__ void snapshot_chunks(uint4 *sb, uint32_t *spre, const uint32_t *bm, const uint8_t *cnt8,
+                                             uint32_t cw0, uint32_t c0, uint32_t CPT, int s, uint32_t pre)
+{
+    for (uint32_t jj = 0; jj < CPT; jj++) {
+        sb[cw0 + jj] = reinterpret_cast<const uint4 *>(bm)[swz(c0 + jj, s)];
+        spre[cw0 + jj] = pre;
+        pre += cnt8[c0 + jj];
+    }
+}
+
+// The valid m of one 16-byte group of packed mu*lpf (4 odd m, indices 4g..4g+3
+// within [i_lo, i_hi]): squarefree with lpf > p.  Bit k of *neg: mu(m) = -1.
+__device__ __forceinline__ uint32_t valid_group(int4 v4, uint64_t g, uint64_t i_lo, uint64_t i_hi, uint32_t p,
+                                                uint32_t *neg)
+{
+    const int32_t vals[4] = {v4.x, v4.y, v4.z, v4.w};
+    uint32_t vm = 0, ng = 0;
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+        const uint64_t i = 4 * g + k;
+        const int32_t v = vals[k];
+        const uint32_t av = (uint32_t)(v > 0 ? v : -v);
+        if (i >= i_lo && i <= i_hi && v != 0 && av > p) {
+            vm |= 1u << k;
+            if (v < 0) ng |= 1u << k;
+        }
+    }
+    *neg = ng;
+    return vm;
+}
+
+// Parameters of one level (p = p_b) for one warp's sub-segment [lo_w, hi_w):
+// xp = x/p, the candidate range (mlo, mhi] of m (m > y/p, u = xp/m in the
+// sub-segment, m <= x/p^3 for a hard leaf), the residue of lo_w + 1 mod p and
+// the bit of the first odd multiple of p (0xFFFFFFFF: none).  Computed for 32
+// levels at a time, one per lane; out of line to keep the level loop small.
+template <class XT> struct LvlPar {
+    XT xp;
+    uint32_t p, mlo, mhi, r0, i0;
+};
+
+template <class XT>
+__device__ __noinline__ void level_params(LvlPar<XT> &o, XT x, uint64_t y, uint64_t p, uint64_t lo_w, uint64_t hi_w)
+{
+    const XT xp = x / (XT)p;
+    uint64_t mlo = y / p;
+    const XT t1 = cpx_qdiv(xp, hi_w);
+    if (t1 > (XT)mlo) mlo = (uint64_t)t1;
+    uint64_t mhi = y;
+    if (lo_w) {
+        const XT t2 = cpx_qdiv(xp, lo_w);
+        if (t2 < (XT)mhi) mhi = (uint64_t)t2;
+    }
+    const XT t3 = xp / (XT)(p * p);  // hard leaves only: m <= x/p^3
+    if (t3 < (XT)mhi) mhi = (uint64_t)t3;
+    if (mhi < mlo) mhi = mlo;
+    o.p = (uint32_t)p;
+    o.xp = xp;
+    o.mlo = (uint32_t)mlo;
+    o.mhi = (uint32_t)mhi;
+    const uint64_t r0 = (lo_w + 1) - cpx_udiv_leaf(lo_w + 1, p) * p;
+    o.r0 = (uint32_t)r0;
+    uint64_t m = lo_w + 1 + (r0 ? p - r0 : 0);
+    if ((m & 1) == 0) m += p;
+    o.i0 = (m < hi_w) ? (uint32_t)((m - lo_w - 1) >> 1) : 0xFFFFFFFFu;
+}
+
 template <class XT>
 __global__ void __launch_bounds__(512, 2) k_hard(const QD *__restrict__ qd, uint32_t Q,
                                               const uint64_t *__restrict__ pre_seg, uint64_t total,
@@ -150,43 +264,9 @@ __global__ void __launch_bounds__(512, 2) k_hard(const QD *__restrict__ qd, uint
     uint32_t *wl = loff + 32 * warp;  // this warp's lane prefixes
 
     const uint32_t c0 = CPT * tid;  // first owned chunk (of the segment)
-    const uint32_t w0 = 4 * c0;     // first owned word
     const uint32_t cw0 = c0 - CPT * 32 * warp;  // first owned chunk of the sub-segment
     // ---- pre-sieve with p_2 .. p_c; chunk counters
-    uint32_t cnt0 = 0;
-    {
-        uint32_t pr[8], rr[8], st[8], Mp[8];
-        const uint32_t np = c - 1;
-#pragma unroll
-        for (uint32_t i = 0; i < 8; i++) {
-            if (i < np) {
-                pr[i] = P[i + 1];
-                rr[i] = (uint32_t)(((lo + 1) % pr[i] + (64ull * w0) % pr[i]) % pr[i]);
-                st[i] = 64u % pr[i];
-                Mp[i] = every_pth_bit(pr[i]);
-            }
-        }
-        for (uint32_t j = 0; j < CPT; j++) {
-            uint32_t wv[4];
-#pragma unroll
-            for (int k = 0; k < 4; k++) {
-                uint32_t m = 0;
-#pragma unroll
-                for (uint32_t i = 0; i < 8; i++) {
-                    if (i < np) {
-                        m |= mult_mask(rr[i], pr[i], Mp[i]);
-                        rr[i] += st[i];
-                        if (rr[i] >= pr[i]) rr[i] -= pr[i];
-                    }
-                }
-                wv[k] = ~m;
-            }
-            const uint32_t cc = __popc(wv[0]) + __popc(wv[1]) + __popc(wv[2]) + __popc(wv[3]);
-            cnt0 += cc;
-            cnt8[c0 + j] = (uint8_t)cc;
-            reinterpret_cast<uint4 *>(bm)[swz(c0 + j, s)] = make_uint4(wv[0], wv[1], wv[2], wv[3]);
-        }
-    }
+    const uint32_t cnt0 = presieve(bm, cnt8, P, c, lo, c0, CPT, s);
     uint32_t tot = __reduce_add_sync(FULL, cnt0);  // survivors of this warp's sub-segment
     __syncwarp();
 
@@ -213,32 +293,14 @@ __global__ void __launch_bounds__(512, 2) k_hard(const QD *__restrict__ qd, uint
     for (uint32_t gb = c + 1; gb <= B; gb += 32, grp++) {
         const uint32_t nl = min(32u, B - gb + 1);
         // ---- level parameters, one level per lane
-        uint32_t lp = 0, lmlo = 0, lmhi = 0, lr0 = 0, li0 = 0xFFFFFFFFu;
-        XT lxp = 0;
-        if (lane < nl) {
-            const uint64_t p = P[gb + lane - 1];
-            const XT xp = x / (XT)p;
-            uint64_t mlo = y / p;
-            const XT t1 = xp / (XT)hi_w;
-            if (t1 > (XT)mlo) mlo = (uint64_t)t1;
-            uint64_t mhi = y;
-            if (lo_w) {
-                const XT t2 = xp / (XT)lo_w;
-                if (t2 < (XT)mhi) mhi = (uint64_t)t2;
-            }
-            const XT t3 = xp / (XT)(p * p);  // hard leaves only: m <= x/p^3
-            if (t3 < (XT)mhi) mhi = (uint64_t)t3;
-            if (mhi < mlo) mhi = mlo;
-            lp = (uint32_t)p;
-            lxp = xp;
-            lmlo = (uint32_t)mlo;
-            lmhi = (uint32_t)mhi;
-            const uint64_t r0 = (lo_w + 1) % p;
-            lr0 = (uint32_t)r0;
-            uint64_t m = lo_w + 1 + (r0 ? p - r0 : 0);
-            if ((m & 1) == 0) m += p;
-            li0 = (m < hi_w) ? (uint32_t)((m - lo_w - 1) >> 1) : 0xFFFFFFFFu;
-        }
+        LvlPar<XT> lv;
+        lv.p = 0;
+        lv.mlo = lv.mhi = lv.r0 = 0;
+        lv.i0 = 0xFFFFFFFFu;
+        lv.xp = 0;
+        if (lane < nl) level_params<XT>(lv, x, y, P[gb + lane - 1], lo_w, hi_w);
+        const uint32_t lp = lv.p, lmlo = lv.mlo, lmhi = lv.mhi, lr0 = lv.r0, li0 = lv.i0;
+        const XT lxp = lv.xp;
         LvlOut mine = {0, 0, 0xFFFFFFFFu, 0};
         for (uint32_t k = 0; k < nl; k++) {
             const uint32_t b = gb + k;
@@ -282,12 +344,7 @@ __global__ void __launch_bounds__(512, 2) k_hard(const QD *__restrict__ qd, uint
                         const size_t stride = snap_stride(lbits_sub_max);
                         uint4 *sb = reinterpret_cast<uint4 *>(snap + (size_t)j * stride);
                         uint32_t *spre = reinterpret_cast<uint32_t *>(sb + ((size_t(1) << lbits_sub_max) >> 7));
-                        uint32_t pre = wl[lane];
-                        for (uint32_t jj = 0; jj < CPT; jj++) {
-                            sb[cw0 + jj] = reinterpret_cast<const uint4 *>(bm)[swz(c0 + jj, s)];
-                            spre[cw0 + jj] = pre;
-                            pre += cnt8[c0 + jj];
-                        }
+                        snapshot_chunks(sb, spre, bm, cnt8, cw0, c0, CPT, s, wl[lane]);
                         if (lane == 0) {
                             HardJob J;
                             J.q = q;
@@ -331,21 +388,19 @@ __global__ void __launch_bounds__(512, 2) k_hard(const QD *__restrict__ qd, uint
                         // any squarefree m with lpf(m) > p: 16-byte loads of packed mu*lpf
                         const uint64_t i_lo = ((uint64_t)mlo + 1) >> 1, i_hi = ((uint64_t)mhi - 1) >> 1;
                         for (uint64_t g = (i_lo >> 2) + lane; g <= (i_hi >> 2); g += 32) {
-                            const int4 v4 = __ldg(reinterpret_cast<const int4 *>(MU) + g);
-                            const int32_t vals[4] = {v4.x, v4.y, v4.z, v4.w};
-#pragma unroll
-                            for (int kq = 0; kq < 4; kq++) {
-                                const uint64_t i = 4 * g + kq;
-                                const int32_t v = vals[kq];
-                                if (i < i_lo || i > i_hi || v == 0) continue;
-                                if ((uint32_t)(v > 0 ? v : -v) <= p) continue;
-                                const uint32_t cv = sub_count((uint64_t)cpx_qdiv(xp, 2 * i + 1));
-                                if (v > 0) {
-                                    S -= cv;
-                                    msl -= 1;
-                                } else {
+                            uint32_t neg;
+                            uint32_t vm = valid_group(__ldg(reinterpret_cast<const int4 *>(MU) + g), g, i_lo, i_hi,
+                                                      p, &neg);
+                            while (vm) {
+                                const int kq = __ffs(vm) - 1;
+                                vm &= vm - 1;
+                                const uint32_t cv = sub_count((uint64_t)cpx_qdiv(xp, 2 * (4 * g + kq) + 1));
+                                if ((neg >> kq) & 1u) {
                                     S += cv;
                                     msl += 1;
+                                } else {
+                                    S -= cv;
+                                    msl -= 1;
                                 }
                             }
                         }
@@ -502,21 +557,18 @@ __global__ void __launch_bounds__(kThreads) k_hard_leaves(const HardJob *__restr
             for (uint64_t k = 0; k < kJobGroups / 32; k++) {
                 const uint64_t g = g0 + 32 * k + lane;
                 if (g > gl) break;
-                const int4 v4 = __ldg(reinterpret_cast<const int4 *>(MU) + g);
-                const int32_t vals[4] = {v4.x, v4.y, v4.z, v4.w};
-#pragma unroll
-                for (int kq = 0; kq < 4; kq++) {
-                    const uint64_t i = 4 * g + kq;
-                    const int32_t v = vals[kq];
-                    if (i < i_lo || i > i_hi || v == 0) continue;
-                    if ((uint32_t)(v > 0 ? v : -v) <= p) continue;
-                    const uint32_t cv = count((uint64_t)cpx_qdiv(xp, 2 * i + 1));
-                    if (v > 0) {
-                        S -= cv;
-                        ms -= 1;
-                    } else {
+                uint32_t neg;
+                uint32_t vm = valid_group(__ldg(reinterpret_cast<const int4 *>(MU) + g), g, i_lo, i_hi, p, &neg);
+                while (vm) {
+                    const int kq = __ffs(vm) - 1;
+                    vm &= vm - 1;
+                    const uint32_t cv = count((uint64_t)cpx_qdiv(xp, 2 * (4 * g + kq) + 1));
+                    if ((neg >> kq) & 1u) {
                         S += cv;
                         ms += 1;
+                    } else {
+                        S -= cv;
+                        ms -= 1;
                     }
                 }
             }
@@ -679,13 +731,26 @@ template <class XT> static void hard_go(cpx_ctx *ctx, const Plan &pl)
     }
 }
 
+// The dynamic shared-memory limit of k_hard is a property of the function,
+// shared by every context and thread of the process, so it is raised to the
+// device's opt-in maximum once (under a lock) instead of per launch: a lane
+// lowering it while another lane launches a larger segment would fail.
 void prepare_hard(cpx_ctx *ctx, const Plan &pl)
 {
-    (void)ctx;
     if (!pl.n_seg) return;
-    const int smem = (int)hard_smem(pl.lbits_max, pl.hard_threads);
-    if (pl.wide) CPX_CUDA(cudaFuncSetAttribute(k_hard<u128>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-    else CPX_CUDA(cudaFuncSetAttribute(k_hard<uint64_t>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    const size_t smem = hard_smem(pl.lbits_max, pl.hard_threads);
+    if (smem > ctx->smem_optin) fail(CPX_EINVAL, "hard-leaf segment needs more shared memory than a block can have");
+    static std::mutex m;
+    static int done_dev[2] = {-1, -1};
+    std::lock_guard<std::mutex> g(m);
+    const int w = pl.wide ? 1 : 0;
+    if (done_dev[w] == ctx->device) return;
+    if (pl.wide)
+        CPX_CUDA(cudaFuncSetAttribute(k_hard<u128>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ctx->smem_optin));
+    else
+        CPX_CUDA(cudaFuncSetAttribute(k_hard<uint64_t>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)ctx->smem_optin));
+    done_dev[w] = ctx->device;
 }
 
 void launch_hard(cpx_ctx *ctx, const Plan &pl)

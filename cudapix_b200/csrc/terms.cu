@@ -194,7 +194,7 @@ struct EasyP {
 };
 
 template <class XT>
-__device__ __forceinline__ bool easy_plan(XT x, uint64_t y, uint64_t p, uint64_t prm_max,
+__device__ __noinline__ bool easy_plan(XT x, uint64_t y, uint64_t p, uint64_t prm_max,
                                           const cpx_pient *__restrict__ T, XT &xp, EasyP &e)
 {
     xp = x / (XT)p;

@@ -229,6 +229,46 @@ typedef struct {
 int cpx_pi_batch(cpx_ctx *ctx, const cpx_u128 *xs, size_t n, const cpx_params *params,
                  cpx_u128 *out);
 
+/* ---- serving: continuous batching over resident tables -------------------
+ * A server owns `lanes` worker threads, each with its own CUDA stream, batch
+ * buffers and graph; all lanes share the tables of the context the server is
+ * created from (that context answers no other call while the server exists:
+ * CPX_ESTATE).  A free lane takes the waiting requests in arrival order into
+ * one batch while they fit: at most max_batch queries, covered by the
+ * resident tables, and a summed footprint estimate within admit_fraction of
+ * the free HBM (measured at creation) divided among the lanes.  Batches of
+ * different lanes run concurrently on the device.  A request that needs
+ * larger tables waits until every lane is idle; the tables then grow once for
+ * all waiting requests.  Latencies run from arrival (submit, or the scheduled
+ * arrival of a replay) to the moment the batch's results are on the host.
+ * No reference counterpart: the reference answers one x per
+ * deleglise_rivat64/128 object (src/Deleglise-Rivat/deleglise-rivat.cpp:13-80). */
+typedef struct cpx_server cpx_server;
+typedef struct {
+    uint32_t lanes;         /* worker lanes (streams), 1..16; 0 = 4 */
+    uint32_t max_batch;     /* queries per batch; 0 = 4096 */
+    double admit_fraction;  /* share of free HBM for batch buffers, (0, 0.95]; 0 = 0.5 */
+    cpx_u128 reserve_x;     /* grow the tables for x up to this at creation (0: on demand) */
+    cpx_params params;      /* y rule, c, hard-leaf tuning, CPX_BATCH_* flags */
+} cpx_serve_config;
+typedef struct {
+    uint64_t submitted, completed, failed, pending;
+    uint64_t batches, max_batch_seen, table_growths;
+    double busy_ms;         /* summed lane time spent in batches */
+} cpx_serve_counters;
+int cpx_serve_create(cpx_ctx *ctx, const cpx_serve_config *cfg, cpx_server **out);
+/* waits for every admitted request, then stops the lanes */
+int cpx_serve_destroy(cpx_server *srv);
+int cpx_serve_submit(cpx_server *srv, cpx_u128 x, uint64_t *ticket);
+/* blocks until the request is answered; each ticket can be waited for once */
+int cpx_serve_wait(cpx_server *srv, uint64_t ticket, cpx_u128 *pi, double *latency_ms);
+/* submits xs[i] at arrival_s[i] seconds after the call (non-decreasing), waits
+ * for all of them; latency_ms may be NULL */
+int cpx_serve_replay(cpx_server *srv, const cpx_u128 *xs, const double *arrival_s, size_t n, cpx_u128 *pi,
+                     double *latency_ms);
+int cpx_serve_stats(cpx_server *srv, cpx_serve_counters *out);
+const char *cpx_serve_last_error(cpx_server *srv);
+
 /* Every term for n queries in one batched pass; ys[i] = 0 (or ys = NULL)
  * selects the y rule of params.  out[i] as filled by cpx_pi_u128. */
 int cpx_terms_batch(cpx_ctx *ctx, const cpx_u128 *xs, const uint64_t *ys, size_t n,
