@@ -110,6 +110,10 @@ class Context:
     def set_hard_offload(self, min_candidates):
         self.call("cpx_set_hard_offload", min_candidates)
 
+    def set_p2_window(self, limit):
+        """z above `limit`: P2 over pi-table windows (resident table to sqrt x)."""
+        self.call("cpx_set_p2_window", limit)
+
     def set_timing(self, on=True):
         self.call("cpx_set_timing", 1 if on else 0)
 

@@ -140,6 +140,7 @@ _SIGS = {
     "cpx_device_count": (ctypes.c_int, []),
     "cpx_set_hard_params": (ctypes.c_int, [P, u32, u32]),
     "cpx_set_hard_offload": (ctypes.c_int, [P, u32]),
+    "cpx_set_p2_window": (ctypes.c_int, [P, u64]),
     "cpx_last_hard_stats": (ctypes.c_int, [P, ctypes.POINTER(ctypes.c_float), ctypes.POINTER(ctypes.c_double)]),
     "cpx_set_timing": (ctypes.c_int, [P, ctypes.c_int]),
     "cpx_last_batch_ms": (ctypes.c_int, [P, ctypes.POINTER(ctypes.c_float)]),

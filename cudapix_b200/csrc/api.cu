@@ -192,6 +192,14 @@ int cpx_set_hard_offload(cpx_ctx *ctx, uint32_t min_candidates)
     return guarded(ctx, [&] { ctx->hard_offload_min = min_candidates; });
 }
 
+int cpx_set_p2_window(cpx_ctx *ctx, uint64_t limit)
+{
+    return guarded(ctx, [&] {
+        if (limit < (1ull << 20)) fail(CPX_EINVAL, "limit must be at least 2^20");
+        ctx->p2_table_limit = limit;
+    });
+}
+
 int cpx_mem_info(cpx_ctx *ctx, uint64_t *free_bytes, uint64_t *total_bytes)
 {
     return guarded(ctx, [&] {

@@ -100,6 +100,7 @@ struct cpx_ctx {
     uint32_t hard_threads = 256;
     uint32_t hard_offload_min = 1024;  // candidates of a (sub-segment, level) sent to k_hard_leaves
     uint64_t hard_offload_bytes = 4ull << 30;  // snapshot pool budget of one batch
+    uint64_t p2_table_limit = 1ull << 36;      // z beyond this: P2 by pi-table windows
     // kernel timing (CUDA events around the hard-leaf sieve)
     bool timing = false;
     cudaEvent_t ev_hard0 = nullptr, ev_hard1 = nullptr;

@@ -292,7 +292,16 @@ void compute_needs(const BatchReq &rq, std::vector<QD> &qd, TableNeed &need, boo
         d.cx = cx;
         d.r4 = r4;
         d.tx = cpx_isqrt(z128);
-        if (mask & TERM_P2) N = std::max<uint64_t>(N, std::max(d.z, sx) + 1);
+        if (mask & TERM_P2) {
+            if (d.z + 1 > rq.p2_table_limit) {
+                // P2 by table windows over [sqrt x, z]: the resident table reaches sqrt x
+                d.p2win = 1;
+                N = std::max<uint64_t>(N, sx + 2);
+                Pneed = std::max<uint64_t>(Pneed, cpx_isqrt((u128)d.z) + 2);
+            } else {
+                N = std::max<uint64_t>(N, std::max(d.z, sx) + 1);
+            }
+        }
         if (mask & TERM_TRIV) N = std::max<uint64_t>(N, std::max(y, cx) + 1);
         if (mask & TERM_EASY) N = std::max<uint64_t>(N, std::max(sx, y) + 1);
         if (mask & (TERM_ORD | TERM_HARD)) Y = std::max(Y, y);
@@ -393,7 +402,13 @@ void run_batch(cpx_ctx *ctx, const BatchReq &rq)
     std::vector<QD> qd;
     TableNeed need;
     bool wide = false;
-    compute_needs(rq, qd, need, wide);
+    {
+        BatchReq r2 = rq;
+        r2.p2_table_limit = ctx->p2_table_limit;
+        compute_needs(r2, qd, need, wide);
+    }
+    bool any_p2win = false;
+    for (const QD &d : qd) any_p2win |= d.p2win != 0;
     st.roots_ms = ms_since(clk);
     // ---- tables
     if (ctx->tables_borrowed) {
@@ -429,7 +444,7 @@ void run_batch(cpx_ctx *ctx, const BatchReq &rq)
                 const u128 x = d.x;
                 const uint64_t pc = kSmallPrimes[c];
                 if (mask & TERM_ORD) n_ord = ((d.y + 1) / 2 + 3) / 4;
-                if ((mask & TERM_P2) && d.sx > d.y) n_p2 = ((d.sx - 1) >> 7) - (d.y >> 7) + 1;
+                if ((mask & TERM_P2) && d.sx > d.y && !d.p2win) n_p2 = ((d.sx - 1) >> 7) - (d.y >> 7) + 1;
                 if (mask & TERM_TRIV) n_triv = (d.cx > d.tx) ? ((d.cx - 1) >> 7) - (d.tx >> 7) + 1 : 1;
                 if ((mask & TERM_EASY) && d.cx > pc) n_easy = host_pi(hP, d.cx) - c;  // primes p_c < p <= icbrt(x)
                 if (mask & TERM_EASY) {
@@ -600,11 +615,17 @@ void run_batch(cpx_ctx *ctx, const BatchReq &rq)
             launch_easy_comp(ctx, pl);
         }
         if (mask & TERM_HARD) launch_hard(ctx, pl);
-        launch_finalize(ctx, pl, d_out, mask == TERM_PI);
+        if (!any_p2win) launch_finalize(ctx, pl, d_out, mask == TERM_PI);
     };
     if (ctx->timing) CPX_CUDA(cudaEventRecord(ctx->ev_b0, ctx->stream));
-    if (rq.graph) launch_as_graph(ctx, launch_all);
+    if (rq.graph && !any_p2win) launch_as_graph(ctx, launch_all);
     else launch_all();
+    if (any_p2win) {
+        // P2 of the queries beyond the resident table, window by window
+        for (uint32_t i = 0; i < Q; i++)
+            if (qd[i].p2win) p2_windowed(ctx, qd[i], d_acc + (size_t)i * kAccStride + 2 * ACC_P2, wide);
+        launch_finalize(ctx, pl, d_out, mask == TERM_PI);
+    }
     if (ctx->timing) CPX_CUDA(cudaEventRecord(ctx->ev_b1, ctx->stream));
 
     st.launch_ms = ms_since(clk);

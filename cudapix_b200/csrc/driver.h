@@ -23,6 +23,7 @@ struct BatchReq {
     uint32_t lbits = 0, threads = 0;        // hard-leaf tuning (0 = context default)
     unsigned terms = TERM_PI;
     uint64_t max_table_n = 1ull << 40;      // largest pi-table bound accepted
+    uint64_t p2_table_limit = 1ull << 36;   // z beyond this: P2 by table windows
     u128 *out_pi = nullptr;                 // n entries
     i128 *out_terms = nullptr;              // 7 per query: P2 ord triv easy hard pi_y pi
     uint64_t *out_y = nullptr;

@@ -116,6 +116,90 @@ __global__ void __launch_bounds__(kThreads) k_p2(const QD *__restrict__ qd, uint
     warp_flush(a, acc, ACC_P2);
 }
 
+// P2 for a query whose z lies beyond the resident pi table: the values
+// v = x/p in [A, B) of one table window.  One lane per table entry of p
+// candidates in (plo, phi] (p with x/p in the window); pi(v) = base + odd
+// primes of the window up to v, pi(p) from the resident table.
+template <class XT>
+__global__ void __launch_bounds__(kThreads) k_p2_window(XT x, uint64_t plo, uint64_t phi, uint64_t A,
+                                                        const cpx_pient *__restrict__ Tw, uint64_t base,
+                                                        const cpx_pient *__restrict__ T,
+                                                        unsigned long long *__restrict__ acc_q)
+{
+    const uint64_t w0 = plo >> 7, w1 = (phi - 1) >> 7;
+    const uint64_t w = w0 + (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    int64_t s = 0;
+    if (w <= w1) {
+        const ulonglong2 e = __ldg(reinterpret_cast<const ulonglong2 *>(T) + w);
+        uint64_t bits = e.x & range_mask(w, plo, phi);
+        while (bits) {
+            const int j = __ffsll((long long)bits) - 1;
+            bits &= bits - 1;
+            const uint64_t p = 128 * w + 2 * j + 1;
+            const uint64_t i = 1 + e.y + __popcll(e.x & ((2ull << j) - 1));  // pi(p)
+            const uint64_t v = (uint64_t)cpx_qdiv(x, p);
+            uint64_t piv = base;  // v = A (even): pi(A) = pi(A - 1)
+            if (v > A) {
+                // the entry holding v - 1, as in cpx_pi_from_entry (A is a multiple of 128)
+                const ulonglong2 ew = __ldg(reinterpret_cast<const ulonglong2 *>(Tw) + ((v - 1 - A) >> 7));
+                const uint32_t jv = (uint32_t)(((v - 1) & 127) >> 1);
+                piv += ew.y + __popcll(ew.x & ((2ull << jv) - 1));
+            }
+            s += (int64_t)piv - (int64_t)i + 1;
+        }
+    }
+    __shared__ i128 red[32];
+    const i128 b = cpx_block_sum_i128((i128)s, red);
+    if (threadIdx.x == 0 && b != 0) cpx_atomic_add_i128(acc_q, b);
+}
+
+__global__ void k_pi_at(const cpx_pient *__restrict__ T, uint64_t n, uint64_t *out) { *out = cpx_pi_dev(T, n); }
+
+constexpr uint64_t kP2WindowWords = 1ull << 27;  // at most 2^34 integers (2 GiB of window table) per window
+
+void p2_windowed(cpx_ctx *ctx, const QD &d, unsigned long long *acc_q, bool wide)
+{
+    const u128 x = d.x;
+    const uint64_t y = d.y, sx = d.sx;
+    if (sx <= y) return;
+    const uint64_t vmin = (uint64_t)(x / sx), vmax = (uint64_t)(x / (y + 1));
+    uint64_t A = (vmin >> 7) << 7;
+    // base = pi(A - 1) from the resident table (it reaches sqrt(x) + 1 >= A - 1)
+    uint64_t *d_b = ctx->b_small.as<uint64_t>(8) + 6;
+    k_pi_at<<<1, 1, 0, ctx->stream>>>(ctx->tab.T, A ? A - 1 : 0, d_b);
+    CPX_LAUNCH("k_pi_at");
+    note_launch(ctx);
+    uint64_t base = 0;
+    CPX_CUDA(cudaMemcpyAsync(&base, d_b, 8, cudaMemcpyDeviceToHost, ctx->stream));
+    CPX_CUDA(cudaStreamSynchronize(ctx->stream));
+    // windows of `p2_table_limit` integers (the resident-table bound), at most 2^34
+    const uint64_t ww = std::min<uint64_t>(kP2WindowWords,
+                                           std::max<uint64_t>(kTabSegWords, (ctx->p2_table_limit >> 7) / kTabSegWords *
+                                                                                kTabSegWords));
+    cpx_pient *Tw = ctx->b_win.as<cpx_pient>(ww + kTabSegWords);
+    while (A <= vmax) {
+        const uint64_t nwords = std::min<uint64_t>(ww, ((vmax - A) >> 7) + 1);
+        const uint64_t odd = build_pitable_window(ctx, A >> 7, nwords, Tw);
+        const uint64_t B = A + 128 * ((nwords + kTabSegWords - 1) / kTabSegWords * kTabSegWords);
+        // p in (max(y, x/B), min(sx, x/A)]
+        uint64_t plo = (uint64_t)(x / B), phi = A ? (uint64_t)std::min<u128>(x / A, (u128)sx) : sx;
+        if (plo < y) plo = y;
+        if (phi > plo) {
+            const uint64_t nent = ((phi - 1) >> 7) - (plo >> 7) + 1;
+            const unsigned grid = (unsigned)((nent + kThreads - 1) / kThreads);
+            if (wide)
+                k_p2_window<u128><<<grid, kThreads, 0, ctx->stream>>>(x, plo, phi, A, Tw, base, ctx->tab.T, acc_q);
+            else
+                k_p2_window<uint64_t><<<grid, kThreads, 0, ctx->stream>>>((uint64_t)x, plo, phi, A, Tw, base,
+                                                                           ctx->tab.T, acc_q);
+            CPX_LAUNCH("k_p2_window");
+            note_launch(ctx);
+        }
+        base += odd;
+        A = B;
+    }
+}
+
 // ------------------------------------------------------------------- trivial
 // S1 = C(pi(y) - pi(cbrt x), 2);  U = sum_{isqrt(x/y) < p <= cbrt x} [pi(y) - pi(x/p^2)]
 template <class XT>

@@ -12,6 +12,7 @@ struct __align__(16) QD {
     uint32_t c, nb;                 // nb = pi(r4)
     uint32_t lbits, direct;         // hard segment = 2^lbits odd numbers; direct = count by table
     uint64_t nseg;                  // hard-leaf segments over [0, z]
+    uint32_t p2win, pad;            // p2win: P2 by pi-table windows over [sqrt x, z] (z beyond the table)
 };
 
 // One level of composite easy leaves of one query: odd m = 2i + 1 with
@@ -25,7 +26,8 @@ struct __align__(16) EasyLvl {
 // A heavy (segment, level) leaf set handed from k_hard to k_hard_leaves: the
 // segment's bitmap and per-chunk survivor prefixes at level b-1 sit in
 // snapshot slot `job`; the leaves are m in (mlo, mhi] (prime m only when
-// kind = 1).  unit0/nunits number its work units after the job scan.
+// kind = 1).  nunits counts its k_hard_leaves work units; their offsets are
+// the scanned job-unit array.
 struct __align__(16) HardJob {
     uint32_t q, b, p, kind;
     uint64_t mlo, mhi, lo, slot;  // lo: first number of the warp's sub-segment
@@ -75,6 +77,9 @@ struct Plan {
 
 void launch_ordinary(cpx_ctx *ctx, const Plan &pl);
 void launch_p2(cpx_ctx *ctx, const Plan &pl);
+// P2 of one query by pi-table windows over v = x/p in [sqrt x, x/(y+1)];
+// adds into the query's accumulator acc (device).  Host loop, synchronous.
+void p2_windowed(cpx_ctx *ctx, const QD &d, unsigned long long *acc_q, bool wide);
 void launch_trivial(cpx_ctx *ctx, const Plan &pl);
 void launch_easy(cpx_ctx *ctx, const Plan &pl);
 void launch_easy_comp(cpx_ctx *ctx, const Plan &pl);

@@ -86,6 +86,10 @@ int cpx_set_hard_params(cpx_ctx *ctx, uint32_t log2_bits, uint32_t threads);
  * candidate m is answered by a separate GPU-wide leaf kernel from a snapshot
  * of the sub-segment; 0 answers every leaf inside the sieve (default 1024) */
 int cpx_set_hard_offload(cpx_ctx *ctx, uint32_t min_candidates);
+/* P2 needs pi(x/p) up to z = x/y.  For z above `limit` (default 2^36) the
+ * resident pi table stops at sqrt(x) and P2 is summed over pi-table windows
+ * of 2^34 integers built one after another (the 128-bit path to 1e20). */
+int cpx_set_p2_window(cpx_ctx *ctx, uint64_t limit);
 /* time of the last hard-leaf sieve (CUDA events on the context stream) and
  * its algorithmic byte count (one pass over the segment bitmap per active
  * prime per segment). */

@@ -153,3 +153,17 @@ def test_graph_batches_equal_direct_launches(ctx, cpx, golden):
         assert cpx.pi_batch(xs, ctx=ctx, graph=True) == cpx.pi_batch(xs, ctx=ctx), (n, hi)
     pw = [10**k for k in range(1, 16)]
     assert cpx.pi_batch(pw, ctx=ctx, graph=True) == [golden["pi_pow10"][str(k)] for k in range(1, 16)]
+
+
+@pytest.mark.parametrize("x,y", [(10**12, 10**5), (10**13, 172354), (2**40 + 15, 10**5 + 3)])
+def test_p2_by_table_windows(cpx, orc, x, y):
+    """P2 summed over pi-table windows (forced by a small resident-table bound:
+    many windows of 2^20 integers) equals the oracle, and so does pi(x)."""
+    own = cpx.Context(0)
+    own.set_p2_window(1 << 20)
+    t = cpx.pi_terms(x, y, 6, ctx=own)
+    o = orc.pi_dr(x, y, 6)
+    assert t["P2"] == o["P2"] and t["pi"] == o["pi"], (x, t["P2"], o["P2"])
+    xs = [10**11, 10**12 + 39, 3 * 10**12]
+    assert cpx.pi_batch(xs, ctx=own) == [orc.pi_dr(v, cpx.default_y(v), 6)["pi"] for v in xs]
+    own.close()
