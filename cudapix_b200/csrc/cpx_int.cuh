@@ -136,7 +136,14 @@ __device__ __forceinline__ uint64_t cpx_udiv_leaf(uint64_t n, uint64_t d)
     return u;
 }
 __device__ __forceinline__ uint64_t cpx_qdiv(uint64_t n, uint64_t d) { return cpx_udiv_leaf(n, d); }
-__device__ __forceinline__ u128 cpx_qdiv(u128 n, uint64_t d) { return n / (u128)d; }
+// 128-bit dividend: x/p is below 2^64 for x < 2^64 p, so most leaf
+// quotients of the 128-bit path take the 64-bit route as well
+static __device__ __noinline__ u128 cpx_udiv128_slow(u128 n, uint64_t d) { return n / (u128)d; }
+__device__ __forceinline__ u128 cpx_qdiv(u128 n, uint64_t d)
+{
+    if (!(n >> 64)) return (u128)cpx_udiv_leaf((uint64_t)n, d);
+    return cpx_udiv128_slow(n, d);
+}
 
 // ------------------------------------------------ 128-bit atomic accumulate
 // Two 64-bit atomics; the carry out of the low word is added to the high word

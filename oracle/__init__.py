@@ -50,7 +50,7 @@ def lib():
         L.orc_phi.argtypes = [U64, ctypes.c_uint32]
         L.orc_phisieve_counts.restype = None
         L.orc_phisieve_counts.argtypes = [ctypes.c_uint32, U64, ctypes.c_void_p]
-        for name in ("orc_P2", "orc_trivial"):
+        for name in ("orc_P2", "orc_P2_windowed", "orc_trivial"):
             getattr(L, name).restype = None
             getattr(L, name).argtypes = [U64, U64, U64, ctypes.c_void_p]
         for name in ("orc_ordinary", "orc_hard", "orc_easy"):
@@ -152,6 +152,12 @@ def phisieve_counts(a, nbits):
 
 def P2(x, y):
     return _call128(lib().orc_P2, *_split(x), y)
+
+
+def P2_windowed(x, y):
+    """P2 with pi(x/p) from windows of 2^31 integers (no table to z); used
+    for z beyond host memory and checked against P2 where both fit."""
+    return _call128(lib().orc_P2_windowed, *_split(x), y)
 
 
 def trivial(x, y):

@@ -491,6 +491,7 @@ static void dr_init(drctx_t *D, u128 x, uint64_t y, uint32_t c, uint64_t tabmax)
     D->cbrtx = icbrt128(x);
     D->qrtx = isqrt128(D->sqrtx);
     uint64_t pmax = D->y > D->sqrtx ? D->y : D->sqrtx;
+    if (pmax > 0xFFFFFF00ull) pmax = 0xFFFFFF00ull; /* uint32 list; larger p are sieved where needed */
     D->P = primes_upto(pmax + 64, &D->np);
     D->have_tab = tabmax > 0;
     if (D->have_tab) D->tab = pitab_build(tabmax);
@@ -733,6 +734,117 @@ static i128 term_hard(const drctx_t *D, const int8_t *mu, const uint32_t *lpf)
     return H;
 }
 
+/* P2 without a table to z: the values v = x/p in [sqrt x, x/(y+1)] are
+ * covered by consecutive windows [A, B) of 2^31 integers, each sieved into a
+ * window table (odd bitmap + prefix counts relative to A); pi(v) = pi(A - 1) +
+ * the window count, and pi(A - 1) runs from window to window.  The primes p
+ * with x/p in [A, B) form the range (x/B, x/A], sieved per window with the
+ * primes up to sqrt(sqrt x) (p can exceed 32 bits).  With a = pi(y) and
+ * b = pi(sqrt x) = a + the primes found, Sum_{y<p<=sqrt x} (1 - pi(p)) =
+ * (b - a) - (b(b+1) - a(a+1))/2.  Same sum as term_P2 (src/P2.cu:76-133);
+ * only the tables are windowed. */
+static i128 term_P2_windowed(const drctx_t *D)
+{
+    if (D->y >= D->sqrtx) return 0;
+    const u128 x = D->x;
+    const uint64_t y = D->y, sx = D->sqrtx;
+    const uint64_t vmin = (uint64_t)(x / sx), vmax = (uint64_t)(x / (y + 1));
+    const uint64_t chunk_words = 1 << 14, win_words = 1ull << 24; /* 2^31 integers per window */
+    uint64_t A = (vmin >> 7) << 7;
+    /* pi(A - 1) and pi(y): a table to max(A, y) + 2 (A <= sqrt x + 2) */
+    pitab_t small = pitab_build((A > y ? A : y) + 2);
+    uint64_t base = pitab_pi(&small, A - 1);
+    const uint64_t a = pitab_pi(&small, y);
+    pitab_free(&small);
+    uint64_t nsp;
+    uint32_t *SP = primes_upto(isqrt128((u128)vmax + (u128)128 * win_words) + 2, &nsp);
+    uint64_t *bits = (uint64_t *)malloc(win_words * 8), *pre = (uint64_t *)malloc(win_words * 8);
+    uint64_t nchunks = win_words / chunk_words;
+    uint64_t *ctot = (uint64_t *)malloc(nchunks * 8);
+    const uint64_t pchunk_bits = 1 << 20; /* p-range sieve chunk: 2^21 integers */
+    uint64_t *pbits_all = (uint64_t *)malloc((size_t)omp_get_max_threads() * (pchunk_bits / 64) * 8);
+    i128 s = 0;
+    uint64_t nprimes = 0;
+    while (A <= vmax) {
+        const uint64_t B = A + 128 * win_words;
+#pragma omp parallel for schedule(dynamic, 4)
+        for (uint64_t c = 0; c < nchunks; c++) {
+            uint64_t *bb = bits + c * chunk_words;
+            sieve_odd_segment(A + c * chunk_words * 128, chunk_words * 64, SP + 1, nsp - 1, bb);
+            uint64_t t = 0;
+            for (uint64_t w = 0; w < chunk_words; w++) t += __builtin_popcountll(bb[w]);
+            ctot[c] = t;
+        }
+        uint64_t run = 0;
+        for (uint64_t c = 0; c < nchunks; c++) {
+            uint64_t v = ctot[c];
+            ctot[c] = run;
+            run += v;
+        }
+#pragma omp parallel for schedule(static)
+        for (uint64_t c = 0; c < nchunks; c++) {
+            uint64_t t = ctot[c];
+            for (uint64_t w = c * chunk_words; w < (c + 1) * chunk_words; w++) {
+                pre[w] = t;
+                t += __builtin_popcountll(bits[w]);
+            }
+        }
+        /* primes p in (max(y, x/B), min(sx, x/A)], sieved in chunks of 2^21 integers */
+        uint64_t plo = (uint64_t)(x / B), phi = (uint64_t)(x / A);
+        if (plo < y) plo = y;
+        if (phi > sx) phi = sx;
+        if (phi > plo) {
+            const uint64_t lo0 = plo & ~1ull; /* chunks of odd n = lo + 2i + 1 */
+            const uint64_t npc = (phi - lo0 + 2 * pchunk_bits - 1) / (2 * pchunk_bits);
+            i128 ws = 0;
+            uint64_t wn = 0;
+#pragma omp parallel reduction(+ : wn)
+            {
+                uint64_t *pb = pbits_all + (size_t)omp_get_thread_num() * (pchunk_bits / 64);
+                i128 ls = 0;
+#pragma omp for schedule(dynamic, 1)
+                for (uint64_t k = 0; k < npc; k++) {
+                    const uint64_t lo = lo0 + 2 * pchunk_bits * k;
+                    sieve_odd_segment(lo, pchunk_bits, SP + 1, nsp - 1, pb);
+                    for (uint64_t w = 0; w < pchunk_bits / 64; w++) {
+                        uint64_t m = pb[w];
+                        while (m) {
+                            const int j = __builtin_ctzll(m);
+                            m &= m - 1;
+                            const uint64_t p = lo + 2 * (64 * w + j) + 1;
+                            if (p <= plo || p > phi) continue;
+                            const uint64_t v = (uint64_t)(x / p);
+                            uint64_t piv = base;
+                            if (v > A) {
+                                const uint64_t wv = (v - 1 - A) >> 7;
+                                const uint32_t jv = (uint32_t)(((v - 1) & 127) >> 1);
+                                const uint64_t mask = (jv == 63) ? ~0ull : ((2ull << jv) - 1);
+                                piv += pre[wv] + (uint64_t)__builtin_popcountll(bits[wv] & mask);
+                            }
+                            ls += (i128)piv;
+                            wn++;
+                        }
+                    }
+                }
+#pragma omp critical
+                ws += ls;
+            }
+            s += ws;
+            nprimes += wn;
+        }
+        base += run;
+        A = B;
+    }
+    const i128 bb = (i128)a + (i128)nprimes, aa = (i128)a;
+    s += (bb - aa) - (bb * (bb + 1) - aa * (aa + 1)) / 2;
+    free(bits);
+    free(pre);
+    free(ctot);
+    free(pbits_all);
+    free(SP);
+    return s;
+}
+
 static uint64_t tabmax_for(u128 x, uint64_t y)
 {
     uint64_t z = (uint64_t)(x / y), sx = isqrt128(x);
@@ -745,8 +857,25 @@ void orc_P2(uint64_t x_lo, uint64_t x_hi, uint64_t y, uint64_t *out)
 {
     u128 x = mk128(x_lo, x_hi);
     drctx_t D;
-    dr_init(&D, x, y, 6, tabmax_for(x, y));
-    put128(term_P2(&D), out);
+    const uint64_t tm = tabmax_for(x, y);
+    if (tm > (1ull << 33) || isqrt128(x) > 0xFFFFFF00ull) {
+        /* table to z would not fit: windows over [sqrt x, z] */
+        dr_init(&D, x, y, 6, 0);
+        put128(term_P2_windowed(&D), out);
+    } else {
+        dr_init(&D, x, y, 6, tm);
+        put128(term_P2(&D), out);
+    }
+    dr_free(&D);
+}
+
+/* P2 by windows at any size (tests the windowing against term_P2) */
+void orc_P2_windowed(uint64_t x_lo, uint64_t x_hi, uint64_t y, uint64_t *out)
+{
+    u128 x = mk128(x_lo, x_hi);
+    drctx_t D;
+    dr_init(&D, x, y, 6, 0);
+    put128(term_P2_windowed(&D), out);
     dr_free(&D);
 }
 
