@@ -295,11 +295,13 @@ def run_single(args, world, rank, local):
         return
     ms = statistics.median(lat)
     hm, hb = hard[-1]
+    leaves = cpx.leaf_counts(x, t["y"], 6, ctx=ctx)
     print(json.dumps({"metric": "pi(x) single-query latency", "value": ms, "unit": "ms", "n_gpus": world,
                       "steps": args.steps, "warmup": args.warmup, "higher_is_better": False,
                       "config": {"workload": f"single x={x} y={t['y']} z={t['z']} c=6", "alpha": args.alpha},
                       "pi": t["pi"], "terms": {k: t[k] for k in ("P2", "ordinary", "trivial", "easy", "hard")},
                       "hard_ms": hm, "s2_gbs": (hb / (hm / 1000)) / 1e9 if hm else None,
+                      "leaves": leaves, "hard_leaves_per_s": leaves["hard"] / (hm / 1000) if hm else None,
                       "batch_device_ms": ctx.last_batch_ms(), "clocks": clk.summary()}), flush=True)
 
 

@@ -22,7 +22,8 @@ Python int; 64- and 128-bit overloads are chosen by the size of x.
 """
 import ctypes
 
-from ._lib import (BatchStats, CpxError, ExtensionMissing, Params, ServeConfig, ServeCounters, Terms, U128,  # noqa: F401
+from ._lib import (BatchStats, CpxError, ExtensionMissing, LeafCounts, Params, ServeConfig, ServeCounters, Terms,  # noqa: F401
+                   U128,
                    header_symbols, load)
 
 __all__ = [
@@ -252,6 +253,15 @@ def pi_terms(x, y=0, c=6, ctx=None):
         o = ctypes.c_uint64()
         ctx.call("cpx_pi_u64", x, y, c, ctypes.byref(o), ctypes.byref(t))
     return t.as_dict()
+
+
+def leaf_counts(x, y=0, c=6, ctx=None):
+    """Exact special-leaf counts of pi(x) by class: hard, easy_composite,
+    easy_prime, trivial (src/leafcount.cpp:12-202 estimates them)."""
+    ctx = ctx or context()
+    o = LeafCounts()
+    ctx.call("cpx_leaf_count", U128.of(x), y, c, ctypes.byref(o))
+    return {k: getattr(o, k) for k, _ in o._fields_}
 
 
 def pi_deleglise_rivat(x, y=0, c=6, ctx=None):

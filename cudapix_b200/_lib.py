@@ -83,6 +83,11 @@ class BatchStats(ctypes.Structure):
         return {k: getattr(self, k) for k, _ in self._fields_}
 
 
+class LeafCounts(ctypes.Structure):
+    _fields_ = [("hard", ctypes.c_uint64), ("easy_composite", ctypes.c_uint64),
+                ("easy_prime", ctypes.c_uint64), ("trivial", ctypes.c_uint64)]
+
+
 class Params(ctypes.Structure):
     _fields_ = [
         ("alpha_num", ctypes.c_uint32),
@@ -141,6 +146,7 @@ _SIGS = {
     "cpx_set_hard_params": (ctypes.c_int, [P, u32, u32]),
     "cpx_set_hard_offload": (ctypes.c_int, [P, u32]),
     "cpx_set_p2_window": (ctypes.c_int, [P, u64]),
+    "cpx_leaf_count": (ctypes.c_int, [P, U128, u64, u16, ctypes.POINTER(LeafCounts)]),
     "cpx_last_hard_stats": (ctypes.c_int, [P, ctypes.POINTER(ctypes.c_float), ctypes.POINTER(ctypes.c_double)]),
     "cpx_set_timing": (ctypes.c_int, [P, ctypes.c_int]),
     "cpx_last_batch_ms": (ctypes.c_int, [P, ctypes.POINTER(ctypes.c_float)]),

@@ -192,6 +192,21 @@ int cpx_set_hard_offload(cpx_ctx *ctx, uint32_t min_candidates)
     return guarded(ctx, [&] { ctx->hard_offload_min = min_candidates; });
 }
 
+int cpx_leaf_count(cpx_ctx *ctx, cpx_u128 x, uint64_t y, uint16_t c, cpx_leaf_counts *out)
+{
+    return guarded(ctx, [&] {
+        if (!out) fail(CPX_EINVAL, "null output");
+        const u128 xv = U(x);
+        uint64_t yy = y ? y : default_y(xv, 0, 0);
+        uint64_t v[4];
+        leaf_counts(ctx, xv, yy, c ? c : 6, v);
+        out->hard = v[0];
+        out->easy_composite = v[1];
+        out->easy_prime = v[2];
+        out->trivial = v[3];
+    });
+}
+
 int cpx_set_p2_window(cpx_ctx *ctx, uint64_t limit)
 {
     return guarded(ctx, [&] {

@@ -51,7 +51,7 @@ uint64_t default_y(u128 x, uint32_t num, uint32_t den)
     return y;
 }
 
-static const std::vector<uint32_t> &host_primes(cpx_ctx *ctx)
+const std::vector<uint32_t> &host_primes(cpx_ctx *ctx)
 {
     Tables &tb = ctx->tab;
     if (ctx->hP_version != tb.prm_max) {
@@ -62,7 +62,7 @@ static const std::vector<uint32_t> &host_primes(cpx_ctx *ctx)
     return ctx->hP;
 }
 
-static uint64_t host_pi(const std::vector<uint32_t> &P, uint64_t v)
+uint64_t host_pi(const std::vector<uint32_t> &P, uint64_t v)
 {
     return (uint64_t)(std::upper_bound(P.begin(), P.end(), (uint64_t)v,
                                        [](uint64_t a, uint32_t b) { return a < b; }) -

@@ -41,6 +41,11 @@ void run_batch(cpx_ctx *ctx, const BatchReq &rq);
 void compute_needs(const BatchReq &rq, std::vector<QD> &qd, TableNeed &need, bool &wide);
 bool tables_cover(const cpx_ctx *ctx, const TableNeed &need);
 void grow_tables(cpx_ctx *ctx, const TableNeed &need);
+// host mirror of the resident prime list, and pi(v) by binary search in it
+const std::vector<uint32_t> &host_primes(cpx_ctx *ctx);
+uint64_t host_pi(const std::vector<uint32_t> &P, uint64_t v);
+// exact special-leaf counts of one query: hard, easy (composite m), easy (prime m), trivial
+void leaf_counts(cpx_ctx *ctx, u128 x, uint64_t y, uint32_t c, uint64_t out[4]);
 uint64_t default_y(u128 x, uint32_t num, uint32_t den);
 uint32_t alpha_milli(u128 x);
 bool dr_domain_ok(u128 x, uint64_t y, uint32_t c);

@@ -233,6 +233,15 @@ typedef struct {
 int cpx_pi_batch(cpx_ctx *ctx, const cpx_u128 *xs, size_t n, const cpx_params *params,
                  cpx_u128 *out);
 
+/* Exact special-leaf counts of pi(x) with y (0: the y rule), in this
+ * library's split, u = x/(p_b m): trivial u < p_b; easy p_b <= u < p_b^2
+ * (prime m, composite m); hard u >= p_b^2.  Replaces the leaf-count
+ * estimates of src/leafcount.cpp:12-202. */
+typedef struct {
+    uint64_t hard, easy_composite, easy_prime, trivial;
+} cpx_leaf_counts;
+int cpx_leaf_count(cpx_ctx *ctx, cpx_u128 x, uint64_t y, uint16_t c, cpx_leaf_counts *out);
+
 /* ---- serving: continuous batching over resident tables -------------------
  * A server owns `lanes` worker threads, each with its own CUDA stream, batch
  * buffers and graph; all lanes share the tables of the context the server is

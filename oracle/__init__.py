@@ -56,6 +56,8 @@ def lib():
         for name in ("orc_ordinary", "orc_hard", "orc_easy"):
             getattr(L, name).restype = None
             getattr(L, name).argtypes = [U64, U64, U64, ctypes.c_uint32, ctypes.c_void_p]
+        L.orc_leaf_counts.restype = None
+        L.orc_leaf_counts.argtypes = [U64, U64, U64, ctypes.c_uint32, ctypes.c_void_p]
         L.orc_pi_dr.restype = None
         L.orc_pi_dr.argtypes = [U64, U64, U64, ctypes.c_uint32, ctypes.c_int, ctypes.c_void_p]
         _lib = L
@@ -194,3 +196,10 @@ def default_y(x, alpha_num=1, alpha_den=1):
     y = cb * alpha_num // alpha_den
     lo, hi = cb, isqrt(x)
     return max(lo, min(y, hi - 1 if hi > lo else hi))
+
+
+def leaf_counts(x, y, c=6):
+    """Special-leaf counts by class (hard, easy_composite, easy_prime, trivial), brute force."""
+    out = (ctypes.c_uint64 * 4)()
+    lib().orc_leaf_counts(*_split(x), y, c, out)
+    return dict(zip(("hard", "easy_composite", "easy_prime", "trivial"), (int(v) for v in out)))

@@ -1005,3 +1005,44 @@ uint64_t orc_pi_lehmer(uint64_t x)
     free(P);
     return (uint64_t)s;
 }
+
+/* Special-leaf counts by class (tests only): every leaf (b, m), c < b <= pi(y),
+ * y/p_b < m <= y, mu(m) != 0, lpf(m) > p_b, with u = x/(p_b m): out[0] hard
+ * (u >= p_b^2), out[1] easy with composite m, out[2] easy with prime m
+ * (p_b <= u < p_b^2), out[3] trivial (u < p_b).  Brute force over all
+ * leaves; the library's classes of src/leafcount.cpp:12-202's role. */
+void orc_leaf_counts(uint64_t x_lo, uint64_t x_hi, uint64_t y, uint32_t c, uint64_t *out)
+{
+    const u128 x = mk128(x_lo, x_hi);
+    const uint64_t len = y / 2 + 1;
+    int8_t *mu = (int8_t *)malloc(len + 1);
+    uint32_t *lpf = (uint32_t *)malloc((len + 1) * 4);
+    orc_mu_lpf(0, 2 * len, mu, lpf);
+    uint64_t np;
+    uint32_t *P = primes_upto(y, &np);
+    uint64_t h = 0, ec = 0, ep = 0, tv = 0;
+#pragma omp parallel for schedule(dynamic, 1) reduction(+ : h, ec, ep, tv)
+    for (uint64_t b = c + 1; b <= np; b++) {
+        const uint64_t p = P[b - 1];
+        for (uint64_t m = y / p + 1; m <= y; m++) {
+            if (!(m & 1)) continue;
+            const uint64_t i = (m - 1) / 2;
+            if (mu[i] == 0 || lpf[i] <= p) continue;
+            const u128 u = x / ((u128)p * m);
+            if (u < p) tv++;
+            else if (u < (u128)p * p) {
+                if (lpf[i] < m) ec++;
+                else ep++;
+            } else {
+                h++;
+            }
+        }
+    }
+    out[0] = h;
+    out[1] = ec;
+    out[2] = ep;
+    out[3] = tv;
+    free(mu);
+    free(lpf);
+    free(P);
+}

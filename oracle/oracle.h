@@ -52,6 +52,7 @@ void orc_phisieve_counts(uint32_t a, uint64_t nbits, uint32_t *out);
 /* Terms.  x = (x_hi:x_lo).  out[0..1] = signed 128-bit result (lo, hi). */
 void orc_P2(uint64_t x_lo, uint64_t x_hi, uint64_t y, uint64_t *out);
 void orc_P2_windowed(uint64_t x_lo, uint64_t x_hi, uint64_t y, uint64_t *out);
+void orc_leaf_counts(uint64_t x_lo, uint64_t x_hi, uint64_t y, uint32_t c, uint64_t *out);
 void orc_trivial(uint64_t x_lo, uint64_t x_hi, uint64_t y, uint64_t *out);
 void orc_ordinary(uint64_t x_lo, uint64_t x_hi, uint64_t y, uint32_t c, uint64_t *out);
 void orc_easy(uint64_t x_lo, uint64_t x_hi, uint64_t y, uint32_t c, uint64_t *out);

@@ -167,3 +167,11 @@ def test_p2_by_table_windows(cpx, orc, x, y):
     xs = [10**11, 10**12 + 39, 3 * 10**12]
     assert cpx.pi_batch(xs, ctx=own) == [orc.pi_dr(v, cpx.default_y(v), 6)["pi"] for v in xs]
     own.close()
+
+
+@pytest.mark.parametrize("x,y,c", [(10**9, 10**4, 6), (10**10, 30000, 6), (10**12, 10**5, 6),
+                                   (2**40 + 15, 10**5 + 3, 6), (10**11, 50000, 3)])
+def test_leaf_counts(ctx, cpx, orc, x, y, c):
+    """Exact leaf counts by class against the oracle's brute force; the four
+    classes partition the special leaves."""
+    assert cpx.leaf_counts(x, y, c, ctx=ctx) == orc.leaf_counts(x, y, c)
