@@ -96,6 +96,18 @@ class Clocks:
                 "reasons": reasons, "samples": len(rows)}
 
 
+TUNING = os.path.join(ROOT, "cudapix_b200", "tuning", "b200.json")
+
+
+def tuned_context(cpx, device):
+    """A context with the committed B200 tuning table (cpx_autotune output),
+    when present; results are the same with or without it."""
+    ctx = cpx.Context(device)
+    if os.path.exists(TUNING):
+        ctx.tune_load(TUNING)
+    return ctx
+
+
 def peaks():
     try:
         with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
@@ -181,7 +193,7 @@ def serve_sweep(cpx, ctx, args):
     plain = {"qps": len(lat) / (sum(lat) / 1000.0), "p50_ms": lat[len(lat) // 2], "p99_ms": lat[-1],
              "queries": len(lat)}
     rows = []
-    own = cpx.Context(ctx.device)
+    own = tuned_context(cpx, ctx.device)
     with cpx.Server(own, lanes=args.serve_lanes, reserve_x=10**17) as srv:
         for lam in (10.0, 100.0, 1000.0, 10000.0):
             n = int(min(len(pool), max(30, 3 * lam)))
@@ -273,7 +285,7 @@ def run_single(args, world, rank, local):
     latency per query through the plain API, term by term timing of the hard leaves."""
     import cudapix_b200 as cpx
 
-    ctx = cpx.Context(local)
+    ctx = tuned_context(cpx, local)
     ctx.set_timing(True)
     x = int(float(args.single)) if "e" in args.single.lower() else int(args.single)
     y = cpx.default_y(x, args.alpha) if args.alpha else 0
@@ -332,7 +344,7 @@ def main():
 
     import cudapix_b200 as cpx
 
-    ctx = cpx.Context(local)
+    ctx = tuned_context(cpx, local)
     ctx.set_timing(True)
     xs = workload(args.queries, seed=0)
     ref = None
@@ -424,6 +436,7 @@ def main():
         "config": {"workload": "batch4096: x = floor(10^e), e ~ U[9,14], numpy default_rng(0)",
                    "queries": args.queries, "c": 6, "alpha": "reference alpha(x)",
                    "l2": "flushed before every timed step (256 MiB write)",
+                   "tuning": os.path.relpath(TUNING, ROOT) if os.path.exists(TUNING) else None,
                    "parallelism": f"replicas x{world}"},
         "e2e": {"value": nq / t_e2e, "unit": UNIT, "h2d_bytes_per_step": io[0], "d2h_bytes_per_step": io[1]},
         "gpu_launches": int(launches),

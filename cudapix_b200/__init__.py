@@ -21,8 +21,9 @@ Errors raise CpxError (the reference checked none).  Every value is an exact
 Python int; 64- and 128-bit overloads are chosen by the size of x.
 """
 import ctypes
+import os
 
-from ._lib import (BatchStats, CpxError, ExtensionMissing, LeafCounts, Params, ServeConfig, ServeCounters, Terms,  # noqa: F401
+from ._lib import (BatchStats, CpxError, ExtensionMissing, LeafCounts, Params, ServeConfig, ServeCounters, Terms, TuneEntry,  # noqa: F401
                    U128,
                    header_symbols, load)
 
@@ -110,6 +111,29 @@ class Context:
 
     def set_hard_offload(self, min_candidates):
         self.call("cpx_set_hard_offload", min_candidates)
+
+    def autotune(self, decade_lo=9, decade_hi=17, seconds=0.0):
+        """Tunes the plain path per decade of x (lone queries at 10^e and 10^(e+1/2))."""
+        self.call("cpx_autotune", decade_lo, decade_hi, float(seconds))
+
+    def autotune_batch(self, xs):
+        """Tunes the entry used by batches of more than four queries on this sample batch."""
+        self.call("cpx_autotune_batch", _u128_array(xs), len(xs))
+
+    def tune_save(self, path):
+        self.call("cpx_tune_save", os.fsencode(path))
+
+    def tune_load(self, path):
+        self.call("cpx_tune_load", os.fsencode(path))
+
+    def tune_get(self, decade):
+        """Entry of a decade of x (99: the batch entry); threads = 0 means untuned."""
+        t = TuneEntry()
+        self.call("cpx_tune_get", decade, ctypes.byref(t))
+        return {k: getattr(t, k) for k, _ in t._fields_}
+
+    def tune_clear(self):
+        self.call("cpx_tune_clear")
 
     def set_p2_window(self, limit):
         """z above `limit`: P2 over pi-table windows (resident table to sqrt x)."""

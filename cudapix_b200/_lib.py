@@ -88,6 +88,11 @@ class LeafCounts(ctypes.Structure):
                 ("easy_prime", ctypes.c_uint64), ("trivial", ctypes.c_uint64)]
 
 
+class TuneEntry(ctypes.Structure):
+    _fields_ = [("decade", ctypes.c_uint32), ("alpha_scale_milli", ctypes.c_uint32), ("log2_bits", ctypes.c_uint32),
+                ("threads", ctypes.c_uint32), ("offload_min", ctypes.c_uint32), ("ms", ctypes.c_float)]
+
+
 class Params(ctypes.Structure):
     _fields_ = [
         ("alpha_num", ctypes.c_uint32),
@@ -146,6 +151,12 @@ _SIGS = {
     "cpx_set_hard_params": (ctypes.c_int, [P, u32, u32]),
     "cpx_set_hard_offload": (ctypes.c_int, [P, u32]),
     "cpx_set_p2_window": (ctypes.c_int, [P, u64]),
+    "cpx_autotune": (ctypes.c_int, [P, u32, u32, ctypes.c_double]),
+    "cpx_autotune_batch": (ctypes.c_int, [P, pU, ctypes.c_size_t]),
+    "cpx_tune_save": (ctypes.c_int, [P, ctypes.c_char_p]),
+    "cpx_tune_load": (ctypes.c_int, [P, ctypes.c_char_p]),
+    "cpx_tune_get": (ctypes.c_int, [P, u32, ctypes.POINTER(TuneEntry)]),
+    "cpx_tune_clear": (ctypes.c_int, [P]),
     "cpx_leaf_count": (ctypes.c_int, [P, U128, u64, u16, ctypes.POINTER(LeafCounts)]),
     "cpx_last_hard_stats": (ctypes.c_int, [P, ctypes.POINTER(ctypes.c_float), ctypes.POINTER(ctypes.c_double)]),
     "cpx_set_timing": (ctypes.c_int, [P, ctypes.c_int]),

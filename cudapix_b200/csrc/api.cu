@@ -207,6 +207,58 @@ int cpx_leaf_count(cpx_ctx *ctx, cpx_u128 x, uint64_t y, uint16_t c, cpx_leaf_co
     });
 }
 
+int cpx_autotune(cpx_ctx *ctx, uint32_t decade_lo, uint32_t decade_hi, double seconds)
+{
+    return guarded(ctx, [&] { autotune(ctx, decade_lo, decade_hi, seconds > 0 ? seconds : 1e30); });
+}
+
+int cpx_autotune_batch(cpx_ctx *ctx, const cpx_u128 *xs, size_t n)
+{
+    return guarded(ctx, [&] {
+        if (!xs) fail(CPX_EINVAL, "null buffer");
+        std::vector<u128> xv(n);
+        for (size_t i = 0; i < n; i++) xv[i] = U(xs[i]);
+        autotune_batch(ctx, xv.data(), n);
+    });
+}
+
+int cpx_tune_save(cpx_ctx *ctx, const char *path)
+{
+    return guarded(ctx, [&] {
+        if (!path) fail(CPX_EINVAL, "null path");
+        tune_save(ctx, path);
+    });
+}
+
+int cpx_tune_load(cpx_ctx *ctx, const char *path)
+{
+    return guarded(ctx, [&] {
+        if (!path) fail(CPX_EINVAL, "null path");
+        tune_load(ctx, path);
+    });
+}
+
+int cpx_tune_get(cpx_ctx *ctx, uint32_t decade, cpx_tune_entry *out)
+{
+    return guarded(ctx, [&] {
+        if (!out || (decade >= kTuneDecades && decade != kBatchEntry)) fail(CPX_EINVAL, "bad decade or null output");
+        const bool b = decade == kBatchEntry;
+        const TuneEntry &t = b ? ctx->batch_tune : ctx->tune[decade];
+        const bool on = b ? ctx->batch_tuned : ctx->tuned;
+        *out = cpx_tune_entry{decade, t.alpha_milli, t.lbits, on ? t.threads : 0, t.offload, t.ms};
+    });
+}
+
+int cpx_tune_clear(cpx_ctx *ctx)
+{
+    return guarded(ctx, [&] {
+        for (TuneEntry &t : ctx->tune) t = TuneEntry{};
+        ctx->tuned = false;
+        ctx->batch_tune = TuneEntry{};
+        ctx->batch_tuned = false;
+    });
+}
+
 int cpx_set_p2_window(cpx_ctx *ctx, uint64_t limit)
 {
     return guarded(ctx, [&] {

@@ -64,6 +64,15 @@ struct Tables {
     uint64_t version = 0;
 };
 
+// tuned settings (0 = the context default): alpha_milli is the alpha scale
+// in per mille of the reference alpha(x); lbits caps the segment bits
+struct TuneEntry {
+    uint32_t alpha_milli, lbits, threads, offload;
+    float ms;  // sample time when tuned
+};
+constexpr uint32_t kTuneDecades = 40;
+constexpr uint32_t kBatchEntry = 99;  // decade number of the batch entry in the JSON file
+
 struct Timer {
     cudaEvent_t a = nullptr, b = nullptr;
 };
@@ -101,6 +110,10 @@ struct cpx_ctx {
     uint32_t hard_offload_min = 1024;  // candidates of a (sub-segment, level) sent to k_hard_leaves
     uint64_t hard_offload_bytes = 4ull << 30;  // snapshot pool budget of one batch
     uint64_t p2_table_limit = 1ull << 36;      // z beyond this: P2 by pi-table windows
+    cpx::TuneEntry tune[cpx::kTuneDecades] = {};  // per decade (batches of up to 4 queries)
+    bool tuned = false;
+    cpx::TuneEntry batch_tune = {};               // larger batches
+    bool batch_tuned = false;
     // kernel timing (CUDA events around the hard-leaf sieve)
     bool timing = false;
     cudaEvent_t ev_hard0 = nullptr, ev_hard1 = nullptr;

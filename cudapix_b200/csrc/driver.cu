@@ -173,7 +173,8 @@ static uint64_t heavy_leaf_sets(const QD &d, const std::vector<uint32_t> &hP, ui
 // largest queries shrink (one cap for all) until the whole batch has about
 // four segments per SM, so one large query still fills the GPU while a big
 // batch keeps long segments (fewer segment-levels to sieve).
-static void choose_lbits(cpx_ctx *ctx, std::vector<QD> &qd, uint32_t c, uint32_t threads, uint32_t forced)
+static void choose_lbits(cpx_ctx *ctx, std::vector<QD> &qd, uint32_t c, uint32_t threads, uint32_t forced,
+                         uint32_t cap_all, const TuneEntry *tune)
 {
     const uint32_t minb = (threads >= 512) ? 16 : (threads >= 256 ? 15 : 14);
     std::vector<uint32_t> nat(qd.size(), 0);
@@ -184,11 +185,13 @@ static void choose_lbits(cpx_ctx *ctx, std::vector<QD> &qd, uint32_t c, uint32_t
             nat[i] = std::max(minb, std::min<uint32_t>(forced, 20));
             continue;
         }
+        uint32_t qcap = cap_all ? cap_all : ctx->hard_log2_bits;
+        if (!cap_all && tune && tune[decade_of(d.x)].lbits) qcap = tune[decade_of(d.x)].lbits;
         uint32_t lb = minb;
-        while (lb < ctx->hard_log2_bits && (2ull << lb) < d.z + 1) lb++;
+        while (lb < qcap && (2ull << lb) < d.z + 1) lb++;
         nat[i] = lb;
     }
-    uint32_t cap = forced ? 20 : ctx->hard_log2_bits;
+    uint32_t cap = 20;  // the per-query caps are in nat[]; this batch-wide cap only shrinks them
     const uint64_t target = (uint64_t)ctx->sm_count * 4;
     for (;;) {
         uint64_t segs = 0;
@@ -270,7 +273,16 @@ void compute_needs(const BatchReq &rq, std::vector<QD> &qd, TableNeed &need, boo
         const uint64_t sx = cpx_isqrt(x), cx = cpx_icbrt(x), r4 = cpx_iroot4(x);
         uint64_t y = rq.ys ? rq.ys[i] : 0;
         if (mask == TERM_PI) {
-            if (!y) y = default_y(x, rq.alpha_num, rq.alpha_den);
+            if (!y) {
+                uint32_t sc = rq.alpha_scale;
+                if (!sc && rq.tune) sc = rq.tune[decade_of(x)].alpha_milli;
+                if (!rq.alpha_num && sc) {
+                    const uint64_t am = std::max<uint64_t>(1000, (uint64_t)alpha_milli(x) * sc / 1000);
+                    y = default_y(x, (uint32_t)std::min<uint64_t>(am, 0xFFFFFFFFull), 1000);
+                } else {
+                    y = default_y(x, rq.alpha_num, rq.alpha_den);
+                }
+            }
             if (!dr_domain_ok(x, y, c)) {
                 if (x >= ((u128)1 << 32)) fail(CPX_EINVAL, "y outside the Deleglise-Rivat domain for this x");
                 d.direct = 1;
@@ -394,9 +406,12 @@ void run_batch(cpx_ctx *ctx, const BatchReq &rq)
     auto clk = std::chrono::steady_clock::now();
     const uint32_t c = rq.c;
     if (c < 1 || c > 8) fail(CPX_EINVAL, "c must be in 1..8");
-    const uint32_t threads = rq.threads ? rq.threads : ctx->hard_threads;
-    if (threads != 128 && threads != 256 && threads != 512) fail(CPX_EINVAL, "hard threads must be 128/256/512");
     const unsigned mask = rq.terms;
+    // tuned settings: per decade for the plain path (up to 4 queries), the
+    // batch entry above that; a request's own settings win
+    const bool small = Q <= 4;
+    const TuneEntry *tune = (small && ctx->tuned) ? ctx->tune : nullptr;
+    const TuneEntry *btune = (!small && ctx->batch_tuned) ? &ctx->batch_tune : nullptr;
 
     // ---- host planning: roots, y, validity, table bounds
     std::vector<QD> qd;
@@ -405,8 +420,29 @@ void run_batch(cpx_ctx *ctx, const BatchReq &rq)
     {
         BatchReq r2 = rq;
         r2.p2_table_limit = ctx->p2_table_limit;
+        r2.tune = tune;
+        if (btune && !r2.alpha_scale) r2.alpha_scale = btune->alpha_milli;
         compute_needs(r2, qd, need, wide);
     }
+    // threads per segment, offload threshold and segment-bit cap: the tuned
+    // values (of the largest query's decade for the plain path) unless the
+    // request fixes them
+    uint32_t threads = rq.threads ? rq.threads : ctx->hard_threads;
+    uint64_t offload0 = ctx->hard_offload_min;
+    uint32_t lbits_cap = rq.lbits_cap;
+    if (tune) {
+        u128 xmax = 0;
+        for (const QD &d : qd)
+            if (!d.direct && d.x > xmax) xmax = d.x;
+        const TuneEntry &t = tune[decade_of(xmax)];
+        if (!rq.threads && t.threads) threads = t.threads;
+        if (t.offload) offload0 = t.offload;
+    } else if (btune) {
+        if (!rq.threads && btune->threads) threads = btune->threads;
+        if (btune->offload) offload0 = btune->offload;
+        if (!lbits_cap) lbits_cap = btune->lbits;
+    }
+    if (threads != 128 && threads != 256 && threads != 512) fail(CPX_EINVAL, "hard threads must be 128/256/512");
     bool any_p2win = false;
     for (const QD &d : qd) any_p2win |= d.p2win != 0;
     st.roots_ms = ms_since(clk);
@@ -422,7 +458,7 @@ void run_batch(cpx_ctx *ctx, const BatchReq &rq)
     if (mask & TERM_HARD) {
         for (QD &d : qd)
             if (!d.direct) d.nb = (uint32_t)host_pi(hP, d.r4);
-        choose_lbits(ctx, qd, c, threads, rq.lbits);
+        choose_lbits(ctx, qd, c, threads, rq.lbits, lbits_cap, tune);
     }
 
     // ---- units per kernel family (queries planned in parallel blocks)
@@ -561,7 +597,7 @@ void run_batch(cpx_ctx *ctx, const BatchReq &rq)
         // the host; the threshold doubles until the pool fits the budget
         const size_t stride = hard_snapshot_stride(lbits_max - (uint32_t)(__builtin_ctz(threads) - 5));
         const uint64_t budget = std::max<uint64_t>(1, ctx->hard_offload_bytes / (stride + sizeof(HardJob)));
-        uint64_t thr = ctx->hard_offload_min, njobs = 0;
+        uint64_t thr = offload0, njobs = 0;
         while (thr) {
             std::atomic<uint64_t> total(0);
             parallel_blocks(nblk, [&](size_t k) {

@@ -27,6 +27,9 @@ struct BatchReq {
     u128 *out_pi = nullptr;                 // n entries
     i128 *out_terms = nullptr;              // 7 per query: P2 ord triv easy hard pi_y pi
     uint64_t *out_y = nullptr;
+    uint32_t alpha_scale = 0;         // per mille of the reference alpha (0: 1000) when alpha_num = 0
+    uint32_t lbits_cap = 0;           // cap of the hard-leaf segment bits (0: context default)
+    const TuneEntry *tune = nullptr;  // per-decade alpha scale when alpha_num = alpha_scale = 0
     bool wide = false;   // 128-bit kernels even when every x < 2^64
     bool graph = false;  // one CUDA graph launch for the batch's kernels
 };
@@ -44,6 +47,12 @@ void grow_tables(cpx_ctx *ctx, const TableNeed &need);
 // host mirror of the resident prime list, and pi(v) by binary search in it
 const std::vector<uint32_t> &host_primes(cpx_ctx *ctx);
 uint64_t host_pi(const std::vector<uint32_t> &P, uint64_t v);
+// autotuning (autotune.cu)
+uint32_t decade_of(u128 x);
+void autotune(cpx_ctx *ctx, uint32_t e_lo, uint32_t e_hi, double seconds);
+void autotune_batch(cpx_ctx *ctx, const u128 *xs, size_t n);
+void tune_save(const cpx_ctx *ctx, const char *path);
+void tune_load(cpx_ctx *ctx, const char *path);
 // exact special-leaf counts of one query: hard, easy (composite m), easy (prime m), trivial
 void leaf_counts(cpx_ctx *ctx, u128 x, uint64_t y, uint32_t c, uint64_t out[4]);
 uint64_t default_y(u128 x, uint32_t num, uint32_t den);

@@ -233,6 +233,35 @@ typedef struct {
 int cpx_pi_batch(cpx_ctx *ctx, const cpx_u128 *xs, size_t n, const cpx_params *params,
                  cpx_u128 *out);
 
+/* ---- autotuning ---------------------------------------------------------
+ * Candidate settings are timed on the device by coordinate descent: the cap
+ * of the hard-leaf segment bits with the threads per segment, then the alpha
+ * scale (per mille of the reference alpha(x)), then the offload threshold.
+ * cpx_autotune tunes each decade of x in [decade_lo, decade_hi] (6..30) on
+ * lone queries at 10^e and 10^(e+1/2): the plain path, applied to
+ * batches of up to four queries (threads and offload of the largest query's
+ * decade); it stops after the decade that passes `seconds` (0: no limit).
+ * cpx_autotune_batch tunes one entry on a sample batch (>= 5 queries),
+ * applied to larger batches.  Settings a request fixes win.  Results never
+ * change; only the time does.  cpx_tune_get(ctx, 99, ...) reads the batch
+ * entry.  No reference counterpart (its segment length and block shape are
+ * fixed at compile time, src/sieve/S2_hard_device.cuh:7-22, and its alpha is
+ * a formula, src/main.cpp:128-194). */
+typedef struct {
+    uint32_t decade;             /* 99: the batch entry */
+    uint32_t alpha_scale_milli;  /* per mille of the reference alpha; 0 = 1000 */
+    uint32_t log2_bits;          /* segment-bit cap; 0 = context default */
+    uint32_t threads;            /* 0: not tuned */
+    uint32_t offload_min;
+    float ms;                    /* sample time */
+} cpx_tune_entry;
+int cpx_autotune(cpx_ctx *ctx, uint32_t decade_lo, uint32_t decade_hi, double seconds);
+int cpx_autotune_batch(cpx_ctx *ctx, const cpx_u128 *xs, size_t n);
+int cpx_tune_save(cpx_ctx *ctx, const char *path);  /* JSON */
+int cpx_tune_load(cpx_ctx *ctx, const char *path);
+int cpx_tune_get(cpx_ctx *ctx, uint32_t decade, cpx_tune_entry *out);
+int cpx_tune_clear(cpx_ctx *ctx);
+
 /* Exact special-leaf counts of pi(x) with y (0: the y rule), in this
  * library's split, u = x/(p_b m): trivial u < p_b; easy p_b <= u < p_b^2
  * (prime m, composite m); hard u >= p_b^2.  Replaces the leaf-count
