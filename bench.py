@@ -426,8 +426,10 @@ def main():
     roof = {"bound": "hbm", "kernel": "k_hard (special-leaf phi sieve)", "achieved": (hb / hs) / 1e9 if hs else None,
             "peak": hbm, "unit": "GB/s", "frac": ((hb / hs) / 1e9) / hbm if hs else None,
             "peak_kind": kind, "traffic": tr.get("k_hard_dram_bytes_per_launch") if tr else None,
+            "alu_pipe_frac_ncu": tr.get("k_hard_alu_pipe_frac") if tr else None,
             "note": "achieved = S2 bitmap bytes (one pass of the segment bitmap per active prime per segment) / "
-                    "k_hard duration; these passes run in shared memory, so the HBM fraction is a proxy"}
+                    "hard-leaf kernels' duration; these passes run in shared memory and the kernel is integer-ALU "
+                    "bound (alu_pipe_frac_ncu, profiles/k_hard_batch4096.md), so the HBM fraction is a proxy"}
     cpu = None if args.no_cpu else cpu_baseline(xs, args.cpu_budget)
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
