@@ -109,21 +109,23 @@ __device__ __forceinline__ uint64_t cpx_pi_dev(const cpx_pient *__restrict__ T, 
 }
 
 // ------------------------------------------------ leaf quotients floor(n / d)
-// Leaves divide a fixed x/p by many m < 2^32 with quotients below 2^44.  The
-// quotient is taken from the double product n * (1/d) and made exact by one
-// integer correction, instead of the general 64-bit division routine:
+// Leaves and level parameters divide 64-bit values by d < 2^32.  The quotient
+// is taken from the double product n * (1/d) and made exact in integers,
+// instead of the general 64-bit division routine:
 //   r0 = 1/d rounded to float, then one Newton-Raphson step in double
 //   rd = r0 + r0 (1 - d r0), relative error < 2^-45;
-//   v = n * rd is within 0.15 of n/d when n/d < 2^44, so trunc(v) is
-//   floor(n/d) - 1, floor(n/d) or floor(n/d) + 1, and the sign of
-//   n - trunc(v) d settles which.  Other operands use the hardware path.
-// the hardware-path 64-bit quotient, kept out of line: every inlined copy of
-// it would cost the calling loops instruction-cache space
+//   q0 = trunc(n * rd) is within 2^-44.9 n/d + 1 of the quotient.
+//   n/d < 2^44: q0 is floor(n/d) - 1, floor(n/d) or floor(n/d) + 1, and the
+//   sign of n - q0 d settles which.
+//   larger n/d (< 2^64): the remainder r = n - q0 d is below 2^52 in
+//   magnitude, so r and r * rd are exact enough in double; t = floor(r * rd)
+//   corrected by the sign of r - t d gives floor(n/d) = q0 + t.
+// d >= 2^32 uses the hardware path.
 static __device__ __noinline__ uint64_t cpx_udiv_slow(uint64_t n, uint64_t d) { return n / d; }
 
 __device__ __forceinline__ uint64_t cpx_udiv_leaf(uint64_t n, uint64_t d)
 {
-    if ((d >> 32) || (n >> 44) >= d) return cpx_udiv_slow(n, d);
+    if (d >> 32) return cpx_udiv_slow(n, d);
     const uint32_t d32 = (uint32_t)d;
     const double r = (double)__frcp_rn(__uint2float_rn(d32));
     const double dd = (double)d32;
@@ -131,9 +133,16 @@ __device__ __forceinline__ uint64_t cpx_udiv_leaf(uint64_t n, uint64_t d)
     const double rd = __fma_rn(r, e, r);
     uint64_t u = __double2ull_rz(__dmul_rn(__ull2double_rn(n), rd));
     const int64_t rem = (int64_t)(n - u * d);
-    if (rem < 0) u--;
-    else if (rem >= (int64_t)d) u++;
-    return u;
+    if ((n >> 44) < d) {
+        if (rem < 0) u--;
+        else if (rem >= (int64_t)d) u++;
+        return u;
+    }
+    int64_t t = __double2ll_rd(__dmul_rn(__ll2double_rn(rem), rd));
+    const int64_t r2 = rem - t * (int64_t)d32;
+    if (r2 < 0) t--;
+    else if (r2 >= (int64_t)d32) t++;
+    return u + (uint64_t)t;
 }
 __device__ __forceinline__ uint64_t cpx_qdiv(uint64_t n, uint64_t d) { return cpx_udiv_leaf(n, d); }
 // 128-bit dividend: x/p is below 2^64 for x < 2^64 p, so most leaf

@@ -189,7 +189,7 @@ template <class XT> struct LvlPar {
 template <class XT>
 __device__ __noinline__ void level_params(LvlPar<XT> &o, XT x, uint64_t y, uint64_t p, uint64_t lo_w, uint64_t hi_w)
 {
-    const XT xp = x / (XT)p;
+    const XT xp = cpx_qdiv(x, p);
     uint64_t mlo = y / p;
     const XT t1 = cpx_qdiv(xp, hi_w);
     if (t1 > (XT)mlo) mlo = (uint64_t)t1;
@@ -198,7 +198,7 @@ __device__ __noinline__ void level_params(LvlPar<XT> &o, XT x, uint64_t y, uint6
         const XT t2 = cpx_qdiv(xp, lo_w);
         if (t2 < (XT)mhi) mhi = (uint64_t)t2;
     }
-    const XT t3 = xp / (XT)(p * p);  // hard leaves only: m <= x/p^3
+    const XT t3 = cpx_qdiv(xp, p * p);  // hard leaves only: m <= x/p^3
     if (t3 < (XT)mhi) mhi = (uint64_t)t3;
     if (mhi < mlo) mhi = mlo;
     o.p = (uint32_t)p;

@@ -63,7 +63,7 @@ __global__ void __launch_bounds__(kThreads) k_ordinary(const QD *__restrict__ qd
                 const int32_t v = vals[k];
                 if (n > y || v == 0) continue;
                 if ((v > 0 ? v : -v) <= Wh::PC) continue;
-                const XT m = x / (XT)n;
+                const XT m = cpx_qdiv(x, n);
                 const XT qw = m / (XT)Wh::W;
                 const uint32_t r = (uint32_t)(m - qw * (XT)Wh::W);
                 const i128 ph = (i128)qw * (i128)Wh::TOT + (i128)__ldg(WH + ((r + 1) >> 1));
@@ -281,11 +281,11 @@ template <class XT>
 __device__ __noinline__ bool easy_plan(XT x, uint64_t y, uint64_t p, uint64_t prm_max,
                                           const cpx_pient *__restrict__ T, XT &xp, EasyP &e)
 {
-    xp = x / (XT)p;
+    xp = cpx_qdiv(x, p);
     uint64_t qlo = y / p;
     if (qlo < p) qlo = p;
-    const XT xpp = xp / (XT)p;
-    const XT x3 = xpp / (XT)p;  // p <= iroot4(x): only q > x/p^3 (x/(pq) < p^2) are easy
+    const XT xpp = cpx_qdiv(xp, p);
+    const XT x3 = cpx_qdiv(xpp, p);  // p <= iroot4(x): only q > x/p^3 (x/(pq) < p^2) are easy
     if (x3 > (XT)qlo) qlo = (x3 >= (XT)y) ? y : (uint64_t)x3;
     const uint64_t qhi = (xpp < (XT)y) ? (uint64_t)xpp : y;
     if (qhi <= qlo) return false;
@@ -427,7 +427,7 @@ __global__ void __launch_bounds__(kThreads) k_easy_comp(const QD *__restrict__ q
         }
         const EasyLvl r = lv[lo];
         const QD &d = qd[r.q];
-        const XT xp = xload<XT>(d) / (XT)r.p;
+        const XT xp = cpx_qdiv(xload<XT>(d), r.p);
         const uint64_t base = r.i_base + (unit - r.unit0) * 1024;  // multiple of 4
         int64_t s = 0;
         for (int it = 0; it < 8; it++) {
