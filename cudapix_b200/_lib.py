@@ -93,6 +93,11 @@ class TuneEntry(ctypes.Structure):
                 ("threads", ctypes.c_uint32), ("offload_min", ctypes.c_uint32), ("ms", ctypes.c_float)]
 
 
+class HardLevel(ctypes.Structure):
+    _fields_ = [("count", ctypes.c_uint64), ("msum", ctypes.c_int64), ("carry0", ctypes.c_uint64),
+                ("anchored", ctypes.c_uint32), ("pad", ctypes.c_uint32)]
+
+
 class Params(ctypes.Structure):
     _fields_ = [
         ("alpha_num", ctypes.c_uint32),
@@ -151,6 +156,9 @@ _SIGS = {
     "cpx_set_hard_params": (ctypes.c_int, [P, u32, u32]),
     "cpx_set_hard_offload": (ctypes.c_int, [P, u32]),
     "cpx_set_p2_window": (ctypes.c_int, [P, u64]),
+    "cpx_S2_hard_layout": (ctypes.c_int, [P, U128, u64, u16, u32, pu64, pu32]),
+    "cpx_S2_hard_part": (ctypes.c_int, [P, U128, u64, u16, u32, u64, u64, pU, ctypes.POINTER(HardLevel)]),
+    "cpx_S2_hard_merge": (ctypes.c_int, [pU, ctypes.POINTER(HardLevel), u32, u32, pU]),
     "cpx_autotune": (ctypes.c_int, [P, u32, u32, ctypes.c_double]),
     "cpx_autotune_batch": (ctypes.c_int, [P, pU, ctypes.c_size_t]),
     "cpx_tune_save": (ctypes.c_int, [P, ctypes.c_char_p]),

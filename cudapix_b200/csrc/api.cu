@@ -99,6 +99,7 @@ void release_context(cpx_ctx *ctx)
     ctx->b_jobs.release();
     ctx->b_jobctl.release();
     ctx->b_snap.release();
+    ctx->b_levels.release();
     if (ctx->graph_exec) cudaGraphExecDestroy(ctx->graph_exec);
     ctx->graph_exec = nullptr;
     for (cudaEvent_t *ev : {&ctx->ev_hard0, &ctx->ev_hard1, &ctx->ev_b0, &ctx->ev_b1, &ctx->ev_t0, &ctx->ev_t1}) {
@@ -205,6 +206,79 @@ int cpx_leaf_count(cpx_ctx *ctx, cpx_u128 x, uint64_t y, uint16_t c, cpx_leaf_co
         out->easy_prime = v[2];
         out->trivial = v[3];
     });
+}
+
+// segment bits a forced request gets for the context's threads (choose_lbits)
+static uint32_t part_bits(const cpx_ctx *ctx, uint32_t log2_bits)
+{
+    const uint32_t th = ctx->hard_threads;
+    const uint32_t minb = (th >= 512) ? 16 : (th >= 256 ? 15 : 14);
+    return std::max(minb, std::min<uint32_t>(log2_bits, 20));
+}
+
+int cpx_S2_hard_layout(cpx_ctx *ctx, cpx_u128 x, uint64_t y, uint16_t c, uint32_t log2_bits, uint64_t *nseg,
+                       uint32_t *nlevels)
+{
+    return guarded(ctx, [&] {
+        if (!nseg || !nlevels || !y) fail(CPX_EINVAL, "null output or y = 0");
+        const u128 xv = U(x);
+        const uint64_t z = (uint64_t)(xv / y), r4 = cpx_iroot4(xv);
+        const uint32_t cc = c ? c : 6;
+        ensure_primes(ctx, r4 + 2);
+        const uint64_t nb = host_pi(host_primes(ctx), r4);
+        const uint64_t span = 2ull << part_bits(ctx, log2_bits);
+        *nseg = (z + 1 + span - 1) / span;
+        *nlevels = nb > cc ? (uint32_t)(nb - cc) : 0;
+    });
+}
+
+int cpx_S2_hard_part(cpx_ctx *ctx, cpx_u128 x, uint64_t y, uint16_t c, uint32_t log2_bits, uint64_t seg_lo,
+                     uint64_t seg_hi, cpx_u128 *h_part, cpx_hard_level *levels)
+{
+    static_assert(sizeof(cpx_hard_level) == sizeof(HardLevel), "level record layout");
+    return guarded(ctx, [&] {
+        if (!h_part || !levels) fail(CPX_EINVAL, "null output");
+        if (!log2_bits) fail(CPX_EINVAL, "log2_bits must be given (the same for every part)");
+        u128 xv = U(x);
+        uint64_t yv = y;
+        i128 t[7] = {};
+        BatchReq rq;
+        rq.xs = &xv;
+        rq.ys = &yv;
+        rq.n = 1;
+        rq.c = c ? c : 6;
+        rq.terms = TERM_HARD;
+        rq.lbits = log2_bits;
+        rq.threads = ctx->hard_threads;
+        rq.seg_lo = seg_lo;
+        rq.seg_hi = seg_hi;
+        rq.hard_levels = reinterpret_cast<HardLevel *>(levels);
+        rq.out_terms = t;
+        run_batch(ctx, rq);
+        *h_part = C128s(t[4]);
+    });
+}
+
+int cpx_S2_hard_merge(const cpx_u128 *h, const cpx_hard_level *levels, uint32_t nparts, uint32_t nlevels,
+                      cpx_u128 *out)
+{
+    if (!h || !out || (nlevels && !levels)) return CPX_EINVAL;
+    std::vector<u128> carry(nlevels, 0);
+    i128 H = 0;
+    for (uint32_t k = 0; k < nparts; k++) {
+        H += (i128)U(h[k]);
+        for (uint32_t b = 0; b < nlevels; b++) {
+            const cpx_hard_level &lv = levels[(size_t)k * nlevels + b];
+            if (lv.anchored) {
+                carry[b] = (u128)lv.carry0 + lv.count;
+            } else {
+                H += (i128)carry[b] * lv.msum;
+                carry[b] += lv.count;
+            }
+        }
+    }
+    *out = C128s(H);
+    return CPX_OK;
 }
 
 int cpx_autotune(cpx_ctx *ctx, uint32_t decade_lo, uint32_t decade_hi, double seconds)

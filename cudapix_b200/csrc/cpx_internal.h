@@ -92,6 +92,7 @@ struct cpx_ctx {
     cpx::DevBuf b_work[8];   // term kernels' work arrays
     cpx::DevBuf b_flush;     // L2 flush buffer (bench only)
     cpx::DevBuf b_jobs, b_jobctl, b_snap;  // offloaded hard-leaf sets and their snapshots
+    cpx::DevBuf b_levels;                  // per-level records of a part of a split query
     unsigned long long *d_acc = nullptr;  // per-query accumulators (grown)
     size_t acc_cap = 0;
     unsigned long long *h_acc = nullptr;  // pinned mirror

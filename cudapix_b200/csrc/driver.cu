@@ -93,15 +93,16 @@ static uint64_t easy_u_bound(u128 x)
 
 // Segments (of `span` integers) that sieve level b, p = p_b: those with
 // hi > p^2 and (lo = 0 or p^2 lo < x); the same rule as k_hard_plan.
-static uint64_t segments_at_level(u128 x, uint64_t span, uint64_t p, uint64_t nseg)
+static uint64_t segments_at_level(u128 x, uint64_t span, uint64_t p, uint64_t seg0, uint64_t nseg)
 {
     const uint64_t p2 = p * p;  // p <= iroot4(x) < 2^32
-    const uint64_t first = p2 / span;
+    const uint64_t first = std::max<uint64_t>(p2 / span, seg0);
     // largest s >= 0 with s * span * p^2 < x (p^2 span < 2^64 for the segment sizes used)
     const u128 d = (u128)p2 * span;
-    const uint64_t last = (x >> 64) || (d >> 64) ? (uint64_t)std::min<u128>((x - 1) / d, (u128)nseg)
+    const uint64_t end = seg0 + nseg;
+    const uint64_t last = (x >> 64) || (d >> 64) ? (uint64_t)std::min<u128>((x - 1) / d, (u128)end)
                                                  : ((uint64_t)x - 1) / (uint64_t)d;
-    const uint64_t hi = std::min<uint64_t>(last, nseg - 1);
+    const uint64_t hi = std::min<uint64_t>(last, end - 1);
     return hi >= first ? hi - first + 1 : 0;
 }
 
@@ -117,7 +118,7 @@ static uint64_t heavy_leaf_sets(const QD &d, const std::vector<uint32_t> &hP, ui
                                 uint64_t limit)
 {
     const uint64_t NW = threads / 32, Lw = (1ull << d.lbits) / NW, span_w = 2 * Lw;
-    const uint64_t nsub = d.nseg * NW, L2 = 2ull << d.lbits;
+    const uint64_t w_beg = d.seg0 * NW, nsub = (d.seg0 + d.nseg) * NW, L2 = 2ull << d.lbits;
     const XT x = (XT)d.x;
     const uint64_t y = d.y;
     uint64_t jobs = 0;
@@ -134,7 +135,7 @@ static uint64_t heavy_leaf_sets(const QD &d, const std::vector<uint32_t> &hP, ui
         const double most = 1.001 * dm * dm * dsw / ((double)xp + dsw * dm) + 2.0;
         if (0.5 * most + 17.0 < (double)thr) continue;
         const bool prime_lvl = p * p > y;
-        for (uint64_t w = (uint64_t)(xp / (XT)mtop) / span_w; w < nsub; w++) {
+        for (uint64_t w = std::max<uint64_t>((uint64_t)(xp / (XT)mtop) / span_w, w_beg); w < nsub; w++) {
             const uint64_t lo_w = w * span_w, hi_w = lo_w + span_w;
             const uint64_t lo = (w / NW) * L2;
             if ((u128)p * p > (u128)(lo + L2 - 1) || (lo && (u128)p * p > (u128)((x - 1) / (XT)lo))) continue;
@@ -407,6 +408,8 @@ void run_batch(cpx_ctx *ctx, const BatchReq &rq)
     const uint32_t c = rq.c;
     if (c < 1 || c > 8) fail(CPX_EINVAL, "c must be in 1..8");
     const unsigned mask = rq.terms;
+    if (rq.seg_hi && (Q != 1 || mask != TERM_HARD || !rq.lbits || rq.seg_lo >= rq.seg_hi))
+        fail(CPX_EINVAL, "a segment range needs one query, the hard term alone and fixed segment bits");
     // tuned settings: per decade for the plain path (up to 4 queries), the
     // batch entry above that; a request's own settings win
     const bool small = Q <= 4;
@@ -512,10 +515,15 @@ void run_batch(cpx_ctx *ctx, const BatchReq &rq)
                 if ((mask & TERM_HARD) && d.nb > c) {
                     const uint64_t span = 2ull << d.lbits;
                     d.nseg = (d.z + 1 + span - 1) / span;
+                    if (rq.seg_hi) {  // one part of a query split over GPUs
+                        d.seg0 = std::min(rq.seg_lo, d.nseg);
+                        d.nseg = std::min(rq.seg_hi, d.nseg) - d.seg0;
+                    }
                     n_seg = d.nseg;
                     n_comb = d.nb - c;
                     uint64_t ent = 0;
-                    for (uint32_t b = c + 1; b <= d.nb; b++) ent += segments_at_level(x, span, hP[b - 1], d.nseg);
+                    for (uint32_t b = c + 1; b <= d.nb; b++)
+                        ent += segments_at_level(x, span, hP[b - 1], d.seg0, d.nseg);
                     q_ent[i] = ent;
                 }
             }
@@ -622,6 +630,12 @@ void run_batch(cpx_ctx *ctx, const BatchReq &rq)
         pl.snap = static_cast<unsigned char *>(ctx->b_snap.get((pl.max_jobs + 1) * stride));
     }
     if (pl.n_easy) pl.easy_off = ctx->b_work[7].as<uint64_t>(pl.n_easy + 1);
+    uint32_t n_levels = 0;
+    if (rq.hard_levels && !qd[0].direct && qd[0].nb > c) {
+        n_levels = qd[0].nb - c;
+        pl.hard_levels = ctx->b_levels.as<HardLevel>(n_levels + 1);
+        CPX_CUDA(cudaMemsetAsync(pl.hard_levels, 0, n_levels * sizeof(HardLevel), ctx->stream));
+    }
     // every buffer the launches touch exists before the first launch (no
     // allocation between kernels, so the sequence can be captured in a graph)
     scan_reserve(ctx, std::max<uint64_t>(std::max<uint64_t>(pl.n_seg, pl.n_easy + 1), (uint64_t)pl.max_jobs + 1));
@@ -688,6 +702,9 @@ void run_batch(cpx_ctx *ctx, const BatchReq &rq)
             o[6] = rd(ACC_PI);
         }
         if (rq.out_y) rq.out_y[i] = qd[i].y;
+    }
+    if (n_levels) {
+        CPX_CUDA(cudaMemcpy(rq.hard_levels, pl.hard_levels, n_levels * sizeof(HardLevel), cudaMemcpyDeviceToHost));
     }
     if (ctx->timing) CPX_CUDA(cudaEventElapsedTime(&ctx->last_batch_ms, ctx->ev_b0, ctx->ev_b1));
     if (pl.time_hard && pl.n_seg) {

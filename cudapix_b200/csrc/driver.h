@@ -30,6 +30,8 @@ struct BatchReq {
     uint32_t alpha_scale = 0;         // per mille of the reference alpha (0: 1000) when alpha_num = 0
     uint32_t lbits_cap = 0;           // cap of the hard-leaf segment bits (0: context default)
     const TuneEntry *tune = nullptr;  // per-decade alpha scale when alpha_num = alpha_scale = 0
+    uint64_t seg_lo = 0, seg_hi = 0;  // one query's hard-leaf segments [seg_lo, seg_hi) (0, 0: all)
+    HardLevel *hard_levels = nullptr; // per-level records of that part (host, nb - c entries)
     bool wide = false;   // 128-bit kernels even when every x < 2^64
     bool graph = false;  // one CUDA graph launch for the batch's kernels
 };

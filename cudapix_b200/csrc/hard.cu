@@ -240,7 +240,7 @@ __global__ void __launch_bounds__(512, 2) k_hard(const QD *__restrict__ qd, uint
     const uint32_t CPT = NC / T;   // chunks per lane (>= 1)
     const int s = __ffs(CPT) - 1;  // log2 CPT
     const uint32_t Lw = L / NW;    // bits of a warp's sub-segment
-    const uint64_t seg = unit - pre_seg[q];
+    const uint64_t seg = unit - pre_seg[q] + d.seg0;
     const uint64_t lo = seg * 2 * (uint64_t)L;
     const uint64_t lo_w = lo + 2 * (uint64_t)Lw * warp, hi_w = lo_w + 2 * (uint64_t)Lw;
     const uint64_t off = seg_off[unit];
@@ -598,7 +598,7 @@ __global__ void k_hard_plan(const QD *__restrict__ qd, uint32_t Q, const uint64_
     if (u >= total) return;
     const uint32_t q = find_q(pre_seg, Q, u);
     const QD &d = qd[q];
-    const uint64_t seg = u - pre_seg[q];
+    const uint64_t seg = u - pre_seg[q] + d.seg0;
     const uint64_t lo = seg * 2 * (1ull << d.lbits), hi = lo + 2 * (1ull << d.lbits);
     const XT x = xload<XT>(d);
     uint64_t v = d.r4;
@@ -631,7 +631,7 @@ __global__ void k_hard_combine(const QD *__restrict__ qd, uint32_t Q, const uint
                                const uint32_t *__restrict__ seg_B, const uint64_t *__restrict__ seg_off,
                                const uint32_t *__restrict__ cnt, const int32_t *__restrict__ ms, uint64_t cap,
                                const uint32_t *__restrict__ P, const cpx_pient *__restrict__ T,
-                               unsigned long long *__restrict__ acc)
+                               unsigned long long *__restrict__ acc, HardLevel *__restrict__ lvl_out)
 {
     const uint64_t u = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const uint32_t lane = threadIdx.x & 31;
@@ -643,12 +643,19 @@ __global__ void k_hard_combine(const QD *__restrict__ qd, uint32_t Q, const uint
     const uint64_t span = 2ull << d.lbits;
     const uint64_t p = P[b - 1];
     const uint64_t first = (p * p) / span;  // first segment with hi > p^2
-    const uint64_t s0 = pre_seg[q] + first, s1 = pre_seg[q + 1];
+    // the query's segments here are seg0 .. seg0 + n - 1 (all of them unless
+    // the query is split over GPUs); carries below the part come from outside
+    const uint64_t g0 = d.seg0, g1 = d.seg0 + (pre_seg[q + 1] - pre_seg[q]);
+    const uint64_t fl = first > g0 ? first : g0;
+    const uint64_t s0 = pre_seg[q] + (fl - g0), s1 = pre_seg[q + 1];
+    const bool anchored = first >= g0 && first < g1;
     uint64_t carry = 0;
-    if (first > 0 && s0 < s1) {
+    if (anchored && first > 0) {
         const uint64_t pl = cpx_pi_dev(T, first * span - 1);
         carry = 1 + (pl > b - 1 ? pl - (b - 1) : 0);
     }
+    const uint64_t carry0 = carry;
+    int64_t msl = 0;
     i128 H = 0;
     for (uint64_t base = s0; base < s1; base += 32) {
         const uint64_t sg = base + lane;
@@ -676,11 +683,17 @@ __global__ void k_hard_combine(const QD *__restrict__ qd, uint32_t Q, const uint
             if (lane >= (uint32_t)o) inc += t;
         }
         H += (i128)(carry + inc - cv) * (i128)mv;
+        msl += mv;
         carry += __shfl_sync(FULL, inc, 31);
         if (stop >= 0) break;
     }
     H = cpx_warp_sum_i128(H);
     if (lane == 0) acc_add(acc, q, ACC_HARD, H);
+    if (lvl_out && q == 0) {
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) msl += __shfl_down_sync(FULL, msl, o);
+        if (lane == 0) lvl_out[lvl] = HardLevel{carry - carry0, msl, carry0, anchored ? 1u : 0u, 0u};
+    }
 }
 
 // ------------------------------------------------------------------ launchers
@@ -725,7 +738,7 @@ template <class XT> static void hard_go(cpx_ctx *ctx, const Plan &pl)
     if (pl.n_comb) {
         k_hard_combine<<<(unsigned)((pl.n_comb * 32 + 255) / 256), 256, 0, ctx->stream>>>(
             pl.qd, pl.Q, pl.pre_comb, pl.n_comb, pl.pre_seg, pl.seg_B, pl.seg_off, pl.hard_cnt, pl.hard_ms,
-            pl.hard_entries, tb.P, tb.T, pl.acc);
+            pl.hard_entries, tb.P, tb.T, pl.acc, pl.hard_levels);
         CPX_LAUNCH("k_hard_combine");
         note_launch(ctx);
     }

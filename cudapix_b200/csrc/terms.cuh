@@ -13,6 +13,17 @@ struct __align__(16) QD {
     uint32_t lbits, direct;         // hard segment = 2^lbits odd numbers; direct = count by table
     uint64_t nseg;                  // hard-leaf segments over [0, z]
     uint32_t p2win, pad;            // p2win: P2 by pi-table windows over [sqrt x, z] (z beyond the table)
+    uint64_t seg0;                  // first hard-leaf segment (a part of a query split over GPUs)
+};
+
+// Per level b of a query's part: survivors of level b-1 over its segments,
+// Sum(-mu) of its leaves, and, when the level's first sieved segment lies in
+// the part, the carry that segment starts with (anchored = 1).
+struct HardLevel {
+    uint64_t count;
+    int64_t msum;
+    uint64_t carry0;
+    uint32_t anchored, pad;
 };
 
 // One level of composite easy leaves of one query: odd m = 2i + 1 with
@@ -73,6 +84,7 @@ struct Plan {
     uint32_t n_elv = 0;
     uint64_t n_ecomp = 0;
     uint64_t *easy_off = nullptr;  // n_easy + 1 chunk offsets of the easy leaves
+    HardLevel *hard_levels = nullptr;  // per-level outputs of query 0 (a part of a split query)
 };
 
 void launch_ordinary(cpx_ctx *ctx, const Plan &pl);

@@ -233,6 +233,33 @@ typedef struct {
 int cpx_pi_batch(cpx_ctx *ctx, const cpx_u128 *xs, size_t n, const cpx_params *params,
                  cpx_u128 *out);
 
+/* ---- one query split over GPUs (hard leaves) -----------------------------
+ * The hard-leaf sieve runs over segments 0 .. nseg-1 of 2^log2_bits odd
+ * numbers (cpx_S2_hard_layout).  Each GPU takes a contiguous range
+ * [seg_lo, seg_hi) with cpx_S2_hard_part: its local hard sum (carries from
+ * below its range taken as 0 unless the level starts inside it) and, per
+ * level b = c+1 .. pi(x^(1/4)), the survivors of level b-1 over its
+ * segments, Sum(-mu) of its leaves, and the start carry when the level's
+ * first segment is in the range.  One exchange of those records (an
+ * all-gather) and cpx_S2_hard_merge, a host-only sum over the parts in
+ * segment order, give S2_hard(x, y, c).  Every part must use the same
+ * log2_bits and the context's threads per segment.  The plan of the
+ * reference's multi-GPU notes; the reference itself runs on one GPU. */
+typedef struct {
+    uint64_t count;     /* survivors of level b-1 in the part's segments */
+    int64_t msum;       /* Sum(-mu(m)) of the part's leaves of level b */
+    uint64_t carry0;    /* start carry of the level when anchored */
+    uint32_t anchored;  /* the level's first sieved segment lies in the part */
+    uint32_t pad;
+} cpx_hard_level;
+int cpx_S2_hard_layout(cpx_ctx *ctx, cpx_u128 x, uint64_t y, uint16_t c, uint32_t log2_bits, uint64_t *nseg,
+                       uint32_t *nlevels);
+int cpx_S2_hard_part(cpx_ctx *ctx, cpx_u128 x, uint64_t y, uint16_t c, uint32_t log2_bits, uint64_t seg_lo,
+                     uint64_t seg_hi, cpx_u128 *h_part, cpx_hard_level *levels);
+/* parts[k] = (h[k], levels[k * nlevels .. ]) for ranges in segment order */
+int cpx_S2_hard_merge(const cpx_u128 *h, const cpx_hard_level *levels, uint32_t nparts, uint32_t nlevels,
+                      cpx_u128 *out);
+
 /* ---- autotuning ---------------------------------------------------------
  * Candidate settings are timed on the device by coordinate descent: the cap
  * of the hard-leaf segment bits with the threads per segment, then the alpha
