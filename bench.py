@@ -246,6 +246,15 @@ def barrier(world):
         dist.barrier()
 
 
+def arm_config(args, world):
+    """The workload both arms report (the reference arm runs it on the host cores)."""
+    return {"workload": "batch4096: x = floor(10^e), e ~ U[9,14], numpy default_rng(0)",
+            "queries": args.queries, "c": 6, "alpha": "reference alpha(x)",
+            "l2": "flushed before every timed step (256 MiB write)",
+            "tuning": os.path.relpath(TUNING, ROOT) if os.path.exists(TUNING) else None,
+            "parallelism": f"replicas x{world}"}
+
+
 def run_reference(args, world, rank):
     if rank != 0:
         return
@@ -273,8 +282,7 @@ def run_reference(args, world, rank):
     line = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": 1000 * t / len(per_step), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "int64/int128", "data": "synthetic",
-            "config": {"workload": "batch4096: x = floor(10^e), e ~ U[9,14], numpy default_rng(0)",
-                       "queries": args.queries, "c": 6, "alpha": "reference alpha(x)"},
+            "config": arm_config(args, world),
             "cpu_baseline": {"value": v, "unit": UNIT, "cores": nthreads, "kind": "port", "sample": sample},
             "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
@@ -435,11 +443,7 @@ def main():
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": max(args.warmup, 3), "ms_per_step": 1000 * t_dev / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "int64/int128", "data": "synthetic",
-        "config": {"workload": "batch4096: x = floor(10^e), e ~ U[9,14], numpy default_rng(0)",
-                   "queries": args.queries, "c": 6, "alpha": "reference alpha(x)",
-                   "l2": "flushed before every timed step (256 MiB write)",
-                   "tuning": os.path.relpath(TUNING, ROOT) if os.path.exists(TUNING) else None,
-                   "parallelism": f"replicas x{world}"},
+        "config": arm_config(args, world),
         "e2e": {"value": nq / t_e2e, "unit": UNIT, "h2d_bytes_per_step": io[0], "d2h_bytes_per_step": io[1]},
         "gpu_launches": int(launches),
         "host_ms": {k: round(statistics.median(h[k] for h in host_stats), 3)
