@@ -80,6 +80,9 @@ __host__ __device__ __forceinline__ size_t snap_stride(uint32_t lbits_sub)
     return (nc * 20 + 255) & ~size_t(255);
 }
 
+// leaves a warp gathers before answering them 32 at a time
+constexpr uint32_t kLeafBuf = 256;
+
 struct LvlOut {
     uint32_t cnt;
     int32_t ms;
@@ -96,6 +99,7 @@ __host__ __device__ __forceinline__ size_t hard_smem(uint32_t lbits, uint32_t th
     o += 2 * (threads / 32) * 32 * sizeof(LvlOut);    // per-warp level outputs, double buffered
     o = (o + 15) & ~size_t(15);
     o += 32 * sizeof(i128);                           // reductions
+    o += (threads / 32) * kLeafBuf * 4;               // per-warp gathered leaves
     return o;
 }
 
@@ -261,6 +265,8 @@ __global__ void __launch_bounds__(512, 2) k_hard(const QD *__restrict__ qd, uint
     o += 2 * NW * 32 * sizeof(LvlOut);
     o = (o + 15) & ~size_t(15);
     i128 *s_red = reinterpret_cast<i128 *>(sp + o);
+    o += 32 * sizeof(i128);
+    uint32_t *lbuf = reinterpret_cast<uint32_t *>(sp + o) + kLeafBuf * warp;  // this warp's gathered leaves
     uint32_t *wl = loff + 32 * warp;  // this warp's lane prefixes
 
     const uint32_t c0 = CPT * tid;  // first owned chunk (of the segment)
@@ -367,44 +373,89 @@ __global__ void __launch_bounds__(512, 2) k_hard(const QD *__restrict__ qd, uint
                     }
                 }
                 if (!offloaded) {
+                    // The lanes gather the level's leaves (m, with bit 31 set when
+                    // mu(m) = -1) into the warp's buffer and answer them 32 at a time,
+                    // so that a lane with many candidates does not hold up the others.
                     int32_t msl = 0;
+                    uint32_t nbuf = 0;
+                    auto flush = [&] {
+                        __syncwarp();
+                        for (uint32_t jj = lane; jj < nbuf; jj += 32) {
+                            const uint32_t e = lbuf[jj];
+                            const uint32_t cv = sub_count((uint64_t)cpx_qdiv(xp, (uint64_t)(e & 0x7FFFFFFFu)));
+                            if (e >> 31) {
+                                S += cv;
+                                msl += 1;
+                            } else {
+                                S -= cv;
+                                msl -= 1;
+                            }
+                        }
+                        __syncwarp();
+                        nbuf = 0;
+                    };
+                    // exclusive offset of this lane's n entries and the warp's total
+                    auto place = [&](uint32_t n, uint32_t &off) -> uint32_t {
+                        uint32_t inc = n;
+#pragma unroll
+                        for (int oo = 1; oo < 32; oo <<= 1) {
+                            const uint32_t t = __shfl_up_sync(FULL, inc, oo);
+                            if (lane >= (uint32_t)oo) inc += t;
+                        }
+                        off = inc - n;
+                        return __shfl_sync(FULL, inc, 31);
+                    };
                     if (prime_lvl) {
                         // m must be a prime q > p: walk the pi-table bitmap of (max(mlo, p), mhi]
                         if (mhi > qa) {
                             const uint64_t w0q = qa >> 7, w1q = ((uint64_t)mhi - 1) >> 7;
-                            for (uint64_t wq = w0q + lane; wq <= w1q; wq += 32) {
-                                const ulonglong2 e = __ldg(reinterpret_cast<const ulonglong2 *>(Tpi) + wq);
-                                uint64_t qb = e.x & range_mask(wq, qa, mhi);
+                            for (uint64_t wb = w0q; wb <= w1q; wb += 32) {
+                                const uint64_t wq = wb + lane;
+                                uint64_t qb = 0;
+                                if (wq <= w1q)
+                                    qb = __ldg(reinterpret_cast<const ulonglong2 *>(Tpi) + wq).x & range_mask(wq, qa, mhi);
+                                uint32_t off;
+                                const uint32_t tot_r = place((uint32_t)__popcll(qb), off);
+                                if (tot_r > kLeafBuf) {  // a dense round: each lane answers its own word
+                                    while (qb) {
+                                        const int j = __ffsll((long long)qb) - 1;
+                                        qb &= qb - 1;
+                                        S += sub_count((uint64_t)cpx_qdiv(xp, 128 * wq + 2 * j + 1));  // mu(q) = -1
+                                        msl += 1;
+                                    }
+                                    continue;
+                                }
+                                if (nbuf + tot_r > kLeafBuf) flush();
+                                uint32_t kk = nbuf + off;
                                 while (qb) {
                                     const int j = __ffsll((long long)qb) - 1;
                                     qb &= qb - 1;
-                                    const uint64_t m = 128 * wq + 2 * j + 1;
-                                    S += sub_count((uint64_t)cpx_qdiv(xp, m));  // mu(q) = -1
-                                    msl += 1;
+                                    lbuf[kk++] = (uint32_t)(128 * wq + 2 * j + 1) | 0x80000000u;
                                 }
+                                nbuf += tot_r;
                             }
                         }
                     } else {
                         // any squarefree m with lpf(m) > p: 16-byte loads of packed mu*lpf
                         const uint64_t i_lo = ((uint64_t)mlo + 1) >> 1, i_hi = ((uint64_t)mhi - 1) >> 1;
-                        for (uint64_t g = (i_lo >> 2) + lane; g <= (i_hi >> 2); g += 32) {
-                            uint32_t neg;
-                            uint32_t vm = valid_group(__ldg(reinterpret_cast<const int4 *>(MU) + g), g, i_lo, i_hi,
-                                                      p, &neg);
+                        for (uint64_t gb = i_lo >> 2; gb <= (i_hi >> 2); gb += 32) {
+                            const uint64_t g = gb + lane;
+                            uint32_t neg = 0, vm = 0;
+                            if (g <= (i_hi >> 2))
+                                vm = valid_group(__ldg(reinterpret_cast<const int4 *>(MU) + g), g, i_lo, i_hi, p, &neg);
+                            uint32_t off;
+                            const uint32_t tot_r = place((uint32_t)__popc(vm), off);
+                            if (nbuf + tot_r > kLeafBuf) flush();
+                            uint32_t kk = nbuf + off;
                             while (vm) {
                                 const int kq = __ffs(vm) - 1;
                                 vm &= vm - 1;
-                                const uint32_t cv = sub_count((uint64_t)cpx_qdiv(xp, 2 * (4 * g + kq) + 1));
-                                if ((neg >> kq) & 1u) {
-                                    S += cv;
-                                    msl += 1;
-                                } else {
-                                    S -= cv;
-                                    msl -= 1;
-                                }
+                                lbuf[kk++] = (uint32_t)(2 * (4 * g + kq) + 1) | (((neg >> kq) & 1u) << 31);
                             }
+                            nbuf += tot_r;
                         }
                     }
+                    flush();
                     ms_b = __reduce_add_sync(FULL, msl);
                 }
                 __syncwarp();
