@@ -558,6 +558,8 @@ __global__ void __launch_bounds__(kThreads) k_hard_leaves(const HardJob *__restr
     const uint64_t nw = ((uint64_t)gridDim.x * blockDim.x) >> 5;
     const size_t stride = snap_stride(lbits_sub);
     const size_t ncmax = (size_t(1) << lbits_sub) >> 7;
+    __shared__ uint32_t s_leaf[kThreads / 32][kLeafBuf];
+    uint32_t *lbuf = s_leaf[threadIdx.x >> 5];
     for (uint64_t unit = gw; unit < total; unit += nw) {
         uint32_t lo_j = 0, hi_j = n;  // unit0[lo_j] <= unit < unit0[hi_j]
         while (hi_j - lo_j > 1) {
@@ -586,44 +588,85 @@ __global__ void __launch_bounds__(kThreads) k_hard_leaves(const HardJob *__restr
         };
         int64_t S = 0;
         int32_t ms = 0;
+        // leaves gathered into the warp's buffer (m, bit 31: mu(m) = -1) and
+        // answered 32 at a time, as in k_hard
+        uint32_t nbuf = 0;
+        auto flush = [&] {
+            __syncwarp();
+            for (uint32_t jj = lane; jj < nbuf; jj += 32) {
+                const uint32_t e = lbuf[jj];
+                const uint32_t cv = count((uint64_t)cpx_qdiv(xp, (uint64_t)(e & 0x7FFFFFFFu)));
+                if (e >> 31) {
+                    S += cv;
+                    ms += 1;
+                } else {
+                    S -= cv;
+                    ms -= 1;
+                }
+            }
+            __syncwarp();
+            nbuf = 0;
+        };
+        auto place = [&](uint32_t cnt, uint32_t &off) -> uint32_t {
+            uint32_t inc = cnt;
+#pragma unroll
+            for (int oo = 1; oo < 32; oo <<= 1) {
+                const uint32_t t = __shfl_up_sync(FULL, inc, oo);
+                if (lane >= (uint32_t)oo) inc += t;
+            }
+            off = inc - cnt;
+            return __shfl_sync(FULL, inc, 31);
+        };
         if (J.kind == 1) {
             const uint64_t qa = J.mlo, mhi = J.mhi;
             const uint64_t w0 = (qa >> 7) + lu * kJobWords, wl = (mhi - 1) >> 7;
             for (uint64_t k = 0; k < kJobWords / 32; k++) {
+                if (w0 + 32 * k > wl) break;  // uniform
                 const uint64_t wq = w0 + 32 * k + lane;
-                if (wq > wl) break;
-                const ulonglong2 e = __ldg(reinterpret_cast<const ulonglong2 *>(Tpi) + wq);
-                uint64_t qb = e.x & range_mask(wq, qa, mhi);
+                uint64_t qb = 0;
+                if (wq <= wl) qb = __ldg(reinterpret_cast<const ulonglong2 *>(Tpi) + wq).x & range_mask(wq, qa, mhi);
+                uint32_t off;
+                const uint32_t tot_r = place((uint32_t)__popcll(qb), off);
+                if (tot_r > kLeafBuf) {  // a dense round: each lane answers its own word
+                    while (qb) {
+                        const int j = __ffsll((long long)qb) - 1;
+                        qb &= qb - 1;
+                        S += count((uint64_t)cpx_qdiv(xp, 128 * wq + 2 * j + 1));  // mu(q) = -1
+                        ms += 1;
+                    }
+                    continue;
+                }
+                if (nbuf + tot_r > kLeafBuf) flush();
+                uint32_t kk = nbuf + off;
                 while (qb) {
                     const int j = __ffsll((long long)qb) - 1;
                     qb &= qb - 1;
-                    S += count((uint64_t)cpx_qdiv(xp, 128 * wq + 2 * j + 1));  // mu(q) = -1
-                    ms += 1;
+                    lbuf[kk++] = (uint32_t)(128 * wq + 2 * j + 1) | 0x80000000u;
                 }
+                nbuf += tot_r;
             }
         } else {
             const uint64_t i_lo = (J.mlo + 1) >> 1, i_hi = (J.mhi - 1) >> 1;
             const uint64_t g0 = (i_lo >> 2) + lu * kJobGroups, gl = i_hi >> 2;
             const uint32_t p = J.p;
             for (uint64_t k = 0; k < kJobGroups / 32; k++) {
+                if (g0 + 32 * k > gl) break;  // uniform
                 const uint64_t g = g0 + 32 * k + lane;
-                if (g > gl) break;
-                uint32_t neg;
-                uint32_t vm = valid_group(__ldg(reinterpret_cast<const int4 *>(MU) + g), g, i_lo, i_hi, p, &neg);
+                uint32_t neg = 0, vm = 0;
+                if (g <= gl) vm = valid_group(__ldg(reinterpret_cast<const int4 *>(MU) + g), g, i_lo, i_hi, p, &neg);
+                uint32_t off;
+                const uint32_t tot_r = place((uint32_t)__popc(vm), off);
+                if (nbuf + tot_r > kLeafBuf) flush();
+                uint32_t kk = nbuf + off;
                 while (vm) {
                     const int kq = __ffs(vm) - 1;
                     vm &= vm - 1;
-                    const uint32_t cv = count((uint64_t)cpx_qdiv(xp, 2 * (4 * g + kq) + 1));
-                    if ((neg >> kq) & 1u) {
-                        S += cv;
-                        ms += 1;
-                    } else {
-                        S -= cv;
-                        ms -= 1;
-                    }
+                    lbuf[kk++] = (uint32_t)(2 * (4 * g + kq) + 1) | (((neg >> kq) & 1u) << 31);
                 }
+                nbuf += tot_r;
             }
         }
+        flush();
         const i128 Sw = cpx_warp_sum_i128((i128)S);
 #pragma unroll
         for (int dd = 16; dd > 0; dd >>= 1) ms += __shfl_down_sync(FULL, ms, dd);
