@@ -112,6 +112,11 @@ class Context:
     def set_hard_offload(self, min_candidates):
         self.call("cpx_set_hard_offload", min_candidates)
 
+    def set_hard_shared(self, mode):
+        """0: one hard-leaf sieve per query; 1: batches share a sieve
+        (default); 2: always share (single queries too)."""
+        self.call("cpx_set_hard_shared", mode)
+
     def autotune(self, decade_lo=9, decade_hi=17, seconds=0.0):
         """Tunes the plain path per decade of x (lone queries at 10^e and 10^(e+1/2))."""
         self.call("cpx_autotune", decade_lo, decade_hi, float(seconds))

@@ -77,6 +77,7 @@ class BatchStats(ctypes.Structure):
         ("segments", ctypes.c_uint64),
         ("hard_jobs", ctypes.c_uint64),
         ("offload_min", ctypes.c_uint64),
+        ("shared_groups", ctypes.c_uint64),
     ]
 
     def as_dict(self):
@@ -155,6 +156,7 @@ _SIGS = {
     "cpx_device_count": (ctypes.c_int, []),
     "cpx_set_hard_params": (ctypes.c_int, [P, u32, u32]),
     "cpx_set_hard_offload": (ctypes.c_int, [P, u32]),
+    "cpx_set_hard_shared": (ctypes.c_int, [P, u32]),
     "cpx_set_p2_window": (ctypes.c_int, [P, u64]),
     "cpx_S2_hard_layout": (ctypes.c_int, [P, U128, u64, u16, u32, pu64, pu32]),
     "cpx_S2_hard_part": (ctypes.c_int, [P, U128, u64, u16, u32, u64, u64, pU, ctypes.POINTER(HardLevel)]),

@@ -193,6 +193,14 @@ int cpx_set_hard_offload(cpx_ctx *ctx, uint32_t min_candidates)
     return guarded(ctx, [&] { ctx->hard_offload_min = min_candidates; });
 }
 
+int cpx_set_hard_shared(cpx_ctx *ctx, uint32_t mode)
+{
+    return guarded(ctx, [&] {
+        if (mode > 2) fail(CPX_EINVAL, "shared-sieve mode must be 0, 1 or 2");
+        ctx->hard_shared = mode;
+    });
+}
+
 int cpx_leaf_count(cpx_ctx *ctx, cpx_u128 x, uint64_t y, uint16_t c, cpx_leaf_counts *out)
 {
     return guarded(ctx, [&] {

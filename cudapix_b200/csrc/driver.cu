@@ -208,6 +208,31 @@ static void choose_lbits(cpx_ctx *ctx, std::vector<QD> &qd, uint32_t c, uint32_t
         if (nat[i]) qd[i].lbits = std::min(nat[i], cap);
 }
 
+// Segment size and group size of the batch-shared sieve (order: the queries
+// with hard leaves, z descending).  The segment is the smallest that covers
+// the largest z, at most the cap; the segment and then the groups (32
+// queries at most) shrink while the batch has fewer than four work units per
+// SM.
+static uint32_t choose_shared(cpx_ctx *ctx, const std::vector<QD> &qd, const std::vector<uint32_t> &order,
+                              uint32_t threads, uint32_t forced, uint32_t cap_all, uint32_t &gsize)
+{
+    const uint32_t minb = (threads >= 512) ? 16 : (threads >= 256 ? 15 : 14);
+    const uint32_t cap = std::max(minb, std::min<uint32_t>(forced ? forced : (cap_all ? cap_all : ctx->hard_log2_bits), 20));
+    uint32_t lb = minb;
+    while (lb < cap && (2ull << lb) < qd[order[0]].z + 1) lb++;
+    auto units = [&](uint32_t l, uint32_t G) {
+        uint64_t u = 0;
+        for (size_t k = 0; k < order.size(); k += G) u += (qd[order[k]].z + 1 + (2ull << l) - 1) / (2ull << l);
+        return u;
+    };
+    const uint64_t target = (uint64_t)ctx->sm_count * 4;
+    gsize = kGroupMax;
+    if (!forced)
+        while (lb > minb && units(lb, gsize) < target) lb--;
+    while (gsize > 1 && units(lb, gsize) < target) gsize /= 2;
+    return lb;
+}
+
 // Captures the launches of one batch into a CUDA graph and runs it.  The
 // executable graph is kept in the context: a later batch with the same kernel
 // sequence only updates its nodes' parameters (grids, pointers) in place, a
@@ -458,10 +483,29 @@ void run_batch(cpx_ctx *ctx, const BatchReq &rq)
     const std::vector<uint32_t> &hP = host_primes(ctx);
     st.tables_ms = ms_since(clk);
 
+    // hard leaves: one sieve per query, or (batches) one shared by groups of queries
+    std::vector<uint32_t> horder;  // queries with hard leaves, z descending
+    bool shared = false;
+    uint32_t gsize = 0, sh_lbits = 0;
     if (mask & TERM_HARD) {
-        for (QD &d : qd)
-            if (!d.direct) d.nb = (uint32_t)host_pi(hP, d.r4);
-        choose_lbits(ctx, qd, c, threads, rq.lbits, lbits_cap, tune);
+        for (uint32_t i = 0; i < Q; i++) {
+            QD &d = qd[i];
+            if (d.direct) continue;
+            d.nb = (uint32_t)host_pi(hP, d.r4);
+            if (d.nb > c) horder.push_back(i);
+        }
+        const uint32_t mode = ctx->hard_shared;
+        shared = !rq.seg_hi && !rq.hard_levels && !horder.empty() &&
+                 (mode == 2 || (mode == 1 && !small && horder.size() >= 8));
+        if (shared) {
+            std::sort(horder.begin(), horder.end(), [&](uint32_t a, uint32_t b) {
+                return qd[a].z != qd[b].z ? qd[a].z > qd[b].z : a < b;
+            });
+            sh_lbits = choose_shared(ctx, qd, horder, threads, rq.lbits, lbits_cap, gsize);
+            for (uint32_t i : horder) qd[i].lbits = sh_lbits;
+        } else {
+            choose_lbits(ctx, qd, c, threads, rq.lbits, lbits_cap, tune);
+        }
     }
 
     // ---- units per kernel family (queries planned in parallel blocks)
@@ -512,7 +556,10 @@ void run_batch(cpx_ctx *ctx, const BatchReq &rq)
                         elv.push_back(r);
                     }
                 }
-                if ((mask & TERM_HARD) && d.nb > c) {
+                if ((mask & TERM_HARD) && d.nb > c && shared) {
+                    const uint64_t span = 2ull << d.lbits;
+                    d.nseg = (d.z + 1 + span - 1) / span;
+                } else if ((mask & TERM_HARD) && d.nb > c) {
                     const uint64_t span = 2ull << d.lbits;
                     d.nseg = (d.z + 1 + span - 1) / span;
                     if (rq.seg_hi) {  // one part of a query split over GPUs
@@ -560,6 +607,50 @@ void run_batch(cpx_ctx *ctx, const BatchReq &rq)
     }
     if (!lbits_max) lbits_max = 15;
 
+    // ---- the batch-shared sieve: groups, and the carry rows of its counting
+    // sweep (row b: the sub-segments of the segments that sieve level b)
+    std::vector<HardGroup> groups;
+    std::vector<uint64_t> pre_grp(1, 0), lvl_off;
+    uint64_t sh_nseg = 0, sh_r4max = 0;
+    u128 sh_xmax = 0;
+    uint32_t sh_nlv = 0;
+    if (shared) {
+        const uint64_t span = 2ull << sh_lbits;
+        const uint64_t NW = threads / 32;
+        for (size_t k = 0; k < horder.size(); k += gsize) {
+            HardGroup hg;
+            memset(&hg, 0, sizeof hg);
+            hg.n = (uint32_t)std::min<size_t>(gsize, horder.size() - k);
+            for (uint32_t t = 0; t < hg.n; t++) {
+                const QD &d = qd[horder[k + t]];
+                hg.q[t] = horder[k + t];
+                hg.xmax = std::max(hg.xmax, d.x);
+                hg.r4max = std::max(hg.r4max, d.r4);
+                hg.nseg = std::max(hg.nseg, d.nseg);
+            }
+            groups.push_back(hg);
+            pre_grp.push_back(pre_grp.back() + hg.nseg);
+            sh_nseg = std::max(sh_nseg, hg.nseg);
+            sh_xmax = std::max(sh_xmax, hg.xmax);
+            sh_r4max = std::max(sh_r4max, hg.r4max);
+        }
+        const uint64_t nbm = host_pi(hP, sh_r4max);
+        sh_nlv = nbm > c ? (uint32_t)(nbm - c) : 0;
+        lvl_off.assign(sh_nlv + 1, 0);
+        double ent = 0.0;  // segment-levels sieved: the sweep, then every unit
+        for (uint32_t lv = 0; lv < sh_nlv; lv++) {
+            const uint64_t n = segments_at_level(sh_xmax, span, hP[c + lv], 0, sh_nseg);
+            lvl_off[lv + 1] = lvl_off[lv] + NW * n;
+            ent += (double)n;
+        }
+        for (const HardGroup &hg : groups) {
+            const uint64_t nbg = host_pi(hP, hg.r4max);
+            for (uint64_t b = c + 1; b <= nbg; b++) ent += (double)segments_at_level(hg.xmax, span, hP[b - 1], 0, hg.nseg);
+        }
+        hard_bytes = ent * (double)(1ull << sh_lbits) / 8.0;
+        lbits_max = sh_lbits;
+    }
+
     // ---- device buffers
     Plan pl;
     pl.Q = Q;
@@ -576,14 +667,16 @@ void run_batch(cpx_ctx *ctx, const BatchReq &rq)
     pl.hard_entries = hard_entries;
     const size_t qd_bytes = sizeof(QD) * Q, pre_bytes = (pre.size() * 8 + 15) & ~size_t(15);
     const size_t elv_bytes = elv.size() * sizeof(EasyLvl);
+    const size_t grp_bytes = groups.size() * sizeof(HardGroup);
+    const size_t pg_bytes = (pre_grp.size() * 8 + 15) & ~size_t(15), lo_bytes = (lvl_off.size() * 8 + 15) & ~size_t(15);
+    const size_t stage_bytes = qd_bytes + pre_bytes + elv_bytes + grp_bytes + pg_bytes + lo_bytes;
     const size_t acc_words = (size_t)Q * kAccStride;
-    unsigned char *dbuf =
-        (unsigned char *)ctx->b_work[0].get(qd_bytes + pre_bytes + elv_bytes + acc_words * 8 + 64);
+    unsigned char *dbuf = (unsigned char *)ctx->b_work[0].get(stage_bytes + acc_words * 8 + 64);
     QD *d_qd = reinterpret_cast<QD *>(dbuf);
     uint64_t *d_pre = reinterpret_cast<uint64_t *>(dbuf + qd_bytes);
     EasyLvl *d_elv = reinterpret_cast<EasyLvl *>(dbuf + qd_bytes + pre_bytes);
-    unsigned long long *d_acc =
-        reinterpret_cast<unsigned long long *>(dbuf + qd_bytes + pre_bytes + elv_bytes);
+    unsigned char *d_sh = dbuf + qd_bytes + pre_bytes + elv_bytes;  // groups, unit offsets, row offsets
+    unsigned long long *d_acc = reinterpret_cast<unsigned long long *>(dbuf + stage_bytes);
     pl.elv = d_elv;
     pl.n_elv = (uint32_t)elv.size();
     pl.n_ecomp = n_ecomp;
@@ -596,11 +689,28 @@ void run_batch(cpx_ctx *ctx, const BatchReq &rq)
     pl.pre_comb = d_pre + 5 * (Q + 1);
     pl.acc = d_acc;
     pl.ticket = ctx->b_work[1].as<unsigned int>(4);
-    if (pl.n_seg) {
-        pl.seg_B = ctx->b_work[2].as<uint32_t>(pl.n_seg + 1);
-        pl.seg_off = ctx->b_work[3].as<uint64_t>(pl.n_seg + 1);
-        pl.hard_cnt = ctx->b_work[4].as<uint32_t>(hard_entries + 1);
-        pl.hard_ms = ctx->b_work[5].as<int32_t>(hard_entries + 1);
+    if (shared) {
+        pl.shared = true;
+        pl.sh_lbits = sh_lbits;
+        pl.sh_nlv = sh_nlv;
+        pl.n_grp = (uint32_t)groups.size();
+        pl.sh_nseg = sh_nseg;
+        pl.sh_r4max = sh_r4max;
+        pl.sh_xmax = sh_xmax;
+        pl.n_gunits = pre_grp.back();
+        pl.n_carry = lvl_off.back();
+        pl.grp = reinterpret_cast<const HardGroup *>(d_sh);
+        pl.pre_grp = reinterpret_cast<const uint64_t *>(d_sh + grp_bytes);
+        pl.lvl_off = reinterpret_cast<const uint64_t *>(d_sh + grp_bytes + pg_bytes);
+        pl.carry = ctx->b_work[4].as<uint64_t>(pl.n_carry + 1);
+    }
+    if (pl.n_seg || pl.n_gunits) {
+        if (!shared) {
+            pl.seg_B = ctx->b_work[2].as<uint32_t>(pl.n_seg + 1);
+            pl.seg_off = ctx->b_work[3].as<uint64_t>(pl.n_seg + 1);
+            pl.hard_cnt = ctx->b_work[4].as<uint32_t>(hard_entries + 1);
+            pl.hard_ms = ctx->b_work[5].as<int32_t>(hard_entries + 1);
+        }
         // snapshot pool for the heavy (sub-segment, level) leaf sets, counted on
         // the host; the threshold doubles until the pool fits the budget
         const size_t stride = hard_snapshot_stride(lbits_max - (uint32_t)(__builtin_ctz(threads) - 5));
@@ -626,6 +736,7 @@ void run_batch(cpx_ctx *ctx, const BatchReq &rq)
         pl.jobs = ctx->b_jobs.as<HardJob>(pl.max_jobs + 1);
         uint64_t *ctl = ctx->b_jobctl.as<uint64_t>(pl.max_jobs + 4);
         pl.njobs = reinterpret_cast<unsigned int *>(ctl);
+        pl.nsnap = reinterpret_cast<unsigned int *>(ctl + 1);
         pl.job_units = ctl + 2;
         pl.snap = static_cast<unsigned char *>(ctx->b_snap.get((pl.max_jobs + 1) * stride));
     }
@@ -640,18 +751,28 @@ void run_batch(cpx_ctx *ctx, const BatchReq &rq)
     // allocation between kernels, so the sequence can be captured in a graph)
     scan_reserve(ctx, std::max<uint64_t>(std::max<uint64_t>(pl.n_seg, pl.n_easy + 1), (uint64_t)pl.max_jobs + 1));
     pl.time_hard = ctx->timing && !rq.graph;
-    if (mask & TERM_HARD) prepare_hard(ctx, pl);
+    if (mask & TERM_HARD) {
+        if (shared) prepare_hard_shared(ctx, pl);
+        else prepare_hard(ctx, pl);
+    }
     u128 *d_out = ctx->b_work[6].as<u128>(Q);
 
     st.plan_ms = ms_since(clk);
-    st.segments = pl.n_seg;
+    st.segments = shared ? pl.n_gunits : pl.n_seg;
+    st.shared_groups = groups.size();
     st.hard_jobs = pl.max_jobs;
     st.offload_min = pl.offload_min;
     // one staging copy host -> device
-    std::vector<unsigned char> stage(qd_bytes + pre_bytes + elv_bytes);
+    std::vector<unsigned char> stage(stage_bytes);
     memcpy(stage.data(), qd.data(), qd_bytes);
     memcpy(stage.data() + qd_bytes, pre.data(), pre.size() * 8);
     if (elv_bytes) memcpy(stage.data() + qd_bytes + pre_bytes, elv.data(), elv_bytes);
+    if (shared) {
+        unsigned char *h_sh = stage.data() + qd_bytes + pre_bytes + elv_bytes;
+        memcpy(h_sh, groups.data(), grp_bytes);
+        memcpy(h_sh + grp_bytes, pre_grp.data(), pre_grp.size() * 8);
+        memcpy(h_sh + grp_bytes + pg_bytes, lvl_off.data(), lvl_off.size() * 8);
+    }
     CPX_CUDA(cudaMemcpyAsync(dbuf, stage.data(), stage.size(), cudaMemcpyHostToDevice, ctx->stream));
     CPX_CUDA(cudaMemsetAsync(d_acc, 0, acc_words * 8, ctx->stream));
 
@@ -664,7 +785,10 @@ void run_batch(cpx_ctx *ctx, const BatchReq &rq)
             launch_easy(ctx, pl);
             launch_easy_comp(ctx, pl);
         }
-        if (mask & TERM_HARD) launch_hard(ctx, pl);
+        if (mask & TERM_HARD) {
+            if (pl.shared) launch_hard_shared(ctx, pl);
+            else launch_hard(ctx, pl);
+        }
         if (!any_p2win) launch_finalize(ctx, pl, d_out, mask == TERM_PI);
     };
     if (ctx->timing) CPX_CUDA(cudaEventRecord(ctx->ev_b0, ctx->stream));
@@ -707,7 +831,7 @@ void run_batch(cpx_ctx *ctx, const BatchReq &rq)
         CPX_CUDA(cudaMemcpy(rq.hard_levels, pl.hard_levels, n_levels * sizeof(HardLevel), cudaMemcpyDeviceToHost));
     }
     if (ctx->timing) CPX_CUDA(cudaEventElapsedTime(&ctx->last_batch_ms, ctx->ev_b0, ctx->ev_b1));
-    if (pl.time_hard && pl.n_seg) {
+    if (pl.time_hard && (pl.n_seg || pl.n_gunits)) {
         float ms = 0.f;
         CPX_CUDA(cudaEventElapsedTime(&ms, ctx->ev_hard0, ctx->ev_hard1));
         ctx->last_hard_ms = ms;

@@ -23,198 +23,14 @@
 // the per-segment (count, Sum(-mu)) pairs go to k_hard_combine, which adds the
 // carries between segments.
 //
-// Bitmap layout: thread t owns chunks [CPT t, CPT (t+1)); chunk c is stored at
-// c ^ ((c >> log2 CPT) & 7) so the owners' 128-bit accesses are free of bank
-// conflicts.  Counters are indexed by the unswizzled chunk.
+// This is the sieve of lone queries and small batches.  Larger batches share
+// the sieve between queries (hard_shared.cu); k_hard_leaves serves both.
 #include <algorithm>
 #include <mutex>
 
-#include "kern_common.cuh"
+#include "sieve.cuh"
 
 namespace cpx {
-
-__device__ __forceinline__ uint32_t swz(uint32_t c, int s) { return s ? (c ^ ((c >> s) & 7u)) : c; }
-
-// bits k < 32 of a word whose first number is = r (mod p) that are multiples of p
-__device__ __forceinline__ uint32_t mult_mask(uint32_t r, uint32_t p, uint32_t Mp)
-{
-    const uint32_t k0 = (r == 0) ? 0u : ((r & 1u) ? (p - r) >> 1 : p - (r >> 1));
-    return k0 < 32 ? (Mp << k0) : 0u;
-}
-__device__ __forceinline__ uint32_t every_pth_bit(uint32_t p)
-{
-    uint32_t m = 0;
-    for (uint32_t k = 0; k < 32; k += p) m |= 1u << k;
-    return m;
-}
-
-// sum of the n 8-bit counters starting at c8 (c8 4-byte aligned when n >= 4)
-__device__ __forceinline__ uint32_t counter_sum(const uint8_t *c8, uint32_t n)
-{
-    uint32_t s = 0;
-    const uint32_t *cw = reinterpret_cast<const uint32_t *>(c8);
-    uint32_t k = 0;
-    for (; k < (n >> 2); k++) s = __dp4a(cw[k], 0x01010101u, s);
-    const uint32_t rem = n & 3;
-    if (rem) {
-        if (reinterpret_cast<uintptr_t>(c8) & 3) {
-            for (uint32_t i = 0; i < rem; i++) s += c8[4 * k + i];
-        } else {
-            s = __dp4a(cw[k] & ((1u << (8 * rem)) - 1u), 0x01010101u, s);
-        }
-    }
-    return s;
-}
-
-// A level whose candidate range in a warp's sub-segment holds at least
-// offload_min odd m (8 per pi-table entry for prime-only levels) is answered
-// by k_hard_leaves (cpx_set_hard_offload; 0 keeps every leaf in the sieve).
-constexpr uint64_t kJobWords = 256;   // pi-table entries per k_hard_leaves unit (prime levels)
-constexpr uint64_t kJobGroups = 256;  // 4-m groups per k_hard_leaves unit (other levels)
-
-// bytes of one snapshot slot of a sub-segment of 2^lbits_sub numbers:
-// 16-byte bitmap chunks + 32-bit survivor prefixes
-__host__ __device__ __forceinline__ size_t snap_stride(uint32_t lbits_sub)
-{
-    const size_t nc = (size_t(1) << lbits_sub) >> 7;
-    return (nc * 20 + 255) & ~size_t(255);
-}
-
-// leaves a warp gathers before answering them 32 at a time
-constexpr uint32_t kLeafBuf = 256;
-
-struct LvlOut {
-    uint32_t cnt;
-    int32_t ms;
-    uint32_t job;
-    uint32_t pad;
-};
-
-__host__ __device__ __forceinline__ size_t hard_smem(uint32_t lbits, uint32_t threads)
-{
-    const size_t L = size_t(1) << lbits;
-    size_t o = L / 8;                                 // bitmap
-    o += ((L / 128) + 15) & ~size_t(15);              // chunk counters
-    o += threads * 4;                                 // lane prefixes
-    o += 2 * (threads / 32) * 32 * sizeof(LvlOut);    // per-warp level outputs, double buffered
-    o = (o + 15) & ~size_t(15);
-    o += 32 * sizeof(i128);                           // reductions
-    o += (threads / 32) * kLeafBuf * 4;               // per-warp gathered leaves
-    return o;
-}
-
-// Pre-sieve of one lane's chunks [c0, c0 + CPT) of the segment starting at lo
-// with p_2 .. p_c (residue masks per 32-bit word); writes the bitmap and the
-// chunk counters and returns the lane's survivors.  Runs once per segment, so
-// it is kept out of line (instruction-cache footprint of the level loop).
-__device__ __noinline__ uint32_t presieve(uint32_t *bm, uint8_t *cnt8, const uint32_t *__restrict__ P, uint32_t c,
-                                          uint64_t lo, uint32_t c0, uint32_t CPT, int s)
-{
-    uint32_t pr[8], rr[8], st[8], Mp[8];
-    const uint32_t np = c - 1;
-    const uint32_t w0 = 4 * c0;
-#pragma unroll
-    for (uint32_t i = 0; i < 8; i++) {
-        if (i < np) {
-            pr[i] = P[i + 1];
-            rr[i] = (uint32_t)(((lo + 1) % pr[i] + (64ull * w0) % pr[i]) % pr[i]);
-            st[i] = 64u % pr[i];
-            Mp[i] = every_pth_bit(pr[i]);
-        }
-    }
-    uint32_t cnt0 = 0;
-    for (uint32_t j = 0; j < CPT; j++) {
-        uint32_t wv[4];
-#pragma unroll
-        for (int k = 0; k < 4; k++) {
-            uint32_t m = 0;
-#pragma unroll
-            for (uint32_t i = 0; i < 8; i++) {
-                if (i < np) {
-                    m |= mult_mask(rr[i], pr[i], Mp[i]);
-                    rr[i] += st[i];
-                    if (rr[i] >= pr[i]) rr[i] -= pr[i];
-                }
-            }
-            wv[k] = ~m;
-        }
-        const uint32_t cc = __popc(wv[0]) + __popc(wv[1]) + __popc(wv[2]) + __popc(wv[3]);
-        cnt0 += cc;
-        cnt8[c0 + j] = (uint8_t)cc;
-        reinterpret_cast<uint4 *>(bm)[swz(c0 + j, s)] = make_uint4(wv[0], wv[1], wv[2], wv[3]);
-    }
-    return cnt0;
-}
-
-// Writes one lane's share of a leaf-set snapshot: its chunks of the
-// sub-segment bitmap and the survivor prefix of each chunk (pre = survivors of
-// the sub-segment before the lane's first chunk).  Out of line: rare path.
-__device__ __noinline__ void snapshot_chunks(uint4 *sb, uint32_t *spre, const uint32_t *bm, const uint8_t *cnt8,
-                                             uint32_t cw0, uint32_t c0, uint32_t CPT, int s, uint32_t pre)
-{
-    for (uint32_t jj = 0; jj < CPT; jj++) {
-        sb[cw0 + jj] = reinterpret_cast<const uint4 *>(bm)[swz(c0 + jj, s)];
-        spre[cw0 + jj] = pre;
-        pre += cnt8[c0 + jj];
-    }
-}
-
-// The valid m of one 16-byte group of packed mu*lpf (4 odd m, indices 4g..4g+3
-// within [i_lo, i_hi]): squarefree with lpf > p.  Bit k of *neg: mu(m) = -1.
-__device__ __forceinline__ uint32_t valid_group(int4 v4, uint64_t g, uint64_t i_lo, uint64_t i_hi, uint32_t p,
-                                                uint32_t *neg)
-{
-    const int32_t vals[4] = {v4.x, v4.y, v4.z, v4.w};
-    uint32_t vm = 0, ng = 0;
-#pragma unroll
-    for (int k = 0; k < 4; k++) {
-        const uint64_t i = 4 * g + k;
-        const int32_t v = vals[k];
-        const uint32_t av = (uint32_t)(v > 0 ? v : -v);
-        if (i >= i_lo && i <= i_hi && v != 0 && av > p) {
-            vm |= 1u << k;
-            if (v < 0) ng |= 1u << k;
-        }
-    }
-    *neg = ng;
-    return vm;
-}
-
-// Parameters of one level (p = p_b) for one warp's sub-segment [lo_w, hi_w):
-// xp = x/p, the candidate range (mlo, mhi] of m (m > y/p, u = xp/m in the
-// sub-segment, m <= x/p^3 for a hard leaf), the residue of lo_w + 1 mod p and
-// the bit of the first odd multiple of p (0xFFFFFFFF: none).  Computed for 32
-// levels at a time, one per lane; out of line to keep the level loop small.
-template <class XT> struct LvlPar {
-    XT xp;
-    uint32_t p, mlo, mhi, r0, i0;
-};
-
-template <class XT>
-__device__ __noinline__ void level_params(LvlPar<XT> &o, XT x, uint64_t y, uint64_t p, uint64_t lo_w, uint64_t hi_w)
-{
-    const XT xp = cpx_qdiv(x, p);
-    uint64_t mlo = y / p;
-    const XT t1 = cpx_qdiv(xp, hi_w);
-    if (t1 > (XT)mlo) mlo = (uint64_t)t1;
-    uint64_t mhi = y;
-    if (lo_w) {
-        const XT t2 = cpx_qdiv(xp, lo_w);
-        if (t2 < (XT)mhi) mhi = (uint64_t)t2;
-    }
-    const XT t3 = cpx_qdiv(xp, p * p);  // hard leaves only: m <= x/p^3
-    if (t3 < (XT)mhi) mhi = (uint64_t)t3;
-    if (mhi < mlo) mhi = mlo;
-    o.p = (uint32_t)p;
-    o.xp = xp;
-    o.mlo = (uint32_t)mlo;
-    o.mhi = (uint32_t)mhi;
-    const uint64_t r0 = (lo_w + 1) - cpx_udiv_leaf(lo_w + 1, p) * p;
-    o.r0 = (uint32_t)r0;
-    uint64_t m = lo_w + 1 + (r0 ? p - r0 : 0);
-    if ((m & 1) == 0) m += p;
-    o.i0 = (m < hi_w) ? (uint32_t)((m - lo_w - 1) >> 1) : 0xFFFFFFFFu;
-}
 
 template <class XT>
 __global__ void __launch_bounds__(512, 2) k_hard(const QD *__restrict__ qd, uint32_t Q,
@@ -276,22 +92,7 @@ __global__ void __launch_bounds__(512, 2) k_hard(const QD *__restrict__ qd, uint
     uint32_t tot = __reduce_add_sync(FULL, cnt0);  // survivors of this warp's sub-segment
     __syncwarp();
 
-    // survivors of the warp's sub-segment with n <= uu (uu in [lo_w, hi_w))
-    auto sub_count = [&](uint64_t uu) -> uint32_t {
-        const uint32_t kk = (uint32_t)((uu - lo_w + 1) >> 1);  // bits [0, kk) of the sub-segment
-        if (!kk) return 0u;
-        const uint32_t jb = kk - 1, w = jb >> 5;
-        const uint32_t chs = w >> 2, ow = chs >> s;      // chunk in the sub-segment, owning lane
-        const uint32_t ch = chs + CPT * 32 * warp;       // chunk in the segment
-        uint32_t cv = wl[ow] + counter_sum(cnt8 + ch - (chs - ow * CPT), chs - ow * CPT);
-        const uint4 v4 = reinterpret_cast<const uint4 *>(bm)[swz(ch, s)];
-        const uint32_t wi = w & 3, msk = (2u << (jb & 31)) - 1u;
-        if (wi == 0) cv += __popc(v4.x & msk);
-        else if (wi == 1) cv += __popc(v4.x) + __popc(v4.y & msk);
-        else if (wi == 2) cv += __popc(v4.x) + __popc(v4.y) + __popc(v4.z & msk);
-        else cv += __popc(v4.x) + __popc(v4.y) + __popc(v4.z) + __popc(v4.w & msk);
-        return cv;
-    };
+    auto sub_count = [&](uint64_t uu) -> uint32_t { return sub_survivors(uu, lo_w, wl, cnt8, bm, CPT, s, warp); };
 
     int64_t S = 0;       // this lane's share of the hard sum (survivor counts within sub-segments)
     i128 Sx = 0;         // warp 0: carries between the CTA's sub-segments
@@ -366,6 +167,7 @@ __global__ void __launch_bounds__(512, 2) k_hard(const QD *__restrict__ qd, uint
                                                     ((((uint64_t)mlo + 1) >> 1) >> 2) + kJobGroups) /
                                                        kJobGroups;
                             J.carry = 0;  // filled in by the group combine below
+                            J.snap = j;
                             job_units[j] = J.nunits;
                             J.xp = (u128)xp;
                             jobs[j] = J;
@@ -394,17 +196,7 @@ __global__ void __launch_bounds__(512, 2) k_hard(const QD *__restrict__ qd, uint
                         __syncwarp();
                         nbuf = 0;
                     };
-                    // exclusive offset of this lane's n entries and the warp's total
-                    auto place = [&](uint32_t n, uint32_t &off) -> uint32_t {
-                        uint32_t inc = n;
-#pragma unroll
-                        for (int oo = 1; oo < 32; oo <<= 1) {
-                            const uint32_t t = __shfl_up_sync(FULL, inc, oo);
-                            if (lane >= (uint32_t)oo) inc += t;
-                        }
-                        off = inc - n;
-                        return __shfl_sync(FULL, inc, 31);
-                    };
+                    auto place = [&](uint32_t n, uint32_t &off) -> uint32_t { return warp_place(n, lane, off); };
                     if (prime_lvl) {
                         // m must be a prime q > p: walk the pi-table bitmap of (max(mlo, p), mhi]
                         if (mhi > qa) {
@@ -461,50 +253,8 @@ __global__ void __launch_bounds__(512, 2) k_hard(const QD *__restrict__ qd, uint
                 __syncwarp();
             }
             // ---- cross off p_b in the sub-segment
-            uint32_t cleared = 0;
-            if (p < 128) {
-                // each lane masks its own words; p < 32 has several multiples per word
-                const uint32_t Mp = every_pth_bit(p);
-                const uint32_t stp = 64u % p;
-                const uint32_t r0 = __shfl_sync(FULL, lr0, k);
-                uint32_t r = (r0 + (64u * (cw0 * 4)) % p) % p;  // first owned word of the sub-segment
-                for (uint32_t j = 0; j < CPT; j++) {
-                    uint4 v = reinterpret_cast<const uint4 *>(bm)[swz(c0 + j, s)];
-                    uint32_t a4[4] = {v.x, v.y, v.z, v.w};
-                    uint32_t cj = 0;
-#pragma unroll
-                    for (int kk = 0; kk < 4; kk++) {
-                        const uint32_t mk = mult_mask(r, p, Mp);
-                        cj += __popc(a4[kk] & mk);
-                        a4[kk] &= ~mk;
-                        r += stp;
-                        if (r >= p) r -= p;
-                    }
-                    if (cj) {
-                        cnt8[c0 + j] = (uint8_t)(cnt8[c0 + j] - cj);
-                        reinterpret_cast<uint4 *>(bm)[swz(c0 + j, s)] = make_uint4(a4[0], a4[1], a4[2], a4[3]);
-                    }
-                    cleared += cj;
-                }
-            } else {
-                // p >= 128: the lanes of one step clear bits p apart, so they touch
-                // distinct words and distinct chunk counters (plain read-modify-write)
-                const uint32_t i0 = __shfl_sync(FULL, li0, k);
-                if (i0 != 0xFFFFFFFFu) {
-                    const uint32_t base_ch = CPT * 32 * warp;
-                    for (uint64_t i = (uint64_t)i0 + (uint64_t)lane * p; i < Lw; i += 32ull * p) {
-                        const uint32_t w = (uint32_t)(i >> 5), bit = 1u << (i & 31);
-                        const uint32_t ch = base_ch + (w >> 2);
-                        uint32_t *pw = bm + ((swz(ch, s) << 2) | (w & 3));
-                        const uint32_t old = *pw;
-                        if (old & bit) {
-                            *pw = old & ~bit;
-                            cleared++;
-                            cnt8[ch] = (uint8_t)(cnt8[ch] - 1);
-                        }
-                    }
-                }
-            }
+            const uint32_t cleared = cross_off(bm, cnt8, p, __shfl_sync(FULL, lr0, k), __shfl_sync(FULL, li0, k), c0, cw0,
+                                               CPT, s, CPT * 32 * warp, lane, Lw);
             tot -= __reduce_add_sync(FULL, cleared);
             __syncwarp();
             if (lane == k) {
@@ -539,8 +289,9 @@ __global__ void __launch_bounds__(512, 2) k_hard(const QD *__restrict__ qd, uint
 // Leaves of the offloaded (segment, level) sets.  A warp takes one unit: 256
 // pi-table entries of prime m (prime-only levels) or 256 groups of 4 odd m
 // read as packed mu*lpf (other levels).  Each leaf's survivor count is the
-// snapshot's chunk prefix plus popcounts inside the 16-byte chunk; the sums go
-// to the query's hard-leaf accumulator and Sum(-mu) to the level's slot.
+// job's carry plus the snapshot's chunk prefix plus popcounts inside the
+// 16-byte chunk; the sums go to the query's hard-leaf accumulator and
+// Sum(-mu) to the level's slot (none when slot = ~0: the carry was complete).
 template <class XT>
 __global__ void __launch_bounds__(kThreads) k_hard_leaves(const HardJob *__restrict__ jobs,
                                                           const unsigned int *njobs, uint32_t max_jobs,
@@ -569,15 +320,16 @@ __global__ void __launch_bounds__(kThreads) k_hard_leaves(const HardJob *__restr
         }
         const HardJob &J = jobs[lo_j];
         const uint64_t lu = unit - __ldg(unit0 + lo_j);
-        const uint4 *sb = reinterpret_cast<const uint4 *>(snap + (size_t)lo_j * stride);
+        const uint4 *sb = reinterpret_cast<const uint4 *>(snap + (size_t)J.snap * stride);
         const uint32_t *spre = reinterpret_cast<const uint32_t *>(sb + ncmax);
         const XT xp = (XT)J.xp;
         const uint64_t lo = J.lo;
+        // survivors of the sub-segment with n <= uu (the carry is added per unit)
         auto count = [&](uint64_t uu) -> uint32_t {
             const uint32_t kk = (uint32_t)((uu - lo + 1) >> 1);
-            if (!kk) return (uint32_t)J.carry;  // u = lo: no number of the sub-segment is <= u
+            if (!kk) return 0u;  // u = lo: no number of the sub-segment is <= u
             const uint32_t jb = kk - 1, w = jb >> 5, ch = w >> 2;
-            uint32_t cv = (uint32_t)J.carry + __ldg(spre + ch);
+            uint32_t cv = __ldg(spre + ch);
             const uint4 v4 = __ldg(sb + ch);
             const uint32_t wi = w & 3, msk = (2u << (jb & 31)) - 1u;
             if (wi == 0) cv += __popc(v4.x & msk);
@@ -671,18 +423,13 @@ __global__ void __launch_bounds__(kThreads) k_hard_leaves(const HardJob *__restr
 #pragma unroll
         for (int dd = 16; dd > 0; dd >>= 1) ms += __shfl_down_sync(FULL, ms, dd);
         if (lane == 0) {
-            if (ms) atomicAdd(out_ms + J.slot, ms);
-            acc_add(acc, J.q, ACC_HARD, Sw);
+            if (ms && J.slot != ~0ull) atomicAdd(out_ms + J.slot, ms);
+            acc_add(acc, J.q, ACC_HARD, Sw + (i128)J.carry * ms);
         }
     }
 }
 
-// B(seg) = pi(min(r4, isqrt((x - 1) / lo), isqrt(hi - 1))): the levels b a
-// segment sieves.  p_b^2 * lo < x bounds the levels whose leaves can reach
-// the segment or a later one; p_b^2 < hi skips the levels whose leaves all lie
-// above the segment, because below p_b^2 the carry phi(v, b - 1) is
-// 1 + pi(v) - (b - 1) and k_hard_combine reads it from the pi table.
-// Levels per segment = max(0, B - c).
+// B(seg) of every work unit (seg_levels) and its level count max(0, B - c).
 template <class XT>
 __global__ void k_hard_plan(const QD *__restrict__ qd, uint32_t Q, const uint64_t *__restrict__ pre_seg,
                             uint64_t total, const uint32_t *__restrict__ P, uint32_t np,
@@ -694,20 +441,7 @@ __global__ void k_hard_plan(const QD *__restrict__ qd, uint32_t Q, const uint64_
     const QD &d = qd[q];
     const uint64_t seg = u - pre_seg[q] + d.seg0;
     const uint64_t lo = seg * 2 * (1ull << d.lbits), hi = lo + 2 * (1ull << d.lbits);
-    const XT x = xload<XT>(d);
-    uint64_t v = d.r4;
-    if (lo) {
-        const uint64_t v1 = cpx_isqrt((u128)((x - 1) / (XT)lo));
-        if (v1 < v) v = v1;
-    }
-    const uint64_t v2 = cpx_isqrt((u128)(hi - 1));
-    if (v2 < v) v = v2;
-    uint32_t a = 0, bnd = np;  // count of P[i] <= v
-    while (a < bnd) {
-        const uint32_t mid = (a + bnd) >> 1;
-        if (P[mid] <= v) a = mid + 1;
-        else bnd = mid;
-    }
+    const uint32_t a = seg_levels<XT>(xload<XT>(d), d.r4, lo, hi, P, np);
     seg_B[u] = a;
     seg_lv[u] = a > d.c ? a - d.c : 0;
 }
@@ -800,6 +534,20 @@ size_t hard_smem_bytes(uint32_t lbits, uint32_t threads, bool wide)
     return hard_smem(lbits, threads);
 }
 
+void launch_hard_leaves(cpx_ctx *ctx, const Plan &pl, uint32_t lbits_sub)
+{
+    const Tables &tb = ctx->tab;
+    scan_u64(ctx, pl.job_units, pl.max_jobs + 1);
+    if (pl.wide)
+        k_hard_leaves<u128><<<(unsigned)ctx->sm_count * 8, kThreads, 0, ctx->stream>>>(
+            pl.jobs, pl.njobs, pl.max_jobs, pl.job_units, pl.snap, lbits_sub, tb.MU, tb.T, pl.hard_ms, pl.acc);
+    else
+        k_hard_leaves<uint64_t><<<(unsigned)ctx->sm_count * 8, kThreads, 0, ctx->stream>>>(
+            pl.jobs, pl.njobs, pl.max_jobs, pl.job_units, pl.snap, lbits_sub, tb.MU, tb.T, pl.hard_ms, pl.acc);
+    CPX_LAUNCH("k_hard_leaves");
+    note_launch(ctx);
+}
+
 template <class XT> static void hard_go(cpx_ctx *ctx, const Plan &pl)
 {
     const Tables &tb = ctx->tab;
@@ -821,13 +569,7 @@ template <class XT> static void hard_go(cpx_ctx *ctx, const Plan &pl)
         (uint32_t)std::min<uint64_t>(pl.offload_min, 0xFFFFFFFFull));
     CPX_LAUNCH("k_hard");
     note_launch(ctx);
-    if (pl.max_jobs) {
-        scan_u64(ctx, pl.job_units, pl.max_jobs + 1);
-        k_hard_leaves<XT><<<(unsigned)ctx->sm_count * 8, kThreads, 0, ctx->stream>>>(
-            pl.jobs, pl.njobs, pl.max_jobs, pl.job_units, pl.snap, lbits_sub, tb.MU, tb.T, pl.hard_ms, pl.acc);
-        CPX_LAUNCH("k_hard_leaves");
-        note_launch(ctx);
-    }
+    if (pl.max_jobs) launch_hard_leaves(ctx, pl, lbits_sub);
     if (pl.time_hard) CPX_CUDA(cudaEventRecord(ctx->ev_hard1, ctx->stream));
     if (pl.n_comb) {
         k_hard_combine<<<(unsigned)((pl.n_comb * 32 + 255) / 256), 256, 0, ctx->stream>>>(

@@ -1,0 +1,476 @@
+// hard_shared.cu -- the hard special leaves of a batch on one shared sieve.
+//
+// The state of the segmented phi sieve after crossing off p_c+1 .. p_b-1 does
+// not depend on x; only the leaves do.  A batch therefore sieves each
+// segment once for many queries:
+//  (1) k_sieve_counts sweeps the segments [0, nseg) once, for the largest x of
+//      the batch, and records the survivors of level b-1 of every warp
+//      sub-segment;
+//  (2) k_carry_scan turns each level's row of counts into the carries
+//      phi(lo_w - 1, b - 1), the survivors below each sub-segment (a level's
+//      first sieved segment starts from the pi table: below p_b^2 the
+//      survivors of level b-1 are 1 and the primes from p_b on);
+//  (3) k_hard_shared runs one CTA per (group of up to 32 queries, segment).
+//      Its warps sieve their sub-segments level by level as k_hard does; at
+//      each level the lanes compute the candidate range of one query each,
+//      the warp gathers the leaves of every query of the group and answers
+//      them 32 at a time, and each leaf's -mu(m) phi(u, b-1) =
+//      -mu(m) (carry + survivors of the sub-segment <= u) goes straight into
+//      its query's sum: no per-segment outputs and no carry combine.
+// Heavy (query, sub-segment, level) leaf sets go to k_hard_leaves with one
+// snapshot per (sub-segment, level) for all queries of the group.
+//
+// Restates the reference's hard-leaf sieve (src/sieve/S2_hard_host.cu:49-191,
+// src/sieve/S2_hard_device.cu:12-382), which sieves [0, z) once per x, for many
+// x at a time.
+#include <mutex>
+
+#include "sieve.cuh"
+
+namespace cpx {
+
+// shared memory of k_sieve_counts: bitmap and chunk counters
+__host__ __device__ __forceinline__ size_t counts_smem(uint32_t lbits)
+{
+    const size_t L = size_t(1) << lbits;
+    return L / 8 + (((L / 128) + 15) & ~size_t(15));
+}
+
+// shared memory of k_hard_shared
+__host__ __device__ __forceinline__ size_t shared_smem(uint32_t lbits, uint32_t threads)
+{
+    size_t o = counts_smem(lbits);
+    o += threads * 4;                      // lane prefixes
+    o += (threads / 32) * kLeafBuf * 8;    // gathered leaves: m, query | (mu(m) = -1) << 31
+    o += (threads / 32) * kGroupMax * 16;  // per-warp sums of the group's queries
+    return o;
+}
+
+template <class XT> __device__ __forceinline__ XT shfl_xt(XT v, uint32_t src)
+{
+    if (sizeof(XT) == 8) return (XT)__shfl_sync(FULL, (unsigned long long)v, src);
+    const unsigned long long a0 = __shfl_sync(FULL, (unsigned long long)v, src);
+    const unsigned long long a1 = __shfl_sync(FULL, (unsigned long long)((u128)v >> 64), src);
+    return (XT)(((u128)a1 << 64) | a0);
+}
+
+// (1) One CTA per segment: survivors of level b-1 of each warp sub-segment w,
+// for every level b the segment sieves, into row b at w - NW * first(b), where
+// first(b) = p_b^2 / span is the level's first segment.
+__global__ void __launch_bounds__(512, 2) k_sieve_counts(uint64_t nseg, uint32_t lbits, u128 xmax, uint64_t r4max,
+                                                       uint32_t c, const uint32_t *__restrict__ P, uint32_t np,
+                                                       const uint64_t *__restrict__ lvl_off, uint32_t nlv,
+                                                       uint64_t *__restrict__ cnt)
+{
+    extern __shared__ uint4 smem4[];
+    __shared__ uint32_t s_B;
+    const uint64_t seg = blockIdx.x;
+    if (seg >= nseg) return;
+    const uint32_t T = blockDim.x, tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, NW = T >> 5;
+    const uint32_t L = 1u << lbits, NC = L >> 7, CPT = NC / T;
+    const int s = __ffs(CPT) - 1;
+    const uint32_t Lw = L / NW;
+    const uint64_t span = 2ull * L, lo = seg * span;
+    const uint64_t lo_w = lo + 2ull * Lw * warp, hi_w = lo_w + 2ull * Lw;
+    if (tid == 0) s_B = seg_levels<u128>(xmax, r4max, lo, lo + span, P, np);
+    __syncthreads();
+    const uint32_t B = min(s_B, c + nlv);  // rows exist up to level c + nlv
+    if (B <= c) return;                    // uniform over the CTA
+    uint32_t *bm = reinterpret_cast<uint32_t *>(smem4);
+    uint8_t *cnt8 = reinterpret_cast<uint8_t *>(smem4) + L / 8;
+    const uint32_t c0 = CPT * tid, cw0 = c0 - CPT * 32 * warp;
+    uint32_t tot = __reduce_add_sync(FULL, presieve(bm, cnt8, P, c, lo, c0, CPT, s));
+    __syncwarp();
+    const uint64_t w = seg * NW + warp;
+    for (uint32_t gb = c + 1; gb <= B; gb += 32) {
+        const uint32_t nl = min(32u, B - gb + 1);
+        uint32_t lp = 0, lr0 = 0, li0 = 0xFFFFFFFFu;
+        if (lane < nl) {
+            lp = P[gb + lane - 1];
+            cross_params(lp, lo_w, hi_w, lr0, li0);
+        }
+        for (uint32_t k = 0; k < nl; k++) {
+            const uint32_t b = gb + k;
+            const uint32_t p = __shfl_sync(FULL, lp, k);
+            if (lane == 0) {
+                const uint64_t first = ((uint64_t)p * p) / span;
+                const uint64_t idx = lvl_off[b - c - 1] + (w - first * NW);
+                if (idx < lvl_off[b - c]) cnt[idx] = tot;
+            }
+            const uint32_t cleared = cross_off(bm, cnt8, p, __shfl_sync(FULL, lr0, k), __shfl_sync(FULL, li0, k), c0,
+                                               cw0, CPT, s, CPT * 32 * warp, lane, Lw);
+            tot -= __reduce_add_sync(FULL, cleared);
+            __syncwarp();
+        }
+    }
+}
+
+// (2) One CTA per level: exclusive scan of the level's row in place, from the
+// carry of its first segment.
+__global__ void __launch_bounds__(1024) k_carry_scan(uint32_t nlv, uint32_t c, uint64_t span,
+                                                     const uint32_t *__restrict__ P, const cpx_pient *__restrict__ T,
+                                                     const uint64_t *__restrict__ lvl_off, uint64_t *__restrict__ cnt)
+{
+    __shared__ uint64_t s_w[32];
+    const uint32_t lv = blockIdx.x;
+    if (lv >= nlv) return;
+    const uint32_t b = c + 1 + lv;
+    const uint64_t p = P[b - 1];
+    const uint64_t first = (p * p) / span;
+    uint64_t carry = 0;
+    if (first > 0) {
+        const uint64_t pl = cpx_pi_dev(T, first * span - 1);
+        carry = 1 + (pl > b - 1 ? pl - (b - 1) : 0);
+    }
+    const uint64_t r0 = lvl_off[lv], r1 = lvl_off[lv + 1];
+    const uint32_t tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nw = blockDim.x >> 5;
+    for (uint64_t base = r0; base < r1; base += blockDim.x) {
+        const uint64_t i = base + tid;
+        const uint64_t v = i < r1 ? cnt[i] : 0;
+        uint64_t inc = v;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint64_t t = __shfl_up_sync(FULL, inc, o);
+            if (lane >= (uint32_t)o) inc += t;
+        }
+        if (lane == 31) s_w[warp] = inc;
+        __syncthreads();
+        if (warp == 0) {
+            uint64_t wv = lane < nw ? s_w[lane] : 0;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const uint64_t t = __shfl_up_sync(FULL, wv, o);
+                if (lane >= (uint32_t)o) wv += t;
+            }
+            if (lane < nw) s_w[lane] = wv;
+        }
+        __syncthreads();
+        const uint64_t before = warp ? s_w[warp - 1] : 0;
+        if (i < r1) cnt[i] = carry + before + inc - v;
+        carry += s_w[nw - 1];
+        __syncthreads();
+    }
+}
+
+// (3) One CTA per (group, segment).
+template <class XT>
+__global__ void __launch_bounds__(512, 2)
+    k_hard_shared(const QD *__restrict__ qd, const HardGroup *__restrict__ grp, const uint64_t *__restrict__ pre_grp,
+                  uint32_t ngrp, uint64_t total, uint32_t lbits, uint32_t c, const uint32_t *__restrict__ P,
+                  uint32_t np, const int32_t *__restrict__ MU, const cpx_pient *__restrict__ Tpi,
+                  const uint64_t *__restrict__ lvl_off, uint32_t nlv, const uint64_t *__restrict__ carry,
+                  unsigned long long *__restrict__ acc, HardJob *__restrict__ jobs, unsigned int *__restrict__ njobs,
+                  uint64_t *__restrict__ job_units, unsigned char *__restrict__ snap, unsigned int *__restrict__ nsnap,
+                  uint32_t max_jobs, uint32_t lbits_sub, uint32_t offload_min)
+{
+    extern __shared__ uint4 smem4[];
+    __shared__ uint32_t s_B;
+    const uint64_t unit = blockIdx.x;
+    if (unit >= total) return;
+    const uint32_t g = find_q(pre_grp, ngrp, unit);
+    const HardGroup &G = grp[g];
+    const uint64_t seg = unit - pre_grp[g];
+    const uint32_t T = blockDim.x, tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, NW = T >> 5;
+    const uint32_t L = 1u << lbits, NC = L >> 7, CPT = NC / T;
+    const int s = __ffs(CPT) - 1;
+    const uint32_t Lw = L / NW;
+    const uint64_t span = 2ull * L, lo = seg * span;
+    const uint64_t lo_w = lo + 2ull * Lw * warp, hi_w = lo_w + 2ull * Lw;
+    if (tid == 0) s_B = seg_levels<XT>((XT)G.xmax, G.r4max, lo, lo + span, P, np);
+    __syncthreads();
+    const uint32_t B = min(s_B, c + nlv);
+    if (B <= c) return;  // uniform over the CTA
+
+    unsigned char *sp = reinterpret_cast<unsigned char *>(smem4);
+    uint32_t *bm = reinterpret_cast<uint32_t *>(sp);
+    size_t o = L / 8;
+    uint8_t *cnt8 = sp + o;
+    o += ((L / 128) + 15) & ~size_t(15);
+    uint32_t *wl = reinterpret_cast<uint32_t *>(sp + o) + 32 * warp;  // this warp's lane prefixes
+    o += T * 4;
+    uint2 *lbuf = reinterpret_cast<uint2 *>(sp + o) + kLeafBuf * warp;
+    o += NW * kLeafBuf * 8;
+    i128 *sacc = reinterpret_cast<i128 *>(sp + o);  // [NW][32] sums per query
+    i128 *sacc_w = sacc + 32 * warp;
+    sacc_w[lane] = 0;
+
+    // this lane's query
+    const uint32_t nq = G.n;
+    const uint32_t qj = lane < nq ? G.q[lane] : 0xFFFFFFFFu;
+    XT xj = 0;
+    uint64_t yj = 0, zj = 0;
+    if (lane < nq) {
+        const QD &d = qd[qj];
+        xj = xload<XT>(d);
+        yj = d.y;
+        zj = d.z;
+    }
+
+    const uint32_t c0 = CPT * tid, cw0 = c0 - CPT * 32 * warp;
+    presieve(bm, cnt8, P, c, lo, c0, CPT, s);
+    __syncwarp();
+    const uint64_t w = seg * NW + warp;
+    const size_t stride = snap_stride(lbits_sub);
+    auto sub_count = [&](uint64_t uu) -> uint32_t { return sub_survivors(uu, lo_w, wl, cnt8, bm, CPT, s, warp); };
+
+    for (uint32_t gb = c + 1; gb <= B; gb += 32) {
+        const uint32_t nl = min(32u, B - gb + 1);
+        uint32_t lp = 0, lr0 = 0, li0 = 0xFFFFFFFFu;
+        if (lane < nl) {
+            lp = P[gb + lane - 1];
+            cross_params(lp, lo_w, hi_w, lr0, li0);
+        }
+        for (uint32_t k = 0; k < nl; k++) {
+            const uint32_t b = gb + k;
+            const uint32_t p = __shfl_sync(FULL, lp, k);
+            const uint64_t pp = (uint64_t)p * p;
+            // Candidates (mlo, mhi] of this lane's query in the warp's
+            // sub-segment.  None unless some u in it satisfies u <= z,
+            // u >= p^2 and x/(p hi_w) < y (else m > y).
+            XT xp = 0;
+            uint32_t mlo = 0, mhi = 0;
+            bool act = false;
+            if (lane < nq && lo_w <= zj && hi_w > pp && (u128)p * yj * hi_w > (u128)xj) {
+                xp = cpx_qdiv(xj, (uint64_t)p);
+                uint64_t a = cpx_udiv_leaf(yj, p);
+                const XT t1 = cpx_qdiv(xp, hi_w);
+                if (t1 > (XT)a) a = (uint64_t)t1;
+                uint64_t e = yj;
+                if (lo_w) {
+                    const XT t2 = cpx_qdiv(xp, lo_w);
+                    if (t2 < (XT)e) e = (uint64_t)t2;
+                }
+                const XT t3 = cpx_qdiv(xp, pp);  // hard leaves only: m <= x/p^3
+                if (t3 < (XT)e) e = (uint64_t)t3;
+                mlo = (uint32_t)a;
+                mhi = (uint32_t)(e > a ? e : a);
+                act = e > ((pp > yj && p > a) ? (uint64_t)p : a);
+            }
+            const unsigned bal = __ballot_sync(FULL, act);
+            if (bal) {
+                // lane prefixes of the sub-segment from the chunk counters
+                uint32_t off0;
+                warp_place(counter_sum(cnt8 + c0, CPT), lane, off0);
+                wl[lane] = off0;
+                __syncwarp();
+                const uint64_t first = pp / span;
+                const uint64_t ci = lvl_off[b - c - 1] + (w - first * NW);
+                const uint64_t C = ci < lvl_off[b - c] ? __ldg(carry + ci) : 0;  // survivors below the sub-segment
+                uint32_t nbuf = 0, snap_k = 0xFFFFFFFFu;
+                // answers the gathered leaves 32 at a time; the entries are in
+                // query order, so each run of one query is summed by a
+                // segmented warp scan and added once
+                auto flush = [&] {
+                    __syncwarp();
+                    for (uint32_t base = 0; base < nbuf; base += 32) {
+                        const uint32_t jj = base + lane;
+                        const bool ok = jj < nbuf;
+                        uint2 e = make_uint2(1u, 0u);
+                        if (ok) e = lbuf[jj];
+                        const uint32_t key = ok ? (e.y & 31u) : 0xFFu;
+                        const XT xpk = shfl_xt(xp, key & 31u);
+                        int64_t v = 0;
+                        if (ok) {
+                            const int64_t f = (int64_t)(C + sub_count((uint64_t)cpx_qdiv(xpk, (uint64_t)e.x)));
+                            v = (e.y >> 31) ? f : -f;
+                        }
+#pragma unroll
+                        for (int d = 1; d < 32; d <<= 1) {
+                            const int64_t tv = __shfl_up_sync(FULL, v, d);
+                            const uint32_t tk = __shfl_up_sync(FULL, key, d);
+                            if (lane >= (uint32_t)d && tk == key) v += tv;
+                        }
+                        const uint32_t nk = __shfl_down_sync(FULL, key, 1);
+                        if (ok && (lane == 31 || nk != key)) sacc_w[key] += (i128)v;
+                    }
+                    __syncwarp();
+                    nbuf = 0;
+                };
+                for (unsigned rem = bal; rem; rem &= rem - 1) {
+                    const uint32_t j = __ffs(rem) - 1;
+                    const XT xpj = shfl_xt(xp, j);
+                    const uint64_t mloj = __shfl_sync(FULL, mlo, j), mhij = __shfl_sync(FULL, mhi, j);
+                    const uint64_t yq = __shfl_sync(FULL, (unsigned long long)yj, j);
+                    const bool prime_lvl = pp > yq;
+                    const uint64_t qa = mloj > p ? mloj : p;
+                    uint64_t work;
+                    if (prime_lvl) work = (mhij > qa) ? 8 * (((mhij - 1) >> 7) - (qa >> 7) + 1) : 0;
+                    else work = ((mhij - 1) >> 1) - ((mloj + 1) >> 1) + 1;
+                    if (max_jobs && offload_min && work >= offload_min) {
+                        unsigned int jb = 0, sn = snap_k;
+                        if (lane == 0) {
+                            jb = atomicAdd(njobs, 1u);
+                            if (jb < max_jobs && sn == 0xFFFFFFFFu) sn = atomicAdd(nsnap, 1u);
+                        }
+                        jb = __shfl_sync(FULL, jb, 0);
+                        sn = __shfl_sync(FULL, sn, 0);
+                        // (a job slot taken without a snapshot keeps 0 units)
+                        if (jb < max_jobs && sn < max_jobs) {
+                            if (snap_k == 0xFFFFFFFFu) {
+                                snap_k = sn;
+                                uint4 *sb = reinterpret_cast<uint4 *>(snap + (size_t)sn * stride);
+                                uint32_t *spre = reinterpret_cast<uint32_t *>(sb + ((size_t(1) << lbits_sub) >> 7));
+                                snapshot_chunks(sb, spre, bm, cnt8, cw0, c0, CPT, s, wl[lane]);
+                            }
+                            if (lane == 0) {
+                                HardJob J;
+                                J.q = __ldg(&G.q[j]);
+                                J.b = b;
+                                J.p = p;
+                                J.kind = prime_lvl ? 1u : 0u;
+                                J.mlo = prime_lvl ? qa : mloj;
+                                J.mhi = mhij;
+                                J.lo = lo_w;
+                                J.slot = ~0ull;
+                                J.nunits = prime_lvl ? (work / 8 + kJobWords - 1) / kJobWords
+                                                     : ((((mhij - 1) >> 1) >> 2) - (((mloj + 1) >> 1) >> 2) +
+                                                        kJobGroups) /
+                                                           kJobGroups;
+                                J.carry = C;
+                                J.snap = sn;
+                                J.pad = 0;
+                                J.xp = (u128)xpj;
+                                jobs[jb] = J;
+                                job_units[jb] = J.nunits;
+                            }
+                            continue;
+                        }
+                    }
+                    if (prime_lvl) {
+                        // m must be a prime q > p: walk the pi-table bitmap of (max(mlo, p), mhi]
+                        const uint64_t w0q = qa >> 7, w1q = (mhij - 1) >> 7;
+                        for (uint64_t wb = w0q; wb <= w1q; wb += 32) {
+                            const uint64_t wq = wb + lane;
+                            uint64_t qb = 0;
+                            if (wq <= w1q)
+                                qb = __ldg(reinterpret_cast<const ulonglong2 *>(Tpi) + wq).x & range_mask(wq, qa, mhij);
+                            uint32_t off;
+                            const uint32_t tot_r = warp_place((uint32_t)__popcll(qb), lane, off);
+                            if (tot_r > kLeafBuf) {  // a dense round: each lane answers its own word
+                                int64_t v = 0;
+                                while (qb) {
+                                    const int jq = __ffsll((long long)qb) - 1;
+                                    qb &= qb - 1;
+                                    v += (int64_t)(C + sub_count((uint64_t)cpx_qdiv(xpj, 128 * wq + 2 * jq + 1)));
+                                }
+#pragma unroll
+                                for (int d = 16; d > 0; d >>= 1) v += __shfl_xor_sync(FULL, v, d);
+                                if (lane == 0) sacc_w[j] += (i128)v;  // mu(q) = -1
+                                continue;
+                            }
+                            if (nbuf + tot_r > kLeafBuf) flush();
+                            uint32_t kk = nbuf + off;
+                            while (qb) {
+                                const int jq = __ffsll((long long)qb) - 1;
+                                qb &= qb - 1;
+                                lbuf[kk++] = make_uint2((uint32_t)(128 * wq + 2 * jq + 1), j | 0x80000000u);
+                            }
+                            nbuf += tot_r;
+                        }
+                    } else {
+                        // any squarefree m with lpf(m) > p: 16-byte loads of packed mu*lpf
+                        const uint64_t i_lo = (mloj + 1) >> 1, i_hi = (mhij - 1) >> 1;
+                        for (uint64_t gq = i_lo >> 2; gq <= (i_hi >> 2); gq += 32) {
+                            const uint64_t g4 = gq + lane;
+                            uint32_t neg = 0, vm = 0;
+                            if (g4 <= (i_hi >> 2))
+                                vm = valid_group(__ldg(reinterpret_cast<const int4 *>(MU) + g4), g4, i_lo, i_hi, p, &neg);
+                            uint32_t off;
+                            const uint32_t tot_r = warp_place((uint32_t)__popc(vm), lane, off);
+                            if (nbuf + tot_r > kLeafBuf) flush();
+                            uint32_t kk = nbuf + off;
+                            while (vm) {
+                                const int kq = __ffs(vm) - 1;
+                                vm &= vm - 1;
+                                lbuf[kk++] = make_uint2((uint32_t)(2 * (4 * g4 + kq) + 1), j | (((neg >> kq) & 1u) << 31));
+                            }
+                            nbuf += tot_r;
+                        }
+                    }
+                }
+                flush();
+            }
+            // ---- cross off p_b in the sub-segment
+            cross_off(bm, cnt8, p, __shfl_sync(FULL, lr0, k), __shfl_sync(FULL, li0, k), c0, cw0, CPT, s,
+                      CPT * 32 * warp, lane, Lw);
+            __syncwarp();
+        }
+    }
+    __syncthreads();
+    if (warp == 0 && lane < nq) {
+        i128 t = 0;
+        for (uint32_t ww = 0; ww < NW; ww++) t += sacc[32 * ww + lane];
+        acc_add(acc, qj, ACC_HARD, t);
+    }
+}
+
+// ------------------------------------------------------------------ launchers
+
+size_t hard_shared_smem_bytes(uint32_t lbits, uint32_t threads) { return shared_smem(lbits, threads); }
+
+template <class XT> static void shared_go(cpx_ctx *ctx, const Plan &pl)
+{
+    const Tables &tb = ctx->tab;
+    const uint32_t T = pl.hard_threads;
+    const uint32_t lbits_sub = pl.sh_lbits - (uint32_t)(__builtin_ctz(T) - 5);
+    if (pl.time_hard) CPX_CUDA(cudaEventRecord(ctx->ev_hard0, ctx->stream));
+    if (pl.sh_nlv) {
+        k_sieve_counts<<<(unsigned)pl.sh_nseg, T, counts_smem(pl.sh_lbits), ctx->stream>>>(
+            pl.sh_nseg, pl.sh_lbits, pl.sh_xmax, pl.sh_r4max, pl.c, tb.P, (uint32_t)tb.prm_n, pl.lvl_off, pl.sh_nlv,
+            pl.carry);
+        CPX_LAUNCH("k_sieve_counts");
+        k_carry_scan<<<pl.sh_nlv, 1024, 0, ctx->stream>>>(pl.sh_nlv, pl.c, 2ull << pl.sh_lbits, tb.P, tb.T, pl.lvl_off,
+                                                           pl.carry);
+        CPX_LAUNCH("k_carry_scan");
+        note_launch(ctx, 2);
+    }
+    if (pl.max_jobs) {
+        CPX_CUDA(cudaMemsetAsync(pl.njobs, 0, 2 * sizeof(uint64_t), ctx->stream));  // job and snapshot counters
+        CPX_CUDA(cudaMemsetAsync(pl.job_units, 0, (pl.max_jobs + 1) * sizeof(uint64_t), ctx->stream));
+    }
+    k_hard_shared<XT><<<(unsigned)pl.n_gunits, T, shared_smem(pl.sh_lbits, T), ctx->stream>>>(
+        pl.qd, pl.grp, pl.pre_grp, pl.n_grp, pl.n_gunits, pl.sh_lbits, pl.c, tb.P, (uint32_t)tb.prm_n, tb.MU, tb.T,
+        pl.lvl_off, pl.sh_nlv, pl.carry, pl.acc, pl.jobs, pl.njobs, pl.job_units, pl.snap, pl.nsnap, pl.max_jobs,
+        lbits_sub, (uint32_t)std::min<uint64_t>(pl.offload_min, 0xFFFFFFFFull));
+    CPX_LAUNCH("k_hard_shared");
+    note_launch(ctx);
+    if (pl.max_jobs) launch_hard_leaves(ctx, pl, lbits_sub);
+    if (pl.time_hard) CPX_CUDA(cudaEventRecord(ctx->ev_hard1, ctx->stream));
+}
+
+// the largest dynamic shared memory a kernel may ask for: the device's opt-in
+// maximum less the kernel's static shared memory
+template <class K> static void raise_dyn_smem(K *kernel, size_t optin)
+{
+    cudaFuncAttributes fa;
+    CPX_CUDA(cudaFuncGetAttributes(&fa, kernel));
+    CPX_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(optin - fa.sharedSizeBytes)));
+}
+
+// raises the dynamic shared-memory limits once per device (see prepare_hard)
+void prepare_hard_shared(cpx_ctx *ctx, const Plan &pl)
+{
+    if (!pl.n_gunits) return;
+    if (shared_smem(pl.sh_lbits, pl.hard_threads) + 64 > ctx->smem_optin)
+        fail(CPX_EINVAL, "shared hard-leaf segment needs more shared memory than a block can have");
+    static std::mutex m;
+    static int done_dev[2] = {-1, -1};
+    std::lock_guard<std::mutex> g(m);
+    const int w = pl.wide ? 1 : 0;
+    if (done_dev[w] == ctx->device) return;
+    raise_dyn_smem(k_sieve_counts, ctx->smem_optin);
+    if (pl.wide) raise_dyn_smem(k_hard_shared<u128>, ctx->smem_optin);
+    else raise_dyn_smem(k_hard_shared<uint64_t>, ctx->smem_optin);
+    done_dev[w] = ctx->device;
+}
+
+void launch_hard_shared(cpx_ctx *ctx, const Plan &pl)
+{
+    if (!pl.n_gunits) return;
+    if (pl.n_gunits > 0x7FFFFFFFull || pl.sh_nseg > 0x7FFFFFFFull)
+        fail(CPX_ERANGE, "too many hard-leaf segments in one launch");
+    if (pl.wide) shared_go<u128>(ctx, pl);
+    else shared_go<uint64_t>(ctx, pl);
+}
+
+}  // namespace cpx

@@ -357,6 +357,7 @@ int cpx_serve_create(cpx_ctx *ctx, const cpx_serve_config *cfg, cpx_server **out
             l->hard_log2_bits = ctx->hard_log2_bits;
             l->hard_threads = ctx->hard_threads;
             l->hard_offload_min = ctx->hard_offload_min;
+            l->hard_shared = ctx->hard_shared;
             l->hard_offload_bytes = ctx->hard_offload_bytes;
             for (uint32_t e = 0; e < kTuneDecades; e++) l->tune[e] = ctx->tune[e];
             l->tuned = ctx->tuned;

@@ -34,17 +34,33 @@ struct __align__(16) EasyLvl {
     uint64_t i_lo, i_hi, i_base, unit0;
 };
 
-// A heavy (segment, level) leaf set handed from k_hard to k_hard_leaves: the
-// segment's bitmap and per-chunk survivor prefixes at level b-1 sit in
-// snapshot slot `job`; the leaves are m in (mlo, mhi] (prime m only when
+// A heavy (sub-segment, level) leaf set handed from a sieve kernel to
+// k_hard_leaves: the sub-segment's bitmap and per-chunk survivor prefixes at
+// level b-1 sit in snapshot slot `snap` (one slot can serve the sets of
+// several queries); the leaves are m in (mlo, mhi] (prime m only when
 // kind = 1).  nunits counts its k_hard_leaves work units; their offsets are
-// the scanned job-unit array.
+// the scanned job-unit array.  `slot` is the level output that receives
+// Sum(-mu), ~0 when `carry` already counts every survivor below the
+// sub-segment.
 struct __align__(16) HardJob {
     uint32_t q, b, p, kind;
     uint64_t mlo, mhi, lo, slot;  // lo: first number of the warp's sub-segment
     uint64_t nunits;              // k_hard_leaves work units
-    uint64_t carry;               // survivors of level b-1 in the segment below the sub-segment
+    uint64_t carry;               // survivors of level b-1 below the sub-segment (in its segment, or all)
+    uint64_t snap;                // snapshot slot
+    uint64_t pad;
     u128 xp;
+};
+
+// Up to 32 queries of a batch whose hard leaves share one sieve (z
+// descending).  Its work units are the segments [0, nseg) of the group;
+// xmax and r4max = iroot4(xmax) bound the levels each segment sieves.
+constexpr uint32_t kGroupMax = 32;
+struct __align__(16) HardGroup {
+    u128 xmax;
+    uint64_t r4max, nseg;
+    uint32_t n, pad[3];
+    uint32_t q[kGroupMax];
 };
 
 // accumulator slots per query (each a signed 128-bit value = 2 words)
@@ -85,6 +101,18 @@ struct Plan {
     uint64_t n_ecomp = 0;
     uint64_t *easy_off = nullptr;  // n_easy + 1 chunk offsets of the easy leaves
     HardLevel *hard_levels = nullptr;  // per-level outputs of query 0 (a part of a split query)
+    // batch-shared sieve (hard_shared.cu): one counting sweep over the
+    // segments [0, sh_nseg) for xmax, carries per (sub-segment, level) in
+    // rows from lvl_off, then the groups' units
+    bool shared = false;
+    uint32_t sh_lbits = 0, sh_nlv = 0, n_grp = 0;
+    uint64_t sh_nseg = 0, sh_r4max = 0, n_gunits = 0, n_carry = 0;
+    u128 sh_xmax = 0;
+    const HardGroup *grp = nullptr;
+    const uint64_t *pre_grp = nullptr;  // n_grp + 1 unit offsets
+    const uint64_t *lvl_off = nullptr;  // sh_nlv + 1 row offsets into carry
+    uint64_t *carry = nullptr;
+    unsigned int *nsnap = nullptr;      // device counter of snapshot slots
 };
 
 void launch_ordinary(cpx_ctx *ctx, const Plan &pl);
@@ -102,5 +130,11 @@ size_t hard_smem_bytes(uint32_t lbits, uint32_t threads, bool wide);
 // before the launches so that they can be captured in a graph
 void prepare_hard(cpx_ctx *ctx, const Plan &pl);
 size_t hard_snapshot_stride(uint32_t lbits_max);
+// the batch-shared sieve (hard_shared.cu)
+void prepare_hard_shared(cpx_ctx *ctx, const Plan &pl);
+void launch_hard_shared(cpx_ctx *ctx, const Plan &pl);
+size_t hard_shared_smem_bytes(uint32_t lbits, uint32_t threads);
+// k_hard_leaves over the jobs of pl (hard.cu)
+void launch_hard_leaves(cpx_ctx *ctx, const Plan &pl, uint32_t lbits_sub);
 
 }  // namespace cpx

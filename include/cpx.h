@@ -86,6 +86,13 @@ int cpx_set_hard_params(cpx_ctx *ctx, uint32_t log2_bits, uint32_t threads);
  * candidate m is answered by a separate GPU-wide leaf kernel from a snapshot
  * of the sub-segment; 0 answers every leaf inside the sieve (default 1024) */
 int cpx_set_hard_offload(cpx_ctx *ctx, uint32_t min_candidates);
+/* Batches share one hard-leaf sieve between their queries: the survivor
+ * counts of one sweep give every (sub-segment, level) its carry, and each
+ * segment is then sieved once per group of up to 32 queries, answering all
+ * their leaves.  mode 0: never (one sieve per query), 1: batches of more than
+ * four queries with at least eight hard-leaf queries (default), 2: always.
+ * Results are the same in every mode.  No reference counterpart. */
+int cpx_set_hard_shared(cpx_ctx *ctx, uint32_t mode);
 /* P2 needs pi(x/p) up to z = x/y.  For z above `limit` (default 2^36) the
  * resident pi table stops at sqrt(x) and P2 is summed over pi-table windows
  * of 2^34 integers built one after another (the 128-bit path to 1e20). */
@@ -110,9 +117,10 @@ typedef struct {
     double launch_ms;     /* staging copy and kernel launches (enqueue only) */
     double wait_ms;       /* waiting for the device and reading the results */
     uint64_t queries;
-    uint64_t segments;    /* hard-leaf segments */
+    uint64_t segments;    /* hard-leaf sieve work units (CTAs) */
     uint64_t hard_jobs;   /* leaf-set slots reserved for k_hard_leaves */
     uint64_t offload_min; /* candidate threshold of an offloaded leaf set */
+    uint64_t shared_groups; /* query groups sharing a sieve (0: one sieve per query) */
 } cpx_batch_stats;
 int cpx_last_batch_stats(cpx_ctx *ctx, cpx_batch_stats *out);
 /* CUDA-event stopwatch on the context stream: start records an event; stop
