@@ -42,7 +42,8 @@ __host__ __device__ __forceinline__ size_t shared_smem(uint32_t lbits, uint32_t 
     size_t o = counts_smem(lbits);
     o += threads * 4;                      // lane prefixes
     o += (threads / 32) * kLeafBuf * 8;    // gathered leaves: m, query | (mu(m) = -1) << 31
-    o += (threads / 32) * kGroupMax * 16;  // per-warp sums of the group's queries
+    o += (threads / 32) * kGroupMax * 16;  // x/p of the group's queries, per warp
+    o += (threads / 32) * kGroupMax * 12;  // per-warp, per-query level sums and Sum(-mu)
     return o;
 }
 
@@ -152,7 +153,17 @@ __global__ void __launch_bounds__(1024) k_carry_scan(uint32_t nlv, uint32_t c, u
     }
 }
 
-// (3) One CTA per (group, segment).
+// (3) One CTA per (group, segment).  Per level, the lanes hold one query
+// each: its x/p and candidate range in the warp's sub-segment.  The warp then
+// walks the candidates of all the group's queries as one sequence (pi-table
+// words of the prime-only levels, then 4-m groups of packed mu*lpf of the
+// others), 32 words at a time, each lane finding its word's query by a binary
+// search over the warp's exclusive word counts; the leaves found go to the
+// warp's buffer (m, query | (mu(m) = -1) << 31) and are answered 32 at a
+// time.  Each lane keeps a running Sum(-mu) * count and Sum(-mu) for the
+// query of its last leaf and adds them into the warp's per-query slots when
+// the query changes; at the end of the level lane j folds slot j into its
+// 128-bit total as sum + carry * Sum(-mu).
 template <class XT>
 __global__ void __launch_bounds__(512, 2)
     k_hard_shared(const QD *__restrict__ qd, const HardGroup *__restrict__ grp, const uint64_t *__restrict__ pre_grp,
@@ -188,11 +199,16 @@ __global__ void __launch_bounds__(512, 2)
     o += ((L / 128) + 15) & ~size_t(15);
     uint32_t *wl = reinterpret_cast<uint32_t *>(sp + o) + 32 * warp;  // this warp's lane prefixes
     o += T * 4;
-    uint2 *lbuf = reinterpret_cast<uint2 *>(sp + o) + kLeafBuf * warp;
+    uint2 *lbuf0 = reinterpret_cast<uint2 *>(sp + o);
+    uint2 *lbuf = lbuf0 + kLeafBuf * warp;
     o += NW * kLeafBuf * 8;
-    i128 *sacc = reinterpret_cast<i128 *>(sp + o);  // [NW][32] sums per query
-    i128 *sacc_w = sacc + 32 * warp;
-    sacc_w[lane] = 0;
+    XT *s_xp = reinterpret_cast<XT *>(sp + o) + 32 * warp;  // x/p of each query at the current level
+    o += NW * 32 * 16;
+    unsigned long long *s_sum = reinterpret_cast<unsigned long long *>(sp + o) + 32 * warp;
+    o += NW * 32 * 8;
+    int *s_ms = reinterpret_cast<int *>(sp + o) + 32 * warp;
+    s_sum[lane] = 0;
+    s_ms[lane] = 0;
 
     // this lane's query
     const uint32_t nq = G.n;
@@ -205,6 +221,7 @@ __global__ void __launch_bounds__(512, 2)
         yj = d.y;
         zj = d.z;
     }
+    i128 accq = 0;  // this lane's query: its hard sum over the CTA's part of the segment
 
     const uint32_t c0 = CPT * tid, cw0 = c0 - CPT * 32 * warp;
     presieve(bm, cnt8, P, c, lo, c0, CPT, s);
@@ -252,143 +269,185 @@ __global__ void __launch_bounds__(512, 2)
                 uint32_t off0;
                 warp_place(counter_sum(cnt8 + c0, CPT), lane, off0);
                 wl[lane] = off0;
+                if (act) s_xp[lane] = xp;
                 __syncwarp();
                 const uint64_t first = pp / span;
                 const uint64_t ci = lvl_off[b - c - 1] + (w - first * NW);
                 const uint64_t C = ci < lvl_off[b - c] ? __ldg(carry + ci) : 0;  // survivors below the sub-segment
-                uint32_t nbuf = 0, snap_k = 0xFFFFFFFFu;
-                // answers the gathered leaves 32 at a time; the entries are in
-                // query order, so each run of one query is summed by a
-                // segmented warp scan and added once
+                const bool prime_j = pp > yj;  // m must be a prime q > max(mlo, p)
+                const uint32_t qa_j = mlo > p ? mlo : p;
+                uint64_t work = 0;
+                if (act)
+                    work = prime_j ? 8 * ((((uint64_t)mhi - 1) >> 7) - (qa_j >> 7) + 1)
+                                   : ((((uint64_t)mhi - 1) >> 1) - (((uint64_t)mlo + 1) >> 1) + 1);
+                // heavy sets to k_hard_leaves, one snapshot for the warp's level
+                bool off_j = act && max_jobs && offload_min && work >= offload_min;
+                uint32_t snap_k = 0xFFFFFFFFu;
+                for (unsigned offm = __ballot_sync(FULL, off_j); offm; offm &= offm - 1) {
+                    const uint32_t j = __ffs(offm) - 1;
+                    unsigned int jb = 0, sn = snap_k;
+                    if (lane == 0) {
+                        jb = atomicAdd(njobs, 1u);
+                        if (jb < max_jobs && sn == 0xFFFFFFFFu) sn = atomicAdd(nsnap, 1u);
+                    }
+                    jb = __shfl_sync(FULL, jb, 0);
+                    sn = __shfl_sync(FULL, sn, 0);
+                    // (a job slot taken without a snapshot keeps 0 units)
+                    if (jb < max_jobs && sn < max_jobs) {
+                        if (snap_k == 0xFFFFFFFFu) {
+                            snap_k = sn;
+                            uint4 *sb = reinterpret_cast<uint4 *>(snap + (size_t)sn * stride);
+                            uint32_t *spre = reinterpret_cast<uint32_t *>(sb + ((size_t(1) << lbits_sub) >> 7));
+                            snapshot_chunks(sb, spre, bm, cnt8, cw0, c0, CPT, s, wl[lane]);
+                        }
+                        if (lane == j) {
+                            HardJob J;
+                            J.q = qj;
+                            J.b = b;
+                            J.p = p;
+                            J.kind = prime_j ? 1u : 0u;
+                            J.mlo = prime_j ? qa_j : mlo;
+                            J.mhi = mhi;
+                            J.lo = lo_w;
+                            J.slot = ~0ull;
+                            J.nunits = prime_j ? (work / 8 + kJobWords - 1) / kJobWords
+                                               : ((((uint64_t)mhi - 1) >> 3) - (((uint64_t)mlo + 1) >> 3) + kJobGroups) /
+                                                     kJobGroups;
+                            J.carry = C;
+                            J.snap = sn;
+                            J.pad = 0;
+                            J.xp = (u128)xp;
+                            jobs[jb] = J;
+                            job_units[jb] = J.nunits;
+                        }
+                    } else if (lane == j) {
+                        off_j = false;  // no slot left: answered here
+                    }
+                }
+                // running sums of the query of this lane's last leaf
+                uint32_t cur = 0xFFu;
+                int64_t csum = 0;
+                int32_t cms = 0;
+                auto put = [&](uint32_t key, uint32_t cv, bool plus) {
+                    if (key != cur) {
+                        if (cur != 0xFFu) {
+                            atomicAdd(s_sum + cur, (unsigned long long)csum);
+                            atomicAdd(s_ms + cur, cms);
+                        }
+                        cur = key;
+                        csum = 0;
+                        cms = 0;
+                    }
+                    if (plus) {
+                        csum += cv;
+                        cms += 1;
+                    } else {
+                        csum -= cv;
+                        cms -= 1;
+                    }
+                };
+                uint32_t nbuf = 0;
                 auto flush = [&] {
                     __syncwarp();
-                    for (uint32_t base = 0; base < nbuf; base += 32) {
-                        const uint32_t jj = base + lane;
-                        const bool ok = jj < nbuf;
-                        uint2 e = make_uint2(1u, 0u);
-                        if (ok) e = lbuf[jj];
-                        const uint32_t key = ok ? (e.y & 31u) : 0xFFu;
-                        const XT xpk = shfl_xt(xp, key & 31u);
-                        int64_t v = 0;
-                        if (ok) {
-                            const int64_t f = (int64_t)(C + sub_count((uint64_t)cpx_qdiv(xpk, (uint64_t)e.x)));
-                            v = (e.y >> 31) ? f : -f;
-                        }
-#pragma unroll
-                        for (int d = 1; d < 32; d <<= 1) {
-                            const int64_t tv = __shfl_up_sync(FULL, v, d);
-                            const uint32_t tk = __shfl_up_sync(FULL, key, d);
-                            if (lane >= (uint32_t)d && tk == key) v += tv;
-                        }
-                        const uint32_t nk = __shfl_down_sync(FULL, key, 1);
-                        if (ok && (lane == 31 || nk != key)) sacc_w[key] += (i128)v;
+                    for (uint32_t jj = lane; jj < nbuf; jj += 32) {
+                        const uint2 e = lbuf[jj];
+                        const uint32_t key = e.y & 31u;
+                        put(key, sub_count((uint64_t)cpx_qdiv(s_xp[key], (uint64_t)e.x)), (e.y >> 31) != 0);
                     }
                     __syncwarp();
                     nbuf = 0;
                 };
-                for (unsigned rem = bal; rem; rem &= rem - 1) {
-                    const uint32_t j = __ffs(rem) - 1;
-                    const XT xpj = shfl_xt(xp, j);
-                    const uint64_t mloj = __shfl_sync(FULL, mlo, j), mhij = __shfl_sync(FULL, mhi, j);
-                    const uint64_t yq = __shfl_sync(FULL, (unsigned long long)yj, j);
-                    const bool prime_lvl = pp > yq;
-                    const uint64_t qa = mloj > p ? mloj : p;
-                    uint64_t work;
-                    if (prime_lvl) work = (mhij > qa) ? 8 * (((mhij - 1) >> 7) - (qa >> 7) + 1) : 0;
-                    else work = ((mhij - 1) >> 1) - ((mloj + 1) >> 1) + 1;
-                    if (max_jobs && offload_min && work >= offload_min) {
-                        unsigned int jb = 0, sn = snap_k;
-                        if (lane == 0) {
-                            jb = atomicAdd(njobs, 1u);
-                            if (jb < max_jobs && sn == 0xFFFFFFFFu) sn = atomicAdd(nsnap, 1u);
+                // the query owning flat item f: the last lane j with ex[j] <= f
+                auto owner = [&](uint32_t ex, uint32_t f) -> uint32_t {
+                    uint32_t jq = 0;
+#pragma unroll
+                    for (uint32_t st = 16; st; st >>= 1) {
+                        const uint32_t cnd = jq + st;
+                        if (__shfl_sync(FULL, ex, cnd) <= f) jq = cnd;
+                    }
+                    return jq;
+                };
+                {
+                    // prime-only levels: pi-table words of (max(mlo, p), mhi]
+                    const uint32_t nw_j =
+                        (act && !off_j && prime_j) ? (uint32_t)((((uint64_t)mhi - 1) >> 7) - (qa_j >> 7) + 1) : 0u;
+                    uint32_t ex_j;
+                    const uint32_t tot_w = warp_place(nw_j, lane, ex_j);
+                    for (uint32_t base = 0; base < tot_w; base += 32) {
+                        const uint32_t f = base + lane;
+                        const uint32_t jq = owner(ex_j, f);
+                        const uint32_t exq = __shfl_sync(FULL, ex_j, jq);
+                        const uint64_t qaq = __shfl_sync(FULL, qa_j, jq), mhq = __shfl_sync(FULL, mhi, jq);
+                        uint64_t qb = 0, wq = 0;
+                        if (f < tot_w) {
+                            wq = (qaq >> 7) + (f - exq);
+                            qb = __ldg(reinterpret_cast<const ulonglong2 *>(Tpi) + wq).x & range_mask(wq, qaq, mhq);
                         }
-                        jb = __shfl_sync(FULL, jb, 0);
-                        sn = __shfl_sync(FULL, sn, 0);
-                        // (a job slot taken without a snapshot keeps 0 units)
-                        if (jb < max_jobs && sn < max_jobs) {
-                            if (snap_k == 0xFFFFFFFFu) {
-                                snap_k = sn;
-                                uint4 *sb = reinterpret_cast<uint4 *>(snap + (size_t)sn * stride);
-                                uint32_t *spre = reinterpret_cast<uint32_t *>(sb + ((size_t(1) << lbits_sub) >> 7));
-                                snapshot_chunks(sb, spre, bm, cnt8, cw0, c0, CPT, s, wl[lane]);
-                            }
-                            if (lane == 0) {
-                                HardJob J;
-                                J.q = __ldg(&G.q[j]);
-                                J.b = b;
-                                J.p = p;
-                                J.kind = prime_lvl ? 1u : 0u;
-                                J.mlo = prime_lvl ? qa : mloj;
-                                J.mhi = mhij;
-                                J.lo = lo_w;
-                                J.slot = ~0ull;
-                                J.nunits = prime_lvl ? (work / 8 + kJobWords - 1) / kJobWords
-                                                     : ((((mhij - 1) >> 1) >> 2) - (((mloj + 1) >> 1) >> 2) +
-                                                        kJobGroups) /
-                                                           kJobGroups;
-                                J.carry = C;
-                                J.snap = sn;
-                                J.pad = 0;
-                                J.xp = (u128)xpj;
-                                jobs[jb] = J;
-                                job_units[jb] = J.nunits;
+                        uint32_t off;
+                        const uint32_t tot_r = warp_place((uint32_t)__popcll(qb), lane, off);
+                        if (tot_r > kLeafBuf) {  // a dense round: each lane answers its own word
+                            const XT xq = s_xp[jq];
+                            while (qb) {
+                                const int jb = __ffsll((long long)qb) - 1;
+                                qb &= qb - 1;
+                                put(jq, sub_count((uint64_t)cpx_qdiv(xq, 128 * wq + 2 * jb + 1)), true);  // mu(q) = -1
                             }
                             continue;
                         }
+                        if (nbuf + tot_r > kLeafBuf) flush();
+                        uint32_t kk = nbuf + off;
+                        while (qb) {
+                            const int jb = __ffsll((long long)qb) - 1;
+                            qb &= qb - 1;
+                            lbuf[kk++] = make_uint2((uint32_t)(128 * wq + 2 * jb + 1), jq | 0x80000000u);
+                        }
+                        nbuf += tot_r;
                     }
-                    if (prime_lvl) {
-                        // m must be a prime q > p: walk the pi-table bitmap of (max(mlo, p), mhi]
-                        const uint64_t w0q = qa >> 7, w1q = (mhij - 1) >> 7;
-                        for (uint64_t wb = w0q; wb <= w1q; wb += 32) {
-                            const uint64_t wq = wb + lane;
-                            uint64_t qb = 0;
-                            if (wq <= w1q)
-                                qb = __ldg(reinterpret_cast<const ulonglong2 *>(Tpi) + wq).x & range_mask(wq, qa, mhij);
-                            uint32_t off;
-                            const uint32_t tot_r = warp_place((uint32_t)__popcll(qb), lane, off);
-                            if (tot_r > kLeafBuf) {  // a dense round: each lane answers its own word
-                                int64_t v = 0;
-                                while (qb) {
-                                    const int jq = __ffsll((long long)qb) - 1;
-                                    qb &= qb - 1;
-                                    v += (int64_t)(C + sub_count((uint64_t)cpx_qdiv(xpj, 128 * wq + 2 * jq + 1)));
-                                }
-#pragma unroll
-                                for (int d = 16; d > 0; d >>= 1) v += __shfl_xor_sync(FULL, v, d);
-                                if (lane == 0) sacc_w[j] += (i128)v;  // mu(q) = -1
-                                continue;
-                            }
-                            if (nbuf + tot_r > kLeafBuf) flush();
-                            uint32_t kk = nbuf + off;
-                            while (qb) {
-                                const int jq = __ffsll((long long)qb) - 1;
-                                qb &= qb - 1;
-                                lbuf[kk++] = make_uint2((uint32_t)(128 * wq + 2 * jq + 1), j | 0x80000000u);
-                            }
-                            nbuf += tot_r;
+                }
+                {
+                    // other levels: squarefree m with lpf(m) > p, 16-byte groups of packed mu*lpf
+                    uint32_t ng_j = 0;
+                    if (act && !off_j && !prime_j)
+                        ng_j = (uint32_t)(((((uint64_t)mhi - 1) >> 1) >> 2) - ((((uint64_t)mlo + 1) >> 1) >> 2) + 1);
+                    uint32_t ex_j;
+                    const uint32_t tot_g = warp_place(ng_j, lane, ex_j);
+                    for (uint32_t base = 0; base < tot_g; base += 32) {
+                        const uint32_t f = base + lane;
+                        const uint32_t jq = owner(ex_j, f);
+                        const uint32_t exq = __shfl_sync(FULL, ex_j, jq);
+                        const uint64_t mlq = __shfl_sync(FULL, mlo, jq), mhq = __shfl_sync(FULL, mhi, jq);
+                        const uint64_t i_lo = (mlq + 1) >> 1, i_hi = (mhq - 1) >> 1;
+                        uint32_t neg = 0, vm = 0;
+                        uint64_t g4 = 0;
+                        if (f < tot_g) {
+                            g4 = (i_lo >> 2) + (f - exq);
+                            vm = valid_group(__ldg(reinterpret_cast<const int4 *>(MU) + g4), g4, i_lo, i_hi, p, &neg);
                         }
-                    } else {
-                        // any squarefree m with lpf(m) > p: 16-byte loads of packed mu*lpf
-                        const uint64_t i_lo = (mloj + 1) >> 1, i_hi = (mhij - 1) >> 1;
-                        for (uint64_t gq = i_lo >> 2; gq <= (i_hi >> 2); gq += 32) {
-                            const uint64_t g4 = gq + lane;
-                            uint32_t neg = 0, vm = 0;
-                            if (g4 <= (i_hi >> 2))
-                                vm = valid_group(__ldg(reinterpret_cast<const int4 *>(MU) + g4), g4, i_lo, i_hi, p, &neg);
-                            uint32_t off;
-                            const uint32_t tot_r = warp_place((uint32_t)__popc(vm), lane, off);
-                            if (nbuf + tot_r > kLeafBuf) flush();
-                            uint32_t kk = nbuf + off;
-                            while (vm) {
-                                const int kq = __ffs(vm) - 1;
-                                vm &= vm - 1;
-                                lbuf[kk++] = make_uint2((uint32_t)(2 * (4 * g4 + kq) + 1), j | (((neg >> kq) & 1u) << 31));
-                            }
-                            nbuf += tot_r;
+                        uint32_t off;
+                        const uint32_t tot_r = warp_place((uint32_t)__popc(vm), lane, off);
+                        if (nbuf + tot_r > kLeafBuf) flush();
+                        uint32_t kk = nbuf + off;
+                        while (vm) {
+                            const int kq = __ffs(vm) - 1;
+                            vm &= vm - 1;
+                            lbuf[kk++] = make_uint2((uint32_t)(2 * (4 * g4 + kq) + 1), jq | (((neg >> kq) & 1u) << 31));
                         }
+                        nbuf += tot_r;
                     }
                 }
                 flush();
+                if (cur != 0xFFu) {
+                    atomicAdd(s_sum + cur, (unsigned long long)csum);
+                    atomicAdd(s_ms + cur, cms);
+                }
+                __syncwarp();
+                // the level's sums of this lane's query: Sum(-mu)(carry + count)
+                if (lane < nq) {
+                    accq += (i128)(int64_t)s_sum[lane] + (i128)C * (i128)s_ms[lane];
+                    s_sum[lane] = 0;
+                    s_ms[lane] = 0;
+                }
+                __syncwarp();
             }
             // ---- cross off p_b in the sub-segment
             cross_off(bm, cnt8, p, __shfl_sync(FULL, lr0, k), __shfl_sync(FULL, li0, k), c0, cw0, CPT, s,
@@ -396,10 +455,13 @@ __global__ void __launch_bounds__(512, 2)
             __syncwarp();
         }
     }
+    __syncthreads();  // every warp is past its levels: the leaf buffers take the per-warp totals
+    i128 *red = reinterpret_cast<i128 *>(lbuf0);
+    red[32 * warp + lane] = accq;
     __syncthreads();
     if (warp == 0 && lane < nq) {
         i128 t = 0;
-        for (uint32_t ww = 0; ww < NW; ww++) t += sacc[32 * ww + lane];
+        for (uint32_t ww = 0; ww < NW; ww++) t += red[32 * ww + lane];
         acc_add(acc, qj, ACC_HARD, t);
     }
 }
