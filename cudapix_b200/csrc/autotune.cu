@@ -3,9 +3,10 @@
 // No reference counterpart (the reference fixes its segment length and block
 // shape at compile time, src/sieve/S2_hard_device.cuh:7-22, and chooses alpha
 // by a formula, src/main.cpp:128-194).  Candidate settings are timed with
-// CUDA events by coordinate descent: the cap of the hard-leaf segment bits
-// with the threads per segment, then the alpha scale (per mille of the
-// reference alpha), then the candidate threshold of offloaded leaf sets.
+// CUDA events by coordinate descent: the alpha scale (per mille of the
+// reference alpha), the cap of the hard-leaf segment bits with the threads per
+// segment, the alpha scale again, then the candidate threshold of offloaded
+// leaf sets.
 // Results are exact under every setting; only the time changes.  Two kinds of
 // entries: one per decade of x, tuned on lone queries at the bottom and the
 // geometric middle of the decade (the plain path; used by batches of up to
@@ -59,8 +60,14 @@ static float time_batch(cpx_ctx *ctx, const std::vector<u128> &xs, uint32_t lb, 
 // (segment-bit cap, threads per segment) candidates
 static const uint32_t kCand[][2] = {{15, 128}, {16, 256}, {17, 256}, {18, 256}, {18, 512}, {19, 512}, {20, 512}};
 
+// alpha scales (per mille of the reference alpha; 0 = the reference alpha).
+// A batch whose queries share one sieve pays little for a longer sieve
+// interval, so its best alpha lies well below the reference's.
+static const uint32_t kScales[] = {0, 125, 250, 500, 2000, 4000};
+
 // Coordinate descent; the cost of a setting is the summed time of the sample
-// batches (each timed on its own).
+// batches (each timed on its own).  Alpha first, then the segment bits with
+// the threads, alpha again, then the offload threshold.
 static TuneEntry descend(cpx_ctx *ctx, const std::vector<std::vector<u128>> &samples, uint32_t off0)
 {
     auto cost = [&](uint32_t lb, uint32_t th, uint32_t off, uint32_t sc) {
@@ -71,24 +78,30 @@ static TuneEntry descend(cpx_ctx *ctx, const std::vector<std::vector<u128>> &sam
     TuneEntry b;
     b.lbits = 0;
     b.threads = ctx->hard_threads;
-    b.alpha_milli = 0;  // alpha scale; 0 = the reference alpha
+    b.alpha_milli = 0;
     b.offload = off0;
     b.ms = cost(0, b.threads, off0, 0);
+    auto alpha_pass = [&] {
+        const uint32_t cur = b.alpha_milli;
+        for (const uint32_t sc : kScales) {
+            if (sc == cur) continue;
+            const float ms = cost(b.lbits, b.threads, off0, sc);
+            if (ms < b.ms) {
+                b.ms = ms;
+                b.alpha_milli = sc;
+            }
+        }
+    };
+    alpha_pass();
     for (const auto &cd : kCand) {
-        const float ms = cost(cd[0], cd[1], off0, 0);
+        const float ms = cost(cd[0], cd[1], off0, b.alpha_milli);
         if (ms < b.ms) {
             b.ms = ms;
             b.lbits = cd[0];
             b.threads = cd[1];
         }
     }
-    for (const uint32_t sc : {500u, 2000u, 4000u}) {
-        const float ms = cost(b.lbits, b.threads, off0, sc);
-        if (ms < b.ms) {
-            b.ms = ms;
-            b.alpha_milli = sc;
-        }
-    }
+    alpha_pass();
     for (const uint32_t off : {256u, 4096u, 16384u}) {
         const float ms = cost(b.lbits, b.threads, off, b.alpha_milli);
         if (ms < b.ms) {

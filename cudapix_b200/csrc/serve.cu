@@ -215,10 +215,13 @@ static void run_lane(cpx_server *S, size_t li)
 
 // Admission data of one request: its table bounds and a device footprint
 // estimate (per (segment, level) outputs of the hard leaves, 8 bytes each,
-// plus the per-query records).
+// plus the per-query records).  A lane runs a request with the per-decade
+// tuning when its batch is small and with the batch tuning otherwise (the
+// alpha, hence y and z, differ), so the bounds cover both.
 static Req make_req(cpx_server *S, u128 x, Clock::time_point t)
 {
     const cpx_params &P = S->cfg.params;
+    const cpx_ctx *M = S->master;
     BatchReq rq;
     rq.xs = &x;
     rq.n = 1;
@@ -226,14 +229,26 @@ static Req make_req(cpx_server *S, u128 x, Clock::time_point t)
     rq.alpha_num = P.alpha_num;
     rq.alpha_den = P.alpha_den;
     rq.terms = TERM_PI;
+    rq.p2_table_limit = M->p2_table_limit;
+    rq.tune = M->tuned ? M->tune : nullptr;
     std::vector<QD> qd;
     Req r;
     bool wide = false;
     compute_needs(rq, qd, r.need, wide);
+    QD d = qd[0];
+    if (M->batch_tuned && M->batch_tune.alpha_milli && !P.alpha_num) {
+        BatchReq rb = rq;
+        rb.tune = nullptr;
+        rb.alpha_scale = M->batch_tune.alpha_milli;
+        std::vector<QD> qb;
+        TableNeed nb;
+        compute_needs(rb, qb, nb, wide);
+        r.need = merge(r.need, nb);
+        if (qb[0].z > d.z) d = qb[0];
+    }
     r.x = x;
     r.t_arrive = t;
     uint64_t foot = 4096;
-    const QD &d = qd[0];
     if (!d.direct && d.r4 > 1) {
         const uint32_t lb = P.hard_log2_bits ? P.hard_log2_bits : S->master->hard_log2_bits;
         const double nseg = (double)d.z / (double)(2ull << lb) + 1.0;
