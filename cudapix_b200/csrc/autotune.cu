@@ -57,8 +57,10 @@ static float time_batch(cpx_ctx *ctx, const std::vector<u128> &xs, uint32_t lb, 
     return best;
 }
 
-// (segment-bit cap, threads per segment) candidates
-static const uint32_t kCand[][2] = {{15, 128}, {16, 256}, {17, 256}, {18, 256}, {18, 512}, {19, 512}, {20, 512}};
+// (segment-bit cap, threads per segment) candidates; 1024 threads only in
+// batches that share the sieve (others run them as 512)
+static const uint32_t kCand[][2] = {{15, 128}, {16, 256}, {17, 256}, {18, 256}, {18, 512},
+                                    {19, 512},  {20, 512}, {19, 1024}, {20, 1024}};
 
 // alpha scales (per mille of the reference alpha; 0 = the reference alpha).
 // A batch whose queries share one sieve pays little for a longer sieve
@@ -205,7 +207,7 @@ void tune_load(cpx_ctx *ctx, const char *path)
                    "\"decade\": %u, \"alpha_scale_milli\": %u, \"log2_bits\": %u, \"threads\": %u, "
                    "\"offload_min\": %u, \"ms\": %lf",
                    &e, &am, &lb, &th, &off, &ms) != 6 ||
-            (e >= kTuneDecades && e != kBatchEntry) || (th != 128 && th != 256 && th != 512) ||
+            (e >= kTuneDecades && e != kBatchEntry) || (th != 128 && th != 256 && th != 512 && th != 1024) ||
             (lb && (lb < 15 || lb > 20))) {
             fclose(f);
             fail(CPX_EINVAL, std::string("malformed tuning entry in ") + path);

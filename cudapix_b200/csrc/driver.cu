@@ -216,7 +216,7 @@ static void choose_lbits(cpx_ctx *ctx, std::vector<QD> &qd, uint32_t c, uint32_t
 static uint32_t choose_shared(cpx_ctx *ctx, const std::vector<QD> &qd, const std::vector<uint32_t> &order,
                               uint32_t threads, uint32_t forced, uint32_t cap_all, uint32_t &gsize)
 {
-    const uint32_t minb = (threads >= 512) ? 16 : (threads >= 256 ? 15 : 14);
+    const uint32_t minb = (threads >= 1024) ? 17 : (threads >= 512) ? 16 : (threads >= 256 ? 15 : 14);
     const uint32_t cap = std::max(minb, std::min<uint32_t>(forced ? forced : (cap_all ? cap_all : ctx->hard_log2_bits), 20));
     uint32_t lb = minb;
     while (lb < cap && (2ull << lb) < qd[order[0]].z + 1) lb++;
@@ -470,7 +470,8 @@ void run_batch(cpx_ctx *ctx, const BatchReq &rq)
         if (btune->offload) offload0 = btune->offload;
         if (!lbits_cap) lbits_cap = btune->lbits;
     }
-    if (threads != 128 && threads != 256 && threads != 512) fail(CPX_EINVAL, "hard threads must be 128/256/512");
+    if (threads != 128 && threads != 256 && threads != 512 && threads != 1024)
+        fail(CPX_EINVAL, "hard threads must be 128/256/512/1024");
     bool any_p2win = false;
     for (const QD &d : qd) any_p2win |= d.p2win != 0;
     st.roots_ms = ms_since(clk);
@@ -504,6 +505,7 @@ void run_batch(cpx_ctx *ctx, const BatchReq &rq)
             sh_lbits = choose_shared(ctx, qd, horder, threads, rq.lbits, lbits_cap, gsize);
             for (uint32_t i : horder) qd[i].lbits = sh_lbits;
         } else {
+            threads = std::min<uint32_t>(threads, 512);  // 1024-thread blocks: the shared sieve only
             choose_lbits(ctx, qd, c, threads, rq.lbits, lbits_cap, tune);
         }
     }

@@ -36,12 +36,16 @@ __host__ __device__ __forceinline__ size_t counts_smem(uint32_t lbits)
     return L / 8 + (((L / 128) + 15) & ~size_t(15));
 }
 
+// gathered leaves per warp: 256, or 128 for 32 warps (2^20 bits, 1024
+// threads, fit 227 KB of shared memory)
+__host__ __device__ __forceinline__ uint32_t leaf_cap(uint32_t threads) { return threads >= 1024 ? 128u : kLeafBuf; }
+
 // shared memory of k_hard_shared
 __host__ __device__ __forceinline__ size_t shared_smem(uint32_t lbits, uint32_t threads)
 {
     size_t o = counts_smem(lbits);
-    o += threads * 4;                      // lane prefixes
-    o += (threads / 32) * kLeafBuf * 8;    // gathered leaves: m, query | (mu(m) = -1) << 31
+    o += threads * 4;                              // lane prefixes
+    o += (threads / 32) * leaf_cap(threads) * 8;   // gathered leaves: m, query | (mu(m) = -1) << 31
     o += (threads / 32) * kGroupMax * 16;  // x/p of the group's queries, per warp
     o += (threads / 32) * kGroupMax * 12;  // per-warp, per-query level sums and Sum(-mu)
     return o;
@@ -58,7 +62,7 @@ template <class XT> __device__ __forceinline__ XT shfl_xt(XT v, uint32_t src)
 // (1) One CTA per segment: survivors of level b-1 of each warp sub-segment w,
 // for every level b the segment sieves, into row b at w - NW * first(b), where
 // first(b) = p_b^2 / span is the level's first segment.
-__global__ void __launch_bounds__(512, 2) k_sieve_counts(uint64_t nseg, uint32_t lbits, u128 xmax, uint64_t r4max,
+__global__ void __launch_bounds__(1024, 1) k_sieve_counts(uint64_t nseg, uint32_t lbits, u128 xmax, uint64_t r4max,
                                                        uint32_t c, const uint32_t *__restrict__ P, uint32_t np,
                                                        const uint64_t *__restrict__ lvl_off, uint32_t nlv,
                                                        uint64_t *__restrict__ cnt)
@@ -165,7 +169,7 @@ __global__ void __launch_bounds__(1024) k_carry_scan(uint32_t nlv, uint32_t c, u
 // the query changes; at the end of the level lane j folds slot j into its
 // 128-bit total as sum + carry * Sum(-mu).
 template <class XT>
-__global__ void __launch_bounds__(512, 2)
+__global__ void __launch_bounds__(1024, 1)
     k_hard_shared(const QD *__restrict__ qd, const HardGroup *__restrict__ grp, const uint64_t *__restrict__ pre_grp,
                   uint32_t ngrp, uint64_t total, uint32_t lbits, uint32_t c, const uint32_t *__restrict__ P,
                   uint32_t np, const int32_t *__restrict__ MU, const cpx_pient *__restrict__ Tpi,
@@ -200,8 +204,9 @@ __global__ void __launch_bounds__(512, 2)
     uint32_t *wl = reinterpret_cast<uint32_t *>(sp + o) + 32 * warp;  // this warp's lane prefixes
     o += T * 4;
     uint2 *lbuf0 = reinterpret_cast<uint2 *>(sp + o);
-    uint2 *lbuf = lbuf0 + kLeafBuf * warp;
-    o += NW * kLeafBuf * 8;
+    const uint32_t cap = leaf_cap(T);
+    uint2 *lbuf = lbuf0 + cap * warp;
+    o += NW * cap * 8;
     XT *s_xp = reinterpret_cast<XT *>(sp + o) + 32 * warp;  // x/p of each query at the current level
     o += NW * 32 * 16;
     unsigned long long *s_sum = reinterpret_cast<unsigned long long *>(sp + o) + 32 * warp;
@@ -385,7 +390,7 @@ __global__ void __launch_bounds__(512, 2)
                         }
                         uint32_t off;
                         const uint32_t tot_r = warp_place((uint32_t)__popcll(qb), lane, off);
-                        if (tot_r > kLeafBuf) {  // a dense round: each lane answers its own word
+                        if (tot_r > cap) {  // a dense round: each lane answers its own word
                             const XT xq = s_xp[jq];
                             while (qb) {
                                 const int jb = __ffsll((long long)qb) - 1;
@@ -394,7 +399,7 @@ __global__ void __launch_bounds__(512, 2)
                             }
                             continue;
                         }
-                        if (nbuf + tot_r > kLeafBuf) flush();
+                        if (nbuf + tot_r > cap) flush();
                         uint32_t kk = nbuf + off;
                         while (qb) {
                             const int jb = __ffsll((long long)qb) - 1;
@@ -425,7 +430,7 @@ __global__ void __launch_bounds__(512, 2)
                         }
                         uint32_t off;
                         const uint32_t tot_r = warp_place((uint32_t)__popc(vm), lane, off);
-                        if (nbuf + tot_r > kLeafBuf) flush();
+                        if (nbuf + tot_r > cap) flush();
                         uint32_t kk = nbuf + off;
                         while (vm) {
                             const int kq = __ffs(vm) - 1;

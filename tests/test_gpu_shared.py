@@ -60,7 +60,8 @@ def test_shared_equals_per_query_log_uniform(own, cpx):
     assert got == ref
 
 
-@pytest.mark.parametrize("lbits,threads", [(15, 128), (16, 256), (18, 256), (18, 512), (20, 512)])
+@pytest.mark.parametrize("lbits,threads", [(15, 128), (16, 256), (18, 256), (18, 512), (20, 512), (17, 1024),
+                                           (20, 1024)])
 def test_shared_segment_sizes(own, cpx, lbits, threads):
     rng = np.random.default_rng(lbits * 1000 + threads)
     xs = [int(10**e) for e in rng.uniform(9, 12.5, 150)]
@@ -77,7 +78,7 @@ def test_shared_offload_thresholds(own, cpx, orc, off):
     xs = [10**10, 10**11, 2 * 10**11 + 7, 10**12, 10**12 + 39, 3 * 10**12, 10**11 + 1, 4 * 10**10 + 3, 10**13]
     own.set_hard_shared(2)
     own.set_hard_offload(off)
-    for th in (128, 256, 512):
+    for th in (128, 256, 512, 1024):
         got = cpx.terms_batch(xs, hard_threads=th, ctx=own)
         for x, t in zip(xs, got):
             assert t["hard"] == oracle_hard(orc, x, t["y"]), (off, th, x)
@@ -110,6 +111,15 @@ def test_shared_pi_pow10(own, cpx, golden):
     own.set_hard_shared(2)
     xs = [10**k for k in range(1, 16)]
     assert cpx.pi_batch(xs, ctx=own) == [golden["pi_pow10"][str(k)] for k in range(1, 16)]
+
+
+def test_1024_threads_outside_the_shared_sieve(own, cpx, orc):
+    """A batch that does not share the sieve runs 1024-thread requests as 512."""
+    own.set_hard_shared(0)
+    xs = [10**11, 10**12 + 39]
+    got = cpx.terms_batch(xs, hard_threads=1024, ctx=own)
+    for x, t in zip(xs, got):
+        assert t["hard"] == oracle_hard(orc, x, t["y"]), x
 
 
 def test_shared_mode_argument(own, cpx):
