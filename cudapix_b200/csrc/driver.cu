@@ -233,6 +233,31 @@ static uint32_t choose_shared(cpx_ctx *ctx, const std::vector<QD> &qd, const std
     return lb;
 }
 
+// Alpha scales of a batch under the batch tuning.  Its alpha (tuned on a
+// sample batch) pays off for queries that share their sieve with others; a
+// query with fewer than 16 companions within half a decade of x sieves
+// mostly alone and takes its decade's tuned scale (the reference alpha when
+// untuned).
+static std::vector<uint32_t> batch_alpha_scales(const u128 *xs, uint32_t Q, uint32_t batch_sc, const TuneEntry *tune)
+{
+    std::vector<std::pair<double, uint32_t>> lx(Q);
+    for (uint32_t i = 0; i < Q; i++) lx[i] = {std::log10((double)xs[i]), i};
+    std::sort(lx.begin(), lx.end());
+    std::vector<uint32_t> sc(Q);
+    size_t a = 0, b = 0;
+    for (size_t k = 0; k < Q; k++) {
+        while (lx[k].first - lx[a].first > 0.5) a++;
+        while (b < Q && lx[b].first - lx[k].first <= 0.5) b++;
+        uint32_t v = batch_sc;
+        if (b - a < 17) {
+            const uint32_t e = decade_of(xs[lx[k].second]);
+            v = (tune && e < kTuneDecades && tune[e].alpha_milli) ? tune[e].alpha_milli : 1000;
+        }
+        sc[lx[k].second] = v;
+    }
+    return sc;
+}
+
 // Captures the launches of one batch into a CUDA graph and runs it.  The
 // executable graph is kept in the context: a later batch with the same kernel
 // sequence only updates its nodes' parameters (grids, pointers) in place, a
@@ -300,7 +325,7 @@ void compute_needs(const BatchReq &rq, std::vector<QD> &qd, TableNeed &need, boo
         uint64_t y = rq.ys ? rq.ys[i] : 0;
         if (mask == TERM_PI) {
             if (!y) {
-                uint32_t sc = rq.alpha_scale;
+                uint32_t sc = (rq.alpha_scales && rq.alpha_scales[i]) ? rq.alpha_scales[i] : rq.alpha_scale;
                 if (!sc && rq.tune) sc = rq.tune[decade_of(x)].alpha_milli;
                 if (!rq.alpha_num && sc) {
                     const uint64_t am = std::max<uint64_t>(1000, (uint64_t)alpha_milli(x) * sc / 1000);
@@ -445,11 +470,15 @@ void run_batch(cpx_ctx *ctx, const BatchReq &rq)
     std::vector<QD> qd;
     TableNeed need;
     bool wide = false;
+    std::vector<uint32_t> ascale;
     {
         BatchReq r2 = rq;
         r2.p2_table_limit = ctx->p2_table_limit;
         r2.tune = tune;
-        if (btune && !r2.alpha_scale) r2.alpha_scale = btune->alpha_milli;
+        if (btune && !r2.alpha_scale && !r2.alpha_num && !r2.alpha_scales && btune->alpha_milli) {
+            ascale = batch_alpha_scales(rq.xs, Q, btune->alpha_milli, ctx->tuned ? ctx->tune : nullptr);
+            r2.alpha_scales = ascale.data();
+        }
         compute_needs(r2, qd, need, wide);
     }
     // threads per segment, offload threshold and segment-bit cap: the tuned

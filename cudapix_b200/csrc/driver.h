@@ -28,6 +28,7 @@ struct BatchReq {
     i128 *out_terms = nullptr;              // 7 per query: P2 ord triv easy hard pi_y pi
     uint64_t *out_y = nullptr;
     uint32_t alpha_scale = 0;         // per mille of the reference alpha (0: 1000) when alpha_num = 0
+    const uint32_t *alpha_scales = nullptr;  // per query, overriding alpha_scale where nonzero
     uint32_t lbits_cap = 0;           // cap of the hard-leaf segment bits (0: context default)
     const TuneEntry *tune = nullptr;  // per-decade alpha scale when alpha_num = alpha_scale = 0
     uint64_t seg_lo = 0, seg_hi = 0;  // one query's hard-leaf segments [seg_lo, seg_hi) (0, 0: all)

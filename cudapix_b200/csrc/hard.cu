@@ -92,6 +92,7 @@ __global__ void __launch_bounds__(512, 2) k_hard(const QD *__restrict__ qd, uint
     uint32_t tot = __reduce_add_sync(FULL, cnt0);  // survivors of this warp's sub-segment
     __syncwarp();
 
+    const BoundDiv bd_lo = bound_div(lo_w), bd_hi = bound_div(hi_w);
     auto sub_count = [&](uint64_t uu) -> uint32_t { return sub_survivors(uu, lo_w, wl, cnt8, bm, CPT, s, warp); };
 
     int64_t S = 0;       // this lane's share of the hard sum (survivor counts within sub-segments)
@@ -105,7 +106,7 @@ __global__ void __launch_bounds__(512, 2) k_hard(const QD *__restrict__ qd, uint
         lv.mlo = lv.mhi = lv.r0 = 0;
         lv.i0 = 0xFFFFFFFFu;
         lv.xp = 0;
-        if (lane < nl) level_params<XT>(lv, x, y, P[gb + lane - 1], lo_w, hi_w);
+        if (lane < nl) level_params<XT>(lv, x, y, P[gb + lane - 1], lo_w, hi_w, bd_lo, bd_hi);
         const uint32_t lp = lv.p, lmlo = lv.mlo, lmhi = lv.mhi, lr0 = lv.r0, li0 = lv.i0;
         const XT lxp = lv.xp;
         LvlOut mine = {0, 0, 0xFFFFFFFFu, 0};

@@ -234,6 +234,7 @@ __global__ void __launch_bounds__(1024, 1)
     const uint64_t w = seg * NW + warp;
     const size_t stride = snap_stride(lbits_sub);
     auto sub_count = [&](uint64_t uu) -> uint32_t { return sub_survivors(uu, lo_w, wl, cnt8, bm, CPT, s, warp); };
+    const BoundDiv bd_lo = bound_div(lo_w), bd_hi = bound_div(hi_w);
 
     for (uint32_t gb = c + 1; gb <= B; gb += 32) {
         const uint32_t nl = min(32u, B - gb + 1);
@@ -255,11 +256,11 @@ __global__ void __launch_bounds__(1024, 1)
             if (lane < nq && lo_w <= zj && hi_w > pp && (u128)p * yj * hi_w > (u128)xj) {
                 xp = cpx_qdiv(xj, (uint64_t)p);
                 uint64_t a = cpx_udiv_leaf(yj, p);
-                const XT t1 = cpx_qdiv(xp, hi_w);
+                const XT t1 = div_bound(xp, bd_hi);
                 if (t1 > (XT)a) a = (uint64_t)t1;
                 uint64_t e = yj;
                 if (lo_w) {
-                    const XT t2 = cpx_qdiv(xp, lo_w);
+                    const XT t2 = div_bound(xp, bd_lo);
                     if (t2 < (XT)e) e = (uint64_t)t2;
                 }
                 const XT t3 = cpx_qdiv(xp, pp);  // hard leaves only: m <= x/p^3

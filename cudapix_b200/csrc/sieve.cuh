@@ -171,6 +171,33 @@ __device__ __forceinline__ void cross_params(uint64_t p, uint64_t lo_w, uint64_t
     i0 = (m < hi_w) ? (uint32_t)((m - lo_w - 1) >> 1) : 0xFFFFFFFFu;
 }
 
+// Quotients by a warp's sub-segment bounds.  A bound d at or above 2^32 would
+// take the 64-bit hardware division; with rd = 1/d (double, once per warp) the
+// quotient n/d < 2^32 is the truncated product n * rd, whose relative error
+// (three roundings, at most 3 * 2^-53) leaves it within 1 of floor(n/d), fixed
+// by the sign and size of the exact remainder n - q d.
+struct BoundDiv {
+    uint64_t d;
+    double rd;
+};
+__device__ __forceinline__ BoundDiv bound_div(uint64_t d)
+{
+    BoundDiv b;
+    b.d = d;
+    b.rd = (d >> 32) ? 1.0 / (double)d : 0.0;
+    return b;
+}
+template <class XT> __device__ __forceinline__ XT div_bound(XT n, const BoundDiv &b)
+{
+    if (!(b.d >> 32) || ((u128)n >> 64)) return cpx_qdiv(n, b.d);
+    const uint64_t n64 = (uint64_t)n;
+    uint64_t q = __double2ull_rz(__dmul_rn(__ull2double_rn(n64), b.rd));
+    const int64_t r = (int64_t)(n64 - q * b.d);
+    if (r < 0) q--;
+    else if ((uint64_t)r >= b.d) q++;
+    return (XT)q;
+}
+
 // Parameters of one level (p = p_b) for one warp's sub-segment [lo_w, hi_w):
 // xp = x/p, the candidate range (mlo, mhi] of m (m > y/p, u = xp/m in the
 // sub-segment, m <= x/p^3 for a hard leaf), the residue of lo_w + 1 mod p and
@@ -182,15 +209,16 @@ template <class XT> struct LvlPar {
 };
 
 template <class XT>
-static __device__ __noinline__ void level_params(LvlPar<XT> &o, XT x, uint64_t y, uint64_t p, uint64_t lo_w, uint64_t hi_w)
+static __device__ __noinline__ void level_params(LvlPar<XT> &o, XT x, uint64_t y, uint64_t p, uint64_t lo_w,
+                                                uint64_t hi_w, const BoundDiv &bl, const BoundDiv &bh)
 {
     const XT xp = cpx_qdiv(x, p);
     uint64_t mlo = y / p;
-    const XT t1 = cpx_qdiv(xp, hi_w);
+    const XT t1 = div_bound(xp, bh);
     if (t1 > (XT)mlo) mlo = (uint64_t)t1;
     uint64_t mhi = y;
     if (lo_w) {
-        const XT t2 = cpx_qdiv(xp, lo_w);
+        const XT t2 = div_bound(xp, bl);
         if (t2 < (XT)mhi) mhi = (uint64_t)t2;
     }
     const XT t3 = cpx_qdiv(xp, p * p);  // hard leaves only: m <= x/p^3
@@ -211,8 +239,8 @@ __device__ __forceinline__ uint32_t cross_off(uint32_t *bm, uint8_t *cnt8, uint3
                                               uint32_t lane, uint32_t Lw)
 {
     uint32_t cleared = 0;
-    if (p < 128) {
-        // each lane masks its own words; p < 32 has several multiples per word
+    if (p < 32) {
+        // each lane masks its own words: several multiples per word
         const uint32_t Mp = every_pth_bit(p);
         const uint32_t stp = 64u % p;
         uint32_t r = (r0 + (64u * (cw0 * 4)) % p) % p;  // first owned word of the sub-segment
@@ -233,6 +261,25 @@ __device__ __forceinline__ uint32_t cross_off(uint32_t *bm, uint8_t *cnt8, uint3
                 reinterpret_cast<uint4 *>(bm)[swz(c0 + j, s)] = make_uint4(a4[0], a4[1], a4[2], a4[3]);
             }
             cleared += cj;
+        }
+    } else if (p < 128) {
+        // at most one multiple per word: each lane jumps from multiple to
+        // multiple inside its own chunks (its counters only)
+        if (i0 != 0xFFFFFFFFu) {
+            const uint32_t b0 = cw0 * 128, b1 = b0 + CPT * 128;  // the lane's bits of the sub-segment
+            uint32_t i = i0;
+            if (b0 > i0) i = i0 + ((b0 - i0 + p - 1) / p) * p;
+            for (; i < b1; i += p) {
+                const uint32_t w = i >> 5, bit = 1u << (i & 31);
+                const uint32_t ch = base_ch + (w >> 2);
+                uint32_t *pw = bm + ((swz(ch, s) << 2) | (w & 3));
+                const uint32_t old = *pw;
+                if (old & bit) {
+                    *pw = old & ~bit;
+                    cleared++;
+                    cnt8[ch] = (uint8_t)(cnt8[ch] - 1);
+                }
+            }
         }
     } else if (i0 != 0xFFFFFFFFu) {
         // p >= 128: the lanes of one step clear bits p apart, so they touch

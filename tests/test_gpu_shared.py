@@ -125,3 +125,20 @@ def test_1024_threads_outside_the_shared_sieve(own, cpx, orc):
 def test_shared_mode_argument(own, cpx):
     with pytest.raises(cpx.CpxError):
         own.set_hard_shared(3)
+
+
+def test_batch_alpha_only_for_queries_with_companions(own, cpx):
+    """Under the batch tuning a query with few neighbours in x (here one at
+    1e16 among forty in [1e10, 1e11]) keeps its decade's tuned alpha, so it
+    does not sieve a long interval alone; the results are the same as with
+    one sieve per query."""
+    import os
+
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    own.tune_load(os.path.join(root, "cudapix_b200", "tuning", "b200.json"))
+    xs = [int(10**e) for e in np.random.default_rng(4).uniform(10, 11, 40)] + [10**16 + 1]
+    got = cpx.terms_batch(xs, ctx=own)
+    alone = cpx.terms_batch([10**16 + 1], ctx=own)[0]  # plain path: the decade's tuning
+    assert got[-1]["y"] == alone["y"] and got[-1]["pi"] == alone["pi"]
+    own.set_hard_shared(0)
+    assert cpx.terms_batch(xs, ctx=own) == got
