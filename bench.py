@@ -249,7 +249,9 @@ def barrier(world):
 def arm_config(args, world):
     """The workload both arms report (the reference arm runs it on the host cores)."""
     return {"workload": "batch4096: x = floor(10^e), e ~ U[9,14], numpy default_rng(0)",
-            "queries": args.queries, "c": 6, "alpha": "reference alpha(x)",
+            "queries": args.queries, "c": 6,
+            "alpha": "tuning table: 1/8 of the reference alpha(x) (y >= icbrt x) for queries with 16 or more "
+                     "others within half a decade of x, else the decade's tuned alpha",
             "l2": "flushed before every timed step (256 MiB write)",
             "tuning": os.path.relpath(TUNING, ROOT) if os.path.exists(TUNING) else None,
             "parallelism": f"replicas x{world}"}
@@ -431,13 +433,15 @@ def main():
     hb = hard_bytes[-1]
     hs = statistics.median(hard_ms) / 1000.0
     tr = profile_traffic()
-    roof = {"bound": "hbm", "kernel": "k_hard (special-leaf phi sieve)", "achieved": (hb / hs) / 1e9 if hs else None,
+    roof = {"bound": "hbm", "kernel": "k_hard_shared (batch-shared special-leaf phi sieve)",
+            "achieved": (hb / hs) / 1e9 if hs else None,
             "peak": hbm, "unit": "GB/s", "frac": ((hb / hs) / 1e9) / hbm if hs else None,
-            "peak_kind": kind, "traffic": tr.get("k_hard_dram_bytes_per_launch") if tr else None,
-            "alu_pipe_frac_ncu": tr.get("k_hard_alu_pipe_frac") if tr else None,
-            "note": "achieved = S2 bitmap bytes (one pass of the segment bitmap per active prime per segment) / "
-                    "hard-leaf kernels' duration; these passes run in shared memory and the kernel is integer-ALU "
-                    "bound (alu_pipe_frac_ncu, profiles/k_hard_batch4096.md), so the HBM fraction is a proxy"}
+            "peak_kind": kind, "traffic": tr.get("dram_bytes_per_launch") if tr else None,
+            "alu_pipe_frac_ncu": tr.get("alu_pipe_frac") if tr else None,
+            "note": "achieved = segment-bitmap bytes the sieve passes over (the counting sweep and every group "
+                    "unit: one pass per level per segment) / duration of the hard-leaf kernels (CUDA events); "
+                    "the passes run in shared memory and the kernel is integer-ALU bound (alu_pipe_frac_ncu, "
+                    "profiles/k_hard_shared_batch4096.md), so the HBM fraction is a proxy"}
     cpu = None if args.no_cpu else cpu_baseline(xs, args.cpu_budget)
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,

@@ -501,6 +501,9 @@ void run_batch(cpx_ctx *ctx, const BatchReq &rq)
     }
     if (threads != 128 && threads != 256 && threads != 512 && threads != 1024)
         fail(CPX_EINVAL, "hard threads must be 128/256/512/1024");
+    // serving lanes run their batches side by side: a 1024-thread sieve block
+    // fills an SM and would keep the other lanes' blocks off it
+    if (ctx->tables_borrowed) threads = std::min<uint32_t>(threads, 512);
     bool any_p2win = false;
     for (const QD &d : qd) any_p2win |= d.p2win != 0;
     st.roots_ms = ms_since(clk);

@@ -157,6 +157,94 @@ __global__ void __launch_bounds__(1024) k_carry_scan(uint32_t nlv, uint32_t c, u
     }
 }
 
+// Candidates (mlo, mhi] of one query at level p in a warp's sub-segment
+// [lo_w, hi_w), and x/p.  Out of line (instruction-cache footprint of the
+// level loop); called by the lanes whose query passes the cheap filter.
+template <class XT> struct SlotPar {
+    XT xp;
+    uint32_t mlo, mhi;
+    bool act;
+};
+template <class XT>
+static __device__ __noinline__ void slot_params(SlotPar<XT> &o, XT xj, uint64_t yj, uint64_t p, uint64_t pp,
+                                                uint64_t lo_w, const BoundDiv &bl, const BoundDiv &bh)
+{
+    const XT xp = cpx_qdiv(xj, p);
+    uint64_t a = cpx_udiv_leaf(yj, p);
+    const XT t1 = div_bound(xp, bh);
+    if (t1 > (XT)a) a = (uint64_t)t1;
+    uint64_t e = yj;
+    if (lo_w) {
+        const XT t2 = div_bound(xp, bl);
+        if (t2 < (XT)e) e = (uint64_t)t2;
+    }
+    const XT t3 = cpx_qdiv(xp, pp);  // hard leaves only: m <= x/p^3
+    if (t3 < (XT)e) e = (uint64_t)t3;
+    o.xp = xp;
+    o.mlo = (uint32_t)a;
+    o.mhi = (uint32_t)(e > a ? e : a);
+    o.act = e > ((pp > yj && p > a) ? p : a);
+}
+
+// Hands the heavy leaf sets of one (sub-segment, level) to k_hard_leaves: one
+// snapshot of the sub-segment (bitmap and chunk prefixes) for all of them,
+// one job per set.  Every lane calls; returns whether this lane's set went
+// (a set that finds no job slot left is answered in the sieve).  Rare path,
+// out of line.
+template <class XT>
+static __device__ __noinline__ bool offload_sets(bool off_j, uint32_t lane, uint32_t qj, uint32_t b, uint32_t p,
+                                                 bool prime_j, uint32_t qa_j, uint32_t mlo, uint32_t mhi,
+                                                 uint64_t work, uint64_t lo_w, uint64_t C, XT xp, const uint32_t *bm,
+                                                 const uint8_t *cnt8, uint32_t cw0, uint32_t c0, uint32_t CPT, int s,
+                                                 uint32_t pre, HardJob *__restrict__ jobs,
+                                                 unsigned int *__restrict__ njobs, uint64_t *__restrict__ job_units,
+                                                 unsigned char *__restrict__ snap, unsigned int *__restrict__ nsnap,
+                                                 uint32_t max_jobs, uint32_t lbits_sub)
+{
+    uint32_t snap_k = 0xFFFFFFFFu;
+    for (unsigned offm = __ballot_sync(FULL, off_j); offm; offm &= offm - 1) {
+        const uint32_t j = __ffs(offm) - 1;
+        unsigned int jb = 0, sn = snap_k;
+        if (lane == 0) {
+            jb = atomicAdd(njobs, 1u);
+            if (jb < max_jobs && sn == 0xFFFFFFFFu) sn = atomicAdd(nsnap, 1u);
+        }
+        jb = __shfl_sync(FULL, jb, 0);
+        sn = __shfl_sync(FULL, sn, 0);
+        // (a job slot taken without a snapshot keeps 0 units)
+        if (jb < max_jobs && sn < max_jobs) {
+            if (snap_k == 0xFFFFFFFFu) {
+                snap_k = sn;
+                uint4 *sb = reinterpret_cast<uint4 *>(snap + (size_t)sn * snap_stride(lbits_sub));
+                uint32_t *spre = reinterpret_cast<uint32_t *>(sb + ((size_t(1) << lbits_sub) >> 7));
+                snapshot_chunks(sb, spre, bm, cnt8, cw0, c0, CPT, s, pre);
+            }
+            if (lane == j) {
+                HardJob J;
+                J.q = qj;
+                J.b = b;
+                J.p = p;
+                J.kind = prime_j ? 1u : 0u;
+                J.mlo = prime_j ? qa_j : mlo;
+                J.mhi = mhi;
+                J.lo = lo_w;
+                J.slot = ~0ull;
+                J.nunits = prime_j ? (work / 8 + kJobWords - 1) / kJobWords
+                                   : ((((uint64_t)mhi - 1) >> 3) - (((uint64_t)mlo + 1) >> 3) + kJobGroups) / kJobGroups;
+                J.carry = C;
+                J.snap = sn;
+                J.pad = 0;
+                J.xp = (u128)xp;
+                jobs[jb] = J;
+                job_units[jb] = J.nunits;
+            }
+        } else if (lane == j) {
+            off_j = false;  // no slot left: answered here
+        }
+    }
+    return off_j;
+}
+
 // (3) One CTA per (group, segment).  Per level, the lanes hold one query
 // each: its x/p and candidate range in the warp's sub-segment.  The warp then
 // walks the candidates of all the group's queries as one sequence (pi-table
@@ -232,7 +320,6 @@ __global__ void __launch_bounds__(1024, 1)
     presieve(bm, cnt8, P, c, lo, c0, CPT, s);
     __syncwarp();
     const uint64_t w = seg * NW + warp;
-    const size_t stride = snap_stride(lbits_sub);
     auto sub_count = [&](uint64_t uu) -> uint32_t { return sub_survivors(uu, lo_w, wl, cnt8, bm, CPT, s, warp); };
     const BoundDiv bd_lo = bound_div(lo_w), bd_hi = bound_div(hi_w);
 
@@ -250,25 +337,15 @@ __global__ void __launch_bounds__(1024, 1)
             // Candidates (mlo, mhi] of this lane's query in the warp's
             // sub-segment.  None unless some u in it satisfies u <= z,
             // u >= p^2 and x/(p hi_w) < y (else m > y).
-            XT xp = 0;
-            uint32_t mlo = 0, mhi = 0;
-            bool act = false;
-            if (lane < nq && lo_w <= zj && hi_w > pp && (u128)p * yj * hi_w > (u128)xj) {
-                xp = cpx_qdiv(xj, (uint64_t)p);
-                uint64_t a = cpx_udiv_leaf(yj, p);
-                const XT t1 = div_bound(xp, bd_hi);
-                if (t1 > (XT)a) a = (uint64_t)t1;
-                uint64_t e = yj;
-                if (lo_w) {
-                    const XT t2 = div_bound(xp, bd_lo);
-                    if (t2 < (XT)e) e = (uint64_t)t2;
-                }
-                const XT t3 = cpx_qdiv(xp, pp);  // hard leaves only: m <= x/p^3
-                if (t3 < (XT)e) e = (uint64_t)t3;
-                mlo = (uint32_t)a;
-                mhi = (uint32_t)(e > a ? e : a);
-                act = e > ((pp > yj && p > a) ? (uint64_t)p : a);
-            }
+            SlotPar<XT> sp_j;
+            sp_j.xp = 0;
+            sp_j.mlo = sp_j.mhi = 0;
+            sp_j.act = false;
+            if (lane < nq && lo_w <= zj && hi_w > pp && (u128)p * yj * hi_w > (u128)xj)
+                slot_params<XT>(sp_j, xj, yj, p, pp, lo_w, bd_lo, bd_hi);
+            const XT xp = sp_j.xp;
+            const uint32_t mlo = sp_j.mlo, mhi = sp_j.mhi;
+            const bool act = sp_j.act;
             const unsigned bal = __ballot_sync(FULL, act);
             if (bal) {
                 // lane prefixes of the sub-segment from the chunk counters
@@ -288,48 +365,10 @@ __global__ void __launch_bounds__(1024, 1)
                                    : ((((uint64_t)mhi - 1) >> 1) - (((uint64_t)mlo + 1) >> 1) + 1);
                 // heavy sets to k_hard_leaves, one snapshot for the warp's level
                 bool off_j = act && max_jobs && offload_min && work >= offload_min;
-                uint32_t snap_k = 0xFFFFFFFFu;
-                for (unsigned offm = __ballot_sync(FULL, off_j); offm; offm &= offm - 1) {
-                    const uint32_t j = __ffs(offm) - 1;
-                    unsigned int jb = 0, sn = snap_k;
-                    if (lane == 0) {
-                        jb = atomicAdd(njobs, 1u);
-                        if (jb < max_jobs && sn == 0xFFFFFFFFu) sn = atomicAdd(nsnap, 1u);
-                    }
-                    jb = __shfl_sync(FULL, jb, 0);
-                    sn = __shfl_sync(FULL, sn, 0);
-                    // (a job slot taken without a snapshot keeps 0 units)
-                    if (jb < max_jobs && sn < max_jobs) {
-                        if (snap_k == 0xFFFFFFFFu) {
-                            snap_k = sn;
-                            uint4 *sb = reinterpret_cast<uint4 *>(snap + (size_t)sn * stride);
-                            uint32_t *spre = reinterpret_cast<uint32_t *>(sb + ((size_t(1) << lbits_sub) >> 7));
-                            snapshot_chunks(sb, spre, bm, cnt8, cw0, c0, CPT, s, wl[lane]);
-                        }
-                        if (lane == j) {
-                            HardJob J;
-                            J.q = qj;
-                            J.b = b;
-                            J.p = p;
-                            J.kind = prime_j ? 1u : 0u;
-                            J.mlo = prime_j ? qa_j : mlo;
-                            J.mhi = mhi;
-                            J.lo = lo_w;
-                            J.slot = ~0ull;
-                            J.nunits = prime_j ? (work / 8 + kJobWords - 1) / kJobWords
-                                               : ((((uint64_t)mhi - 1) >> 3) - (((uint64_t)mlo + 1) >> 3) + kJobGroups) /
-                                                     kJobGroups;
-                            J.carry = C;
-                            J.snap = sn;
-                            J.pad = 0;
-                            J.xp = (u128)xp;
-                            jobs[jb] = J;
-                            job_units[jb] = J.nunits;
-                        }
-                    } else if (lane == j) {
-                        off_j = false;  // no slot left: answered here
-                    }
-                }
+                if (__any_sync(FULL, off_j))
+                    off_j = offload_sets<XT>(off_j, lane, qj, b, p, prime_j, qa_j, mlo, mhi, work, lo_w, C, xp, bm, cnt8,
+                                             cw0, c0, CPT, s, wl[lane], jobs, njobs, job_units, snap, nsnap, max_jobs,
+                                             lbits_sub);
                 // running sums of the query of this lane's last leaf
                 uint32_t cur = 0xFFu;
                 int64_t csum = 0;
