@@ -258,6 +258,25 @@ static std::vector<uint32_t> batch_alpha_scales(const u128 *xs, uint32_t Q, uint
     return sc;
 }
 
+// Bytes of the counting sweep's carry rows for the queries `order` of a
+// shared sieve with segments of 2^lbits odd numbers and `threads` per block.
+static uint64_t carry_row_bytes(const std::vector<QD> &qd, const std::vector<uint32_t> &order,
+                                const std::vector<uint32_t> &hP, uint32_t lbits, uint32_t threads, uint32_t c)
+{
+    const uint64_t span = 2ull << lbits;
+    u128 xmax = 0;
+    uint64_t r4max = 0, nseg = 0;
+    for (uint32_t i : order) {
+        xmax = std::max(xmax, qd[i].x);
+        r4max = std::max(r4max, qd[i].r4);
+        nseg = std::max(nseg, (qd[i].z + 1 + span - 1) / span);
+    }
+    const uint64_t nbm = host_pi(hP, r4max);
+    uint64_t rows = 0;
+    for (uint64_t b = c + 1; b <= nbm; b++) rows += segments_at_level(xmax, span, hP[b - 1], 0, nseg);
+    return rows * (threads / 32) * 8;
+}
+
 // Captures the launches of one batch into a CUDA graph and runs it.  The
 // executable graph is kept in the context: a later batch with the same kernel
 // sequence only updates its nodes' parameters (grids, pointers) in place, a
@@ -471,11 +490,13 @@ void run_batch(cpx_ctx *ctx, const BatchReq &rq)
     TableNeed need;
     bool wide = false;
     std::vector<uint32_t> ascale;
+    bool batch_alpha = btune && !rq.alpha_scale && !rq.alpha_num && !rq.alpha_scales && btune->alpha_milli;
+replan:  // again without the batch alpha when its shared sieve would not fit (below)
     {
         BatchReq r2 = rq;
         r2.p2_table_limit = ctx->p2_table_limit;
         r2.tune = tune;
-        if (btune && !r2.alpha_scale && !r2.alpha_num && !r2.alpha_scales && btune->alpha_milli) {
+        if (batch_alpha) {
             ascale = batch_alpha_scales(rq.xs, Q, btune->alpha_milli, ctx->tuned ? ctx->tune : nullptr);
             r2.alpha_scales = ascale.data();
         }
@@ -535,6 +556,18 @@ void run_batch(cpx_ctx *ctx, const BatchReq &rq)
                 return qd[a].z != qd[b].z ? qd[a].z > qd[b].z : a < b;
             });
             sh_lbits = choose_shared(ctx, qd, horder, threads, rq.lbits, lbits_cap, gsize);
+            // the counting sweep keeps 8 bytes per (sub-segment, level) of [0, z_max): above four
+            // times the leaf-set budget (16 GiB by default), plan again without the batch alpha
+            // (shorter z), else one sieve per query
+            if (carry_row_bytes(qd, horder, hP, sh_lbits, threads, c) > 4 * ctx->hard_offload_bytes) {
+                if (batch_alpha) {
+                    batch_alpha = false;
+                    goto replan;
+                }
+                shared = false;
+            }
+        }
+        if (shared) {
             for (uint32_t i : horder) qd[i].lbits = sh_lbits;
         } else {
             threads = std::min<uint32_t>(threads, 512);  // 1024-thread blocks: the shared sieve only

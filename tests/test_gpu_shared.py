@@ -142,3 +142,21 @@ def test_batch_alpha_only_for_queries_with_companions(own, cpx):
     assert got[-1]["y"] == alone["y"] and got[-1]["pi"] == alone["pi"]
     own.set_hard_shared(0)
     assert cpx.terms_batch(xs, ctx=own) == got
+
+
+def test_shared_sieve_over_budget_replans_without_batch_alpha(own, cpx):
+    """Seventeen queries near 1e18 have companions, but the batch alpha would
+    give the shared sieve's counting sweep 22.5 GB of carry rows, above the
+    16 GiB budget: the batch is planned again with each decade's alpha (y as
+    for the query alone; 6.6 GB of rows, so the sieve is still shared) and
+    the answers are exact."""
+    import os
+
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    own.tune_load(os.path.join(root, "cudapix_b200", "tuning", "b200.json"))
+    xs = [10**18 + k * 3 * 10**16 + 1 for k in range(17)]
+    got = cpx.terms_batch(xs, ctx=own)
+    assert own.last_batch_stats()["shared_groups"] >= 1
+    for x, t in list(zip(xs, got))[::8]:
+        alone = cpx.terms_batch([x], ctx=own)[0]
+        assert t["y"] == alone["y"] and t["pi"] == alone["pi"], x
