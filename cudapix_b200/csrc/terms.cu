@@ -331,7 +331,11 @@ __global__ void k_easy_count(const QD *__restrict__ qd, uint32_t Q, const uint64
 
 // Pass 2: each warp owns a contiguous slice of chunks.  A sparse chunk is
 // kEasyChunk table entries of the q range of one p (two entries per lane); a
-// clustered chunk is kEasyClu consecutive u primes of one p.
+// clustered chunk is kEasyClu consecutive u primes of one p.  The sparse
+// primes q of a chunk are gathered into the warp's buffer and answered 32 at
+// a time, so that a lane whose table entries hold many primes does not hold
+// up the others.
+constexpr uint32_t kEasyBuf = 512;  // gathered q per warp
 template <class XT>
 __global__ void __launch_bounds__(kThreads) k_easy(const QD *__restrict__ qd, uint32_t Q,
                                                    const uint64_t *__restrict__ pre, uint64_t total_units,
@@ -342,6 +346,8 @@ __global__ void __launch_bounds__(kThreads) k_easy(const QD *__restrict__ qd, ui
 {
     const int lane = threadIdx.x & 31;
     const WarpSlice sl = warp_slice(off[total_units]);
+    __shared__ uint32_t s_q[kThreads / 32][kEasyBuf];
+    uint32_t *qbuf = s_q[threadIdx.x >> 5];
     LaneAcc a;
     // decoded state of the current p, kept across its consecutive chunks
     uint64_t c_unit = ~0ull, c_first = 0, c_last = 0, b = 0;
@@ -374,16 +380,47 @@ __global__ void __launch_bounds__(kThreads) k_easy(const QD *__restrict__ qd, ui
             const uint64_t w_beg = (e.qlo >> 7) + r * kEasyChunk;
             const uint64_t w_end = min(w_beg + kEasyChunk, ((e.q1 - 1) >> 7) + 1);
             uint64_t ps = 0, cnt = 0;
-            for (uint64_t wq = w_beg + lane; wq < w_end; wq += 32) {
-                const ulonglong2 e2 = __ldg(reinterpret_cast<const ulonglong2 *>(T) + wq);
-                uint64_t qb = e2.x & range_mask(wq, e.qlo, e.q1);
+            uint32_t nbuf = 0;
+            auto flush = [&] {
+                __syncwarp();
+                for (uint32_t jj = lane; jj < nbuf; jj += 32) {
+                    ps += cpx_pi_dev(T, (uint64_t)cpx_qdiv(xp, (uint64_t)qbuf[jj]));
+                    cnt++;
+                }
+                __syncwarp();
+                nbuf = 0;
+            };
+            for (uint64_t wb = w_beg; wb < w_end; wb += 32) {  // uniform over the warp
+                const uint64_t wq = wb + lane;
+                uint64_t qb = 0;
+                if (wq < w_end) qb = __ldg(reinterpret_cast<const ulonglong2 *>(T) + wq).x & range_mask(wq, e.qlo, e.q1);
+                const uint32_t nq = (uint32_t)__popcll(qb);
+                uint32_t inc = nq;
+#pragma unroll
+                for (int o = 1; o < 32; o <<= 1) {
+                    const uint32_t t = __shfl_up_sync(FULL, inc, o);
+                    if (lane >= o) inc += t;
+                }
+                const uint32_t tot = __shfl_sync(FULL, inc, 31);
+                if (tot > kEasyBuf) {  // a dense round: each lane answers its own entry
+                    while (qb) {
+                        const int j2 = __ffsll((long long)qb) - 1;
+                        qb &= qb - 1;
+                        ps += cpx_pi_dev(T, (uint64_t)cpx_qdiv(xp, 128 * wq + 2 * j2 + 1));
+                        cnt++;
+                    }
+                    continue;
+                }
+                if (nbuf + tot > kEasyBuf) flush();
+                uint32_t kk = nbuf + inc - nq;
                 while (qb) {
                     const int j2 = __ffsll((long long)qb) - 1;
                     qb &= qb - 1;
-                    ps += cpx_pi_dev(T, (uint64_t)cpx_qdiv(xp, 128 * wq + 2 * j2 + 1));
-                    cnt++;
+                    qbuf[kk++] = (uint32_t)(128 * wq + 2 * j2 + 1);
                 }
+                nbuf += tot;
             }
+            flush();
             a.v += (i128)ps + (i128)cnt * (2 - (i128)b);
         } else {
             const uint64_t j = r - e.nsp;
