@@ -770,6 +770,10 @@ replan:  // again without the batch alpha when its shared sieve would not fit (b
         pl.pre_grp = reinterpret_cast<const uint64_t *>(d_sh + grp_bytes);
         pl.lvl_off = reinterpret_cast<const uint64_t *>(d_sh + grp_bytes + pg_bytes);
         pl.carry = ctx->b_work[4].as<uint64_t>(pl.n_carry + 1);
+        const size_t ntab = groups.size() * (size_t)sh_nlv * 32, xb = wide ? 16 : 8;
+        unsigned char *tab = static_cast<unsigned char *>(ctx->b_work[5].get(ntab * (xb + 8) + 64));
+        pl.gxp = tab;
+        pl.gae = reinterpret_cast<uint2 *>(tab + ntab * xb);
     }
     if (pl.n_seg || pl.n_gunits) {
         if (!shared) {

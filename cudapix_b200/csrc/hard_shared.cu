@@ -157,33 +157,48 @@ __global__ void __launch_bounds__(1024) k_carry_scan(uint32_t nlv, uint32_t c, u
     }
 }
 
-// Candidates (mlo, mhi] of one query at level p in a warp's sub-segment
-// [lo_w, hi_w), and x/p.  Out of line (instruction-cache footprint of the
-// level loop); called by the lanes whose query passes the cheap filter.
-template <class XT> struct SlotPar {
-    XT xp;
-    uint32_t mlo, mhi;
-    bool act;
+// Quotients n / d by a sub-segment bound d >= 2^13 with rd = 1/d (double,
+// once per warp): for n < 2^64 the quotient is below 2^51, so the truncated
+// product n * rd (relative error at most 3 * 2^-53) is within 1 of it and the
+// sign and size of the remainder n - q d fix it.  128-bit n: exact division.
+struct Recip {
+    uint64_t d;
+    double rd;
 };
-template <class XT>
-static __device__ __noinline__ void slot_params(SlotPar<XT> &o, XT xj, uint64_t yj, uint64_t p, uint64_t pp,
-                                                uint64_t lo_w, const BoundDiv &bl, const BoundDiv &bh)
+template <class XT> __device__ __forceinline__ XT div_recip(XT n, const Recip &r)
 {
-    const XT xp = cpx_qdiv(xj, p);
-    uint64_t a = cpx_udiv_leaf(yj, p);
-    const XT t1 = div_bound(xp, bh);
-    if (t1 > (XT)a) a = (uint64_t)t1;
-    uint64_t e = yj;
-    if (lo_w) {
-        const XT t2 = div_bound(xp, bl);
-        if (t2 < (XT)e) e = (uint64_t)t2;
+    if ((u128)n >> 64) return cpx_qdiv(n, r.d);
+    const uint64_t n64 = (uint64_t)n;
+    uint64_t q = __double2ull_rz(__dmul_rn(__ull2double_rn(n64), r.rd));
+    const int64_t rem = (int64_t)(n64 - q * r.d);
+    if (rem < 0) q--;
+    else if ((uint64_t)rem >= r.d) q++;
+    return (XT)q;
+}
+
+// The per-level constants of every query of every group: x/p, y/p and
+// min(y, x/p^3) at index (g nlv + b - c - 1) 32 + slot.  They do not depend
+// on the segment, so k_hard_shared loads them instead of dividing.
+template <class XT>
+__global__ void k_group_levels(const QD *__restrict__ qd, const HardGroup *__restrict__ grp, uint32_t ngrp,
+                               uint32_t nlv, uint32_t c, const uint32_t *__restrict__ P, XT *__restrict__ gxp,
+                               uint2 *__restrict__ gae)
+{
+    const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= (uint64_t)ngrp * nlv * 32) return;
+    const uint32_t slot = (uint32_t)(i & 31), lv = (uint32_t)((i >> 5) % nlv), g = (uint32_t)((i >> 5) / nlv);
+    XT xp = 0;
+    uint32_t a = 0, e = 0;
+    if (slot < grp[g].n) {
+        const QD &d = qd[grp[g].q[slot]];
+        const uint64_t p = P[c + lv];
+        xp = cpx_qdiv(xload<XT>(d), p);
+        a = (uint32_t)cpx_udiv_leaf(d.y, p);
+        const XT t3 = cpx_qdiv(xp, p * p);
+        e = (uint32_t)(t3 < (XT)d.y ? (uint64_t)t3 : d.y);
     }
-    const XT t3 = cpx_qdiv(xp, pp);  // hard leaves only: m <= x/p^3
-    if (t3 < (XT)e) e = (uint64_t)t3;
-    o.xp = xp;
-    o.mlo = (uint32_t)a;
-    o.mhi = (uint32_t)(e > a ? e : a);
-    o.act = e > ((pp > yj && p > a) ? p : a);
+    gxp[i] = xp;
+    gae[i] = make_uint2(a, e);
 }
 
 // Hands the heavy leaf sets of one (sub-segment, level) to k_hard_leaves: one
@@ -264,7 +279,8 @@ __global__ void __launch_bounds__(1024, 1)
                   const uint64_t *__restrict__ lvl_off, uint32_t nlv, const uint64_t *__restrict__ carry,
                   unsigned long long *__restrict__ acc, HardJob *__restrict__ jobs, unsigned int *__restrict__ njobs,
                   uint64_t *__restrict__ job_units, unsigned char *__restrict__ snap, unsigned int *__restrict__ nsnap,
-                  uint32_t max_jobs, uint32_t lbits_sub, uint32_t offload_min)
+                  uint32_t max_jobs, uint32_t lbits_sub, uint32_t offload_min, const XT *__restrict__ gxp,
+                  const uint2 *__restrict__ gae)
 {
     extern __shared__ uint4 smem4[];
     __shared__ uint32_t s_B;
@@ -321,7 +337,8 @@ __global__ void __launch_bounds__(1024, 1)
     __syncwarp();
     const uint64_t w = seg * NW + warp;
     auto sub_count = [&](uint64_t uu) -> uint32_t { return sub_survivors(uu, lo_w, wl, cnt8, bm, CPT, s, warp); };
-    const BoundDiv bd_lo = bound_div(lo_w), bd_hi = bound_div(hi_w);
+    const Recip r_lo{lo_w, lo_w ? 1.0 / (double)lo_w : 0.0}, r_hi{hi_w, 1.0 / (double)hi_w};
+    const size_t gbase = (size_t)g * nlv * 32 + lane;  // this lane's slot in the group's level table
 
     for (uint32_t gb = c + 1; gb <= B; gb += 32) {
         const uint32_t nl = min(32u, B - gb + 1);
@@ -337,15 +354,25 @@ __global__ void __launch_bounds__(1024, 1)
             // Candidates (mlo, mhi] of this lane's query in the warp's
             // sub-segment.  None unless some u in it satisfies u <= z,
             // u >= p^2 and x/(p hi_w) < y (else m > y).
-            SlotPar<XT> sp_j;
-            sp_j.xp = 0;
-            sp_j.mlo = sp_j.mhi = 0;
-            sp_j.act = false;
-            if (lane < nq && lo_w <= zj && hi_w > pp && (u128)p * yj * hi_w > (u128)xj)
-                slot_params<XT>(sp_j, xj, yj, p, pp, lo_w, bd_lo, bd_hi);
-            const XT xp = sp_j.xp;
-            const uint32_t mlo = sp_j.mlo, mhi = sp_j.mhi;
-            const bool act = sp_j.act;
+            XT xp = 0;
+            uint32_t mlo = 0, mhi = 0;
+            bool act = false;
+            if (lane < nq && lo_w <= zj && hi_w > pp && (u128)p * yj * hi_w > (u128)xj) {
+                const size_t gi = gbase + (size_t)(b - c - 1) * 32;
+                xp = gxp[gi];
+                const uint2 ae = gae[gi];  // y/p, min(y, x/p^3)
+                uint64_t a = ae.x;
+                const XT t1 = div_recip(xp, r_hi);
+                if (t1 > (XT)a) a = (uint64_t)t1;
+                uint64_t e = ae.y;
+                if (lo_w) {
+                    const XT t2 = div_recip(xp, r_lo);
+                    if (t2 < (XT)e) e = (uint64_t)t2;
+                }
+                mlo = (uint32_t)a;
+                mhi = (uint32_t)(e > a ? e : a);
+                act = e > ((pp > yj && p > a) ? (uint64_t)p : a);
+            }
             const unsigned bal = __ballot_sync(FULL, act);
             if (bal) {
                 // lane prefixes of the sub-segment from the chunk counters
@@ -369,6 +396,48 @@ __global__ void __launch_bounds__(1024, 1)
                     off_j = offload_sets<XT>(off_j, lane, qj, b, p, prime_j, qa_j, mlo, mhi, work, lo_w, C, xp, bm, cnt8,
                                              cw0, c0, CPT, s, wl[lane], jobs, njobs, job_units, snap, nsnap, max_jobs,
                                              lbits_sub);
+                const uint32_t nw_j =
+                    (act && !off_j && prime_j) ? (uint32_t)((((uint64_t)mhi - 1) >> 7) - (qa_j >> 7) + 1) : 0u;
+                uint32_t ng_j = 0;
+                if (act && !off_j && !prime_j)
+                    ng_j = (uint32_t)(((((uint64_t)mhi - 1) >> 1) >> 2) - ((((uint64_t)mlo + 1) >> 1) >> 2) + 1);
+                if (!__any_sync(FULL, nw_j > 2 || ng_j > 2)) {
+                    // a sparse level (the common case: about one leaf per query):
+                    // each lane answers its own query's few candidates
+                    int64_t sv = 0;
+                    int32_t sm = 0;
+                    for (uint32_t k2 = 0; k2 < nw_j; k2++) {
+                        const uint64_t wq = (qa_j >> 7) + k2;
+                        uint64_t qb = __ldg(reinterpret_cast<const ulonglong2 *>(Tpi) + wq).x & range_mask(wq, qa_j, mhi);
+                        while (qb) {
+                            const int jb = __ffsll((long long)qb) - 1;
+                            qb &= qb - 1;
+                            sv += sub_count((uint64_t)cpx_qdiv(xp, 128 * wq + 2 * jb + 1));  // mu(q) = -1
+                            sm += 1;
+                        }
+                    }
+                    const uint64_t i_lo = ((uint64_t)mlo + 1) >> 1, i_hi = ((uint64_t)mhi - 1) >> 1;
+                    for (uint32_t k2 = 0; k2 < ng_j; k2++) {
+                        const uint64_t g4 = (i_lo >> 2) + k2;
+                        uint32_t neg = 0;
+                        uint32_t vm =
+                            valid_group(__ldg(reinterpret_cast<const int4 *>(MU) + g4), g4, i_lo, i_hi, p, &neg);
+                        while (vm) {
+                            const int kq = __ffs(vm) - 1;
+                            vm &= vm - 1;
+                            const uint32_t cv = sub_count((uint64_t)cpx_qdiv(xp, 2 * (4 * g4 + kq) + 1));
+                            if ((neg >> kq) & 1u) {
+                                sv += cv;
+                                sm += 1;
+                            } else {
+                                sv -= cv;
+                                sm -= 1;
+                            }
+                        }
+                    }
+                    accq += (i128)sv + (i128)C * (i128)sm;
+                    __syncwarp();
+                } else {
                 // running sums of the query of this lane's last leaf
                 uint32_t cur = 0xFFu;
                 int64_t csum = 0;
@@ -414,8 +483,6 @@ __global__ void __launch_bounds__(1024, 1)
                 };
                 {
                     // prime-only levels: pi-table words of (max(mlo, p), mhi]
-                    const uint32_t nw_j =
-                        (act && !off_j && prime_j) ? (uint32_t)((((uint64_t)mhi - 1) >> 7) - (qa_j >> 7) + 1) : 0u;
                     uint32_t ex_j;
                     const uint32_t tot_w = warp_place(nw_j, lane, ex_j);
                     for (uint32_t base = 0; base < tot_w; base += 32) {
@@ -451,9 +518,6 @@ __global__ void __launch_bounds__(1024, 1)
                 }
                 {
                     // other levels: squarefree m with lpf(m) > p, 16-byte groups of packed mu*lpf
-                    uint32_t ng_j = 0;
-                    if (act && !off_j && !prime_j)
-                        ng_j = (uint32_t)(((((uint64_t)mhi - 1) >> 1) >> 2) - ((((uint64_t)mlo + 1) >> 1) >> 2) + 1);
                     uint32_t ex_j;
                     const uint32_t tot_g = warp_place(ng_j, lane, ex_j);
                     for (uint32_t base = 0; base < tot_g; base += 32) {
@@ -493,6 +557,7 @@ __global__ void __launch_bounds__(1024, 1)
                     s_ms[lane] = 0;
                 }
                 __syncwarp();
+                }
             }
             // ---- cross off p_b in the sub-segment
             cross_off(bm, cnt8, p, __shfl_sync(FULL, lr0, k), __shfl_sync(FULL, li0, k), c0, cw0, CPT, s,
@@ -535,10 +600,18 @@ template <class XT> static void shared_go(cpx_ctx *ctx, const Plan &pl)
         CPX_CUDA(cudaMemsetAsync(pl.njobs, 0, 2 * sizeof(uint64_t), ctx->stream));  // job and snapshot counters
         CPX_CUDA(cudaMemsetAsync(pl.job_units, 0, (pl.max_jobs + 1) * sizeof(uint64_t), ctx->stream));
     }
+    XT *gxp = static_cast<XT *>(pl.gxp);
+    const uint64_t ntab = (uint64_t)pl.n_grp * pl.sh_nlv * 32;
+    if (ntab) {
+        k_group_levels<XT><<<(unsigned)((ntab + 255) / 256), 256, 0, ctx->stream>>>(pl.qd, pl.grp, pl.n_grp,
+                                                                                    pl.sh_nlv, pl.c, tb.P, gxp, pl.gae);
+        CPX_LAUNCH("k_group_levels");
+        note_launch(ctx);
+    }
     k_hard_shared<XT><<<(unsigned)pl.n_gunits, T, shared_smem(pl.sh_lbits, T), ctx->stream>>>(
         pl.qd, pl.grp, pl.pre_grp, pl.n_grp, pl.n_gunits, pl.sh_lbits, pl.c, tb.P, (uint32_t)tb.prm_n, tb.MU, tb.T,
         pl.lvl_off, pl.sh_nlv, pl.carry, pl.acc, pl.jobs, pl.njobs, pl.job_units, pl.snap, pl.nsnap, pl.max_jobs,
-        lbits_sub, (uint32_t)std::min<uint64_t>(pl.offload_min, 0xFFFFFFFFull));
+        lbits_sub, (uint32_t)std::min<uint64_t>(pl.offload_min, 0xFFFFFFFFull), gxp, pl.gae);
     CPX_LAUNCH("k_hard_shared");
     note_launch(ctx);
     if (pl.max_jobs) launch_hard_leaves(ctx, pl, lbits_sub);

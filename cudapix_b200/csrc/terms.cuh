@@ -113,6 +113,8 @@ struct Plan {
     const uint64_t *lvl_off = nullptr;  // sh_nlv + 1 row offsets into carry
     uint64_t *carry = nullptr;
     unsigned int *nsnap = nullptr;      // device counter of snapshot slots
+    void *gxp = nullptr;                // x/p per (group, level, slot): uint64 or u128 (wide)
+    uint2 *gae = nullptr;               // y/p and min(y, x/p^3) per (group, level, slot)
 };
 
 void launch_ordinary(cpx_ctx *ctx, const Plan &pl);
