@@ -401,9 +401,10 @@ __global__ void __launch_bounds__(1024, 1)
                 uint32_t ng_j = 0;
                 if (act && !off_j && !prime_j)
                     ng_j = (uint32_t)(((((uint64_t)mhi - 1) >> 1) >> 2) - ((((uint64_t)mlo + 1) >> 1) >> 2) + 1);
-                if (!__any_sync(FULL, nw_j > 2 || ng_j > 2)) {
-                    // a sparse level (the common case: about one leaf per query):
-                    // each lane answers its own query's few candidates
+                if (!__any_sync(FULL, nw_j > 8 || ng_j > 8)) {
+                    // a sparse level (the common case: about one leaf per query;
+                    // at most 8 table entries or 4-m groups each): each lane
+                    // answers its own query's candidates
                     int64_t sv = 0;
                     int32_t sm = 0;
                     for (uint32_t k2 = 0; k2 < nw_j; k2++) {
