@@ -12,9 +12,11 @@
 //      survivors of level b-1 are 1 and the primes from p_b on);
 //  (3) k_hard_shared runs one CTA per (group of up to 32 queries, segment).
 //      Its warps sieve their sub-segments level by level as k_hard does; at
-//      each level the lanes compute the candidate range of one query each,
-//      the warp gathers the leaves of every query of the group and answers
-//      them 32 at a time, and each leaf's -mu(m) phi(u, b-1) =
+//      each level the lanes compute the candidate range of one query each
+//      (from a per-(group, level) table of x/p, y/p and x/p^3 that
+//      k_group_levels fills once per batch), answer their own query's leaves
+//      when every query has few, or else the warp gathers the leaves of every
+//      query and answers them 32 at a time; each leaf's -mu(m) phi(u, b-1) =
 //      -mu(m) (carry + survivors of the sub-segment <= u) goes straight into
 //      its query's sum: no per-segment outputs and no carry combine.
 // Heavy (query, sub-segment, level) leaf sets go to k_hard_leaves with one
@@ -49,14 +51,6 @@ __host__ __device__ __forceinline__ size_t shared_smem(uint32_t lbits, uint32_t 
     o += (threads / 32) * kGroupMax * 16;  // x/p of the group's queries, per warp
     o += (threads / 32) * kGroupMax * 12;  // per-warp, per-query level sums and Sum(-mu)
     return o;
-}
-
-template <class XT> __device__ __forceinline__ XT shfl_xt(XT v, uint32_t src)
-{
-    if (sizeof(XT) == 8) return (XT)__shfl_sync(FULL, (unsigned long long)v, src);
-    const unsigned long long a0 = __shfl_sync(FULL, (unsigned long long)v, src);
-    const unsigned long long a1 = __shfl_sync(FULL, (unsigned long long)((u128)v >> 64), src);
-    return (XT)(((u128)a1 << 64) | a0);
 }
 
 // (1) One CTA per segment: survivors of level b-1 of each warp sub-segment w,
@@ -261,16 +255,18 @@ static __device__ __noinline__ bool offload_sets(bool off_j, uint32_t lane, uint
 }
 
 // (3) One CTA per (group, segment).  Per level, the lanes hold one query
-// each: its x/p and candidate range in the warp's sub-segment.  The warp then
-// walks the candidates of all the group's queries as one sequence (pi-table
-// words of the prime-only levels, then 4-m groups of packed mu*lpf of the
-// others), 32 words at a time, each lane finding its word's query by a binary
-// search over the warp's exclusive word counts; the leaves found go to the
-// warp's buffer (m, query | (mu(m) = -1) << 31) and are answered 32 at a
-// time.  Each lane keeps a running Sum(-mu) * count and Sum(-mu) for the
-// query of its last leaf and adds them into the warp's per-query slots when
-// the query changes; at the end of the level lane j folds slot j into its
-// 128-bit total as sum + carry * Sum(-mu).
+// each: its x/p and candidate range in the warp's sub-segment.  When no query
+// has more than 8 candidate table entries (most levels: about one leaf per
+// query), each lane answers its own query's leaves into its 128-bit total.
+// Otherwise the warp walks the candidates of all the group's queries as one
+// sequence (pi-table words of the prime-only levels, then 4-m groups of
+// packed mu*lpf of the others), 32 words at a time, each lane finding its
+// word's query by a binary search over the warp's exclusive word counts; the
+// leaves found go to the warp's buffer (m, query | (mu(m) = -1) << 31) and
+// are answered 32 at a time.  Each lane keeps a running Sum(-mu) * count and
+// Sum(-mu) for the query of its last leaf and adds them into the warp's
+// per-query slots when the query changes; at the end of the level lane j
+// folds slot j into its total as sum + carry * Sum(-mu).
 template <class XT>
 __global__ void __launch_bounds__(1024, 1)
     k_hard_shared(const QD *__restrict__ qd, const HardGroup *__restrict__ grp, const uint64_t *__restrict__ pre_grp,
