@@ -23,6 +23,8 @@ Python int; 64- and 128-bit overloads are chosen by the size of x.
 import ctypes
 import os
 
+import numpy as np
+
 from ._lib import (BatchStats, CpxError, ExtensionMissing, LeafCounts, Params, ServeConfig, ServeCounters, Terms, TuneEntry,  # noqa: F401
                    U128,
                    header_symbols, load)
@@ -319,12 +321,25 @@ def _params(alpha, c, hard_log2_bits, hard_threads, wide, graph):
     return p
 
 
+_M64 = (1 << 64) - 1
+
+
 def _u128_array(xs):
+    """A ctypes array of 128-bit values (low word first), filled through a
+    numpy view (a per-element struct loop costs milliseconds per batch)."""
     n = len(xs)
     arr = (U128 * max(n, 1))()
-    for i, x in enumerate(xs):
-        arr[i] = U128.of(x)
+    if n:
+        ints = [int(x) for x in xs]
+        w = np.frombuffer(arr, dtype=np.uint64).reshape(-1, 2)
+        w[:n, 0] = [x & _M64 for x in ints]
+        w[:n, 1] = [(x >> 64) & _M64 for x in ints]
     return arr
+
+
+def _u128_values(arr, n):
+    w = np.frombuffer(arr, dtype=np.uint64).reshape(-1, 2)[:n]
+    return [lo | (hi << 64) if hi else lo for lo, hi in zip(w[:, 0].tolist(), w[:, 1].tolist())]
 
 
 def pi_batch(xs, alpha=None, c=6, hard_log2_bits=0, hard_threads=0, wide=False, graph=False, ctx=None):
@@ -335,7 +350,7 @@ def pi_batch(xs, alpha=None, c=6, hard_log2_bits=0, hard_threads=0, wide=False, 
     out = (U128 * max(n, 1))()
     p = _params(alpha, c, hard_log2_bits, hard_threads, wide, graph)
     ctx.call("cpx_pi_batch", arr, n, ctypes.byref(p), out)
-    return [out[i].value() for i in range(n)]
+    return _u128_values(out, n)
 
 
 class Server:
