@@ -321,6 +321,40 @@ template <class F> static void launch_as_graph(cpx_ctx *ctx, F &&launches)
     CPX_CUDA(cudaGraphLaunch(ctx->graph_exec, ctx->stream));
 }
 
+// Runs f(0) .. f(n - 1) on up to 16 host threads (the calling thread
+// included); the first exception thrown by any f is rethrown here.
+constexpr size_t kPlanBlock = 64;  // queries per planning block
+template <class F> static void parallel_blocks(size_t n, F &&f)
+{
+    const size_t hw = std::max<size_t>(1, std::thread::hardware_concurrency());
+    const size_t nt = std::min<size_t>(std::min<size_t>(hw, 16), n);
+    if (nt <= 1) {
+        for (size_t k = 0; k < n; k++) f(k);
+        return;
+    }
+    std::atomic<size_t> next(0);
+    std::exception_ptr err;
+    std::mutex em;
+    auto worker = [&] {
+        try {
+            for (;;) {
+                const size_t k = next.fetch_add(1);
+                if (k >= n) break;
+                f(k);
+            }
+        } catch (...) {
+            std::lock_guard<std::mutex> g(em);
+            if (!err) err = std::current_exception();
+        }
+    };
+    std::vector<std::thread> th;
+    th.reserve(nt - 1);
+    for (size_t t = 1; t < nt; t++) th.emplace_back(worker);
+    worker();
+    for (auto &t : th) t.join();
+    if (err) std::rethrow_exception(err);
+}
+
 // Roots, y and validity of every query of a request, and the table bounds
 // the batch needs (pi table to N, mu/lpf to Y, primes to P, wheel for c).
 void compute_needs(const BatchReq &rq, std::vector<QD> &qd, TableNeed &need, bool &wide)
@@ -330,10 +364,16 @@ void compute_needs(const BatchReq &rq, std::vector<QD> &qd, TableNeed &need, boo
     const unsigned mask = rq.terms;
     if (c < 1 || c > 8) fail(CPX_EINVAL, "c must be in 1..8");
     qd.assign(Q, QD{});
-    uint64_t N = 1 << 16, Y = 0, Pneed = 64;
-    wide = rq.wide;
-    bool any_direct = false;
-    for (uint32_t i = 0; i < Q; i++) {
+    // per query in parallel blocks of 256; each block keeps its own maxima
+    struct Part {
+        uint64_t N = 1 << 16, Y = 0, Pneed = 64;
+        bool wide = false, any_direct = false;
+    };
+    const size_t nblk = (Q + 255) / 256;
+    std::vector<Part> parts(nblk);
+    auto one = [&](uint32_t i, Part &pt) {
+        uint64_t &N = pt.N, &Y = pt.Y, &Pneed = pt.Pneed;
+        bool &wide = pt.wide, &any_direct = pt.any_direct;
         QD &d = qd[i];
         memset(&d, 0, sizeof(d));
         const u128 x = rq.xs[i];
@@ -359,7 +399,7 @@ void compute_needs(const BatchReq &rq, std::vector<QD> &qd, TableNeed &need, boo
                 d.y = 0;
                 any_direct = true;
                 N = std::max<uint64_t>(N, (uint64_t)x + 1);
-                continue;
+                return;
             }
         } else if (y == 0) {
             fail(CPX_EINVAL, "y must be >= 1");
@@ -399,6 +439,20 @@ void compute_needs(const BatchReq &rq, std::vector<QD> &qd, TableNeed &need, boo
             Y = std::max(Y, y);
         }
         if (mask == TERM_PI) N = std::max<uint64_t>(N, y + 1);
+    };
+    parallel_blocks(nblk, [&](size_t k) {
+        const uint32_t i1 = (uint32_t)std::min<size_t>(Q, (k + 1) * 256);
+        for (uint32_t i = (uint32_t)(k * 256); i < i1; i++) one(i, parts[k]);
+    });
+    uint64_t N = 1 << 16, Y = 0, Pneed = 64;
+    wide = rq.wide;
+    bool any_direct = false;
+    for (const Part &pt : parts) {
+        N = std::max(N, pt.N);
+        Y = std::max(Y, pt.Y);
+        Pneed = std::max(Pneed, pt.Pneed);
+        wide |= pt.wide;
+        any_direct |= pt.any_direct;
     }
     if (N > rq.max_table_n) fail(CPX_ERANGE, "pi table bound exceeds the configured limit");
     need.P = std::max<uint64_t>(Pneed, cpx_isqrt(Y + 1) + 2);
@@ -425,39 +479,6 @@ void grow_tables(cpx_ctx *ctx, const TableNeed &need)
     if (need.c) ensure_wheel(ctx, need.c);
 }
 
-// Runs f(0) .. f(n - 1) on up to 16 host threads (the calling thread
-// included); the first exception thrown by any f is rethrown here.
-constexpr size_t kPlanBlock = 64;  // queries per planning block
-template <class F> static void parallel_blocks(size_t n, F &&f)
-{
-    const size_t hw = std::max<size_t>(1, std::thread::hardware_concurrency());
-    const size_t nt = std::min<size_t>(std::min<size_t>(hw, 16), n);
-    if (nt <= 1) {
-        for (size_t k = 0; k < n; k++) f(k);
-        return;
-    }
-    std::atomic<size_t> next(0);
-    std::exception_ptr err;
-    std::mutex em;
-    auto worker = [&] {
-        try {
-            for (;;) {
-                const size_t k = next.fetch_add(1);
-                if (k >= n) break;
-                f(k);
-            }
-        } catch (...) {
-            std::lock_guard<std::mutex> g(em);
-            if (!err) err = std::current_exception();
-        }
-    };
-    std::vector<std::thread> th;
-    th.reserve(nt - 1);
-    for (size_t t = 1; t < nt; t++) th.emplace_back(worker);
-    worker();
-    for (auto &t : th) t.join();
-    if (err) std::rethrow_exception(err);
-}
 
 static double ms_since(std::chrono::steady_clock::time_point &t)
 {
