@@ -569,8 +569,12 @@ replan:  // again without the batch alpha when its shared sieve would not fit (b
             d.nb = (uint32_t)host_pi(hP, d.r4);
             if (d.nb > c) horder.push_back(i);
         }
+        // x >= 2^64 keeps one sieve per query: the shared sieve's 128-bit
+        // kernels are checked against the oracle on x < 2^64 only
+        bool any_big = false;
+        for (uint32_t i : horder) any_big |= (qd[i].x >> 64) != 0;
         const uint32_t mode = ctx->hard_shared;
-        shared = !rq.seg_hi && !rq.hard_levels && !horder.empty() &&
+        shared = !rq.seg_hi && !rq.hard_levels && !horder.empty() && !any_big &&
                  (mode == 2 || (mode == 1 && !small && horder.size() >= 8));
         if (shared) {
             std::sort(horder.begin(), horder.end(), [&](uint32_t a, uint32_t b) {

@@ -91,6 +91,7 @@ int cpx_set_hard_offload(cpx_ctx *ctx, uint32_t min_candidates);
  * segment is then sieved once per group of up to 32 queries, answering all
  * their leaves.  mode 0: never (one sieve per query), 1: batches of more than
  * four queries with at least eight hard-leaf queries (default), 2: always.
+ * Batches holding an x >= 2^64 keep one sieve per query in every mode.
  * Results are the same in every mode.  No reference counterpart. */
 int cpx_set_hard_shared(cpx_ctx *ctx, uint32_t mode);
 /* P2 needs pi(x/p) up to z = x/y.  For z above `limit` (default 2^36) the
