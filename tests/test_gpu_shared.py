@@ -160,3 +160,17 @@ def test_shared_sieve_over_budget_replans_without_batch_alpha(own, cpx):
     for x, t in list(zip(xs, got))[::8]:
         alone = cpx.terms_batch([x], ctx=own)[0]
         assert t["y"] == alone["y"] and t["pi"] == alone["pi"], x
+
+
+@pytest.mark.parametrize("c", [1, 2, 3, 5, 7, 8])
+def test_shared_other_c(own, cpx, orc, c):
+    """Pre-sieving p_2..p_c and sieving from level c+1 in the shared sieve,
+    for every c the library takes: equal to one sieve per query, and to the
+    oracle's hard leaves."""
+    xs = [10**10 + 7, 3 * 10**10, 10**11, 2 * 10**11 + 1, 10**12, 7 * 10**11, 10**12 + 39, 4 * 10**11 + 3, 10**13]
+    own.set_hard_shared(2)
+    got = cpx.terms_batch(xs, c=c, ctx=own)
+    own.set_hard_shared(0)
+    assert cpx.terms_batch(xs, c=c, ctx=own) == got
+    for x, t in list(zip(xs, got))[:3]:
+        assert t["hard"] == orc.hard(x, t["y"], c), (c, x)
