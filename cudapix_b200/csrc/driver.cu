@@ -14,6 +14,7 @@
 #include <thread>
 
 #include "driver.h"
+#include "misc.h"
 #include "terms.cuh"
 
 namespace cpx {
@@ -138,7 +139,8 @@ static uint64_t heavy_leaf_sets(const QD &d, const std::vector<uint32_t> &hP, ui
         for (uint64_t w = std::max<uint64_t>((uint64_t)(xp / (XT)mtop) / span_w, w_beg); w < nsub; w++) {
             const uint64_t lo_w = w * span_w, hi_w = lo_w + span_w;
             const uint64_t lo = (w / NW) * L2;
-            if ((u128)p * p > (u128)(lo + L2 - 1) || (lo && (u128)p * p > (u128)((x - 1) / (XT)lo))) continue;
+            if (lo && (u128)p * p > (u128)((x - 1) / (XT)lo)) break;  // p^2 lo >= x here and above
+            if ((u128)p * p > (u128)(lo + L2 - 1)) continue;
             uint64_t mlo = y / p;
             const XT t1 = xp / (XT)hi_w;
             if (t1 > (XT)mlo) mlo = (uint64_t)t1;
@@ -275,6 +277,74 @@ static uint64_t carry_row_bytes(const std::vector<QD> &qd, const std::vector<uin
     uint64_t rows = 0;
     for (uint64_t b = c + 1; b <= nbm; b++) rows += segments_at_level(xmax, span, hP[b - 1], 0, nseg);
     return rows * (threads / 32) * 8;
+}
+
+// One query whose per-(segment, level) hard-leaf outputs would take more than
+// kWindowBytes: its other terms run as usual, its hard leaves run in windows
+// of consecutive segments of at most kWindowEntries (segment, level) pairs
+// (the part path of a query split over GPUs, here one window after another
+// on one GPU), and the windows' per-level records are merged in segment order:
+// a level's survivors below a window are the carries its leaves lacked.
+constexpr uint64_t kWindowBytes = 32ull << 30;
+constexpr uint64_t kWindowEntries = 1ull << 31;
+
+static void run_hard_windows(cpx_ctx *ctx, const BatchReq &rq, const QD &d, uint32_t threads)
+{
+    const uint32_t c = rq.c;
+    uint64_t y = d.y;
+    i128 t[7] = {};
+    if (rq.terms & ~(unsigned)TERM_HARD) {
+        BatchReq r1 = rq;
+        r1.terms = rq.terms & ~(unsigned)TERM_HARD;
+        r1.ys = &y;
+        r1.out_pi = nullptr;
+        r1.out_y = nullptr;
+        r1.out_terms = t;
+        run_batch(ctx, r1);
+        t[5] = t[6] = 0;
+    }
+    const uint32_t nlv = d.nb - c;
+    const uint64_t W = std::max<uint64_t>(1, kWindowEntries / nlv);
+    std::vector<HardLevel> rec(nlv);
+    std::vector<u128> carry(nlv, 0);
+    i128 H = 0;
+    for (uint64_t s0 = 0; s0 < d.nseg; s0 += W) {
+        i128 th[7] = {};
+        BatchReq rh;
+        rh.xs = rq.xs;
+        rh.ys = &y;
+        rh.n = 1;
+        rh.c = c;
+        rh.terms = TERM_HARD;
+        rh.lbits = d.lbits;
+        rh.threads = threads;
+        rh.seg_lo = s0;
+        rh.seg_hi = std::min(d.nseg, s0 + W);
+        rh.hard_levels = rec.data();
+        rh.out_terms = th;
+        rh.wide = rq.wide;
+        rh.max_table_n = rq.max_table_n;
+        run_batch(ctx, rh);
+        H += th[4];
+        for (uint32_t b = 0; b < nlv; b++) {
+            const HardLevel &lv = rec[b];
+            if (lv.anchored) {
+                carry[b] = (u128)lv.carry0 + lv.count;
+            } else {
+                H += (i128)carry[b] * lv.msum;
+                carry[b] += lv.count;
+            }
+        }
+    }
+    t[4] = H;
+    if (rq.terms == TERM_PI) {
+        t[5] = (i128)count_primes(ctx, 0, y + 1);
+        t[6] = t[1] + t[2] + t[3] + t[4] + t[5] - 1 - t[0];
+    }
+    if (rq.out_pi) rq.out_pi[0] = (u128)t[6];
+    if (rq.out_terms)
+        for (int k = 0; k < 7; k++) rq.out_terms[k] = t[k];
+    if (rq.out_y) rq.out_y[0] = y;
 }
 
 // Captures the launches of one batch into a CUDA graph and runs it.  The
@@ -698,6 +768,11 @@ replan:  // again without the batch alpha when its shared sieve would not fit (b
         n_ecomp += blk_ecomp[k];
     }
     if (!lbits_max) lbits_max = 15;
+    if (Q == 1 && !shared && (mask & TERM_HARD) && !rq.seg_hi && !rq.hard_levels && !qd[0].direct &&
+        hard_entries * 8 > kWindowBytes) {
+        run_hard_windows(ctx, rq, qd[0], threads);
+        return;
+    }
 
     // ---- the batch-shared sieve: groups, and the carry rows of its counting
     // sweep (row b: the sub-segments of the segments that sieve level b)
