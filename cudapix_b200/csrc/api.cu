@@ -275,15 +275,7 @@ int cpx_S2_hard_merge(const cpx_u128 *h, const cpx_hard_level *levels, uint32_t 
     i128 H = 0;
     for (uint32_t k = 0; k < nparts; k++) {
         H += (i128)U(h[k]);
-        for (uint32_t b = 0; b < nlevels; b++) {
-            const cpx_hard_level &lv = levels[(size_t)k * nlevels + b];
-            if (lv.anchored) {
-                carry[b] = (u128)lv.carry0 + lv.count;
-            } else {
-                H += (i128)carry[b] * lv.msum;
-                carry[b] += lv.count;
-            }
-        }
+        merge_hard_part(carry, H, reinterpret_cast<const HardLevel *>(levels) + (size_t)k * nlevels, nlevels);
     }
     *out = C128s(H);
     return CPX_OK;

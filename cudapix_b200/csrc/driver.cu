@@ -285,6 +285,19 @@ static uint64_t carry_row_bytes(const std::vector<QD> &qd, const std::vector<uin
 // (the part path of a query split over GPUs, here one window after another
 // on one GPU), and the windows' per-level records are merged in segment order:
 // a level's survivors below a window are the carries its leaves lacked.
+void merge_hard_part(std::vector<u128> &carry, i128 &H, const HardLevel *rec, uint32_t nlv)
+{
+    for (uint32_t b = 0; b < nlv; b++) {
+        const HardLevel &lv = rec[b];
+        if (lv.anchored) {
+            carry[b] = (u128)lv.carry0 + lv.count;
+        } else {
+            H += (i128)carry[b] * lv.msum;
+            carry[b] += lv.count;
+        }
+    }
+}
+
 constexpr uint64_t kWindowBytes = 32ull << 30;
 constexpr uint64_t kWindowEntries = 1ull << 31;
 
@@ -326,15 +339,7 @@ static void run_hard_windows(cpx_ctx *ctx, const BatchReq &rq, const QD &d, uint
         rh.max_table_n = rq.max_table_n;
         run_batch(ctx, rh);
         H += th[4];
-        for (uint32_t b = 0; b < nlv; b++) {
-            const HardLevel &lv = rec[b];
-            if (lv.anchored) {
-                carry[b] = (u128)lv.carry0 + lv.count;
-            } else {
-                H += (i128)carry[b] * lv.msum;
-                carry[b] += lv.count;
-            }
-        }
+        merge_hard_part(carry, H, rec.data(), nlv);
     }
     t[4] = H;
     if (rq.terms == TERM_PI) {

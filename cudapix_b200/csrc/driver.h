@@ -44,6 +44,10 @@ struct TableNeed {
 };
 
 void run_batch(cpx_ctx *ctx, const BatchReq &rq);
+// Adds one part's per-level records (in segment order) to the running merge
+// of a query's hard leaves split by segment ranges: carry[b] holds the
+// survivors of level b-1 below the part, H the hard sum.
+void merge_hard_part(std::vector<u128> &carry, i128 &H, const HardLevel *rec, uint32_t nlv);
 void compute_needs(const BatchReq &rq, std::vector<QD> &qd, TableNeed &need, bool &wide);
 bool tables_cover(const cpx_ctx *ctx, const TableNeed &need);
 void grow_tables(cpx_ctx *ctx, const TableNeed &need);
