@@ -3,8 +3,8 @@ context (tables replicated), no data-path collective.  The query list is dealt
 out by estimated work so that every rank finishes at about the same time, and
 the answers are gathered back in the caller's order.
 
-Reference: the reference runs on one GPU only (SURVEY of src/main.cpp:23-194);
-this is the replica layer of the multi-GPU plan (one process per GPU,
+Reference: the reference runs on one GPU only (src/main.cpp:23-194); this is
+the replica layer of the multi-GPU plan (one process per GPU,
 torch.distributed for the plumbing)."""
 
 
