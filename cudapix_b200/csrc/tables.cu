@@ -29,11 +29,15 @@ void check_cuda(cudaError_t e, const char *what)
     fail(code, std::string(what) + ": " + cudaGetErrorString(e));
 }
 
+// Grows by at least half its size: a run of queries of rising size then
+// reallocates a few times instead of at every new maximum (each reallocation
+// frees, which waits for the device, and maps fresh memory).
 void *DevBuf::get(size_t need)
 {
     if (need <= bytes && p) return p;
+    const size_t grown = bytes + bytes / 2;
     release();
-    size_t n = std::max<size_t>(need, 256);
+    size_t n = std::max<size_t>(std::max(need, grown), 256);
     n = (n + 255) & ~size_t(255);
     CPX_CUDA(cudaMalloc(&p, n));
     bytes = n;
