@@ -57,6 +57,16 @@ void one(cpx_ctx *ctx, u128 x, uint64_t y, uint32_t c, unsigned terms, i128 *t7,
 
 namespace cpx {
 
+// every work buffer of a context
+template <class F> static void each_buf(cpx_ctx *ctx, F &&f)
+{
+    for (auto &b : ctx->b_scan) f(b);
+    for (auto &b : ctx->b_work) f(b);
+    for (DevBuf *b : {&ctx->b_segtot, &ctx->b_small, &ctx->b_tmp, &ctx->b_win, &ctx->b_win2, &ctx->b_flush,
+                      &ctx->b_jobs, &ctx->b_jobctl, &ctx->b_snap, &ctx->b_levels})
+        f(*b);
+}
+
 int init_context(cpx_ctx *ctx, int device)
 {
     ctx->device = device;
@@ -72,6 +82,7 @@ int init_context(cpx_ctx *ctx, int device)
         return CPX_ECUDA;
     }
     ctx->smem_optin = (size_t)optin;
+    each_buf(ctx, [&](DevBuf &b) { b.stream = ctx->stream; });
     return CPX_OK;
 }
 
@@ -88,18 +99,9 @@ void release_context(cpx_ctx *ctx)
         if (tb.WH) cudaFree(tb.WH);
     }
     tb = Tables{};
-    for (auto &b : ctx->b_scan) b.release();
-    ctx->b_segtot.release();
-    ctx->b_small.release();
-    ctx->b_tmp.release();
-    ctx->b_win.release();
-    ctx->b_win2.release();
-    for (auto &b : ctx->b_work) b.release();
-    ctx->b_flush.release();
-    ctx->b_jobs.release();
-    ctx->b_jobctl.release();
-    ctx->b_snap.release();
-    ctx->b_levels.release();
+    each_buf(ctx, [](DevBuf &b) { b.release(); });
+    if (ctx->stream) cudaStreamSynchronize(ctx->stream);  // the buffers' stream-ordered frees
+    each_buf(ctx, [](DevBuf &b) { b.stream = nullptr; });
     if (ctx->graph_exec) cudaGraphExecDestroy(ctx->graph_exec);
     ctx->graph_exec = nullptr;
     for (cudaEvent_t *ev : {&ctx->ev_hard0, &ctx->ev_hard1, &ctx->ev_b0, &ctx->ev_b1, &ctx->ev_t0, &ctx->ev_t1}) {

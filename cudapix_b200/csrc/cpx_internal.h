@@ -35,10 +35,12 @@ void check_cuda(cudaError_t e, const char *what);
 #define CPX_CUDA(call) ::cpx::check_cuda((call), #call)
 #define CPX_LAUNCH(what) ::cpx::check_cuda(cudaGetLastError(), what)
 
-// Grow-only device buffer.
+// Grow-only device buffer, allocated and freed in the order of the owning
+// context's stream (a free does not wait for the other contexts' work).
 struct DevBuf {
     void *p = nullptr;
     size_t bytes = 0;
+    cudaStream_t stream = nullptr;
     void *get(size_t need);
     void release();
     ~DevBuf() { release(); }

@@ -39,14 +39,18 @@ void *DevBuf::get(size_t need)
     release();
     size_t n = std::max<size_t>(std::max(need, grown), 256);
     n = (n + 255) & ~size_t(255);
-    CPX_CUDA(cudaMalloc(&p, n));
+    if (stream) CPX_CUDA(cudaMallocAsync(&p, n, stream));
+    else CPX_CUDA(cudaMalloc(&p, n));
     bytes = n;
     return p;
 }
 
 void DevBuf::release()
 {
-    if (p) cudaFree(p);
+    if (p) {
+        if (stream) cudaFreeAsync(p, stream);
+        else cudaFree(p);
+    }
     p = nullptr;
     bytes = 0;
 }
