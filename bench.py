@@ -14,7 +14,9 @@ inputs; the reference publishes no dataset or numbers for this path.
   plain            the same queries one pi_deleglise_rivat call (one launch
                    sequence) each, with p50/p99 latency
   cpu_baseline     the oracle's OpenMP restatement of the term pipeline on
-                   the host cores, on a bounded sample of the same queries
+                   the host cores, on a bounded sample of the same queries;
+                   beside it (reference_terms) the reference's own OpenMP host
+                   term code, Gourdon's A and C, restated and timed the same way
 
 `--impl reference` times that CPU restatement alone (the reference itself
 cannot be built: its CUDASieve / CUDA-uint128 dependencies are not vendored).
@@ -142,7 +144,33 @@ def cpu_baseline(xs, budget_s):
     dt = time.perf_counter() - t0
     return {"value": done / dt, "unit": UNIT, "cores": nthreads, "kind": "port",
             "sample": f"first {done} of the {len(xs)} workload queries (x log-uniform in [1e9, 1e14]), "
-                      f"oracle/oracle.c orc_pi_dr, OpenMP {nthreads} threads, {dt:.1f} s"}
+                      f"oracle/oracle.c orc_pi_dr, OpenMP {nthreads} threads, {dt:.1f} s",
+            "reference_terms": reference_terms_baseline(xs, budget_s / 3)}
+
+
+def reference_terms_baseline(xs, budget_s):
+    """The reference's only CPU term code, Gourdon's sums A and C
+    (src/Gourdon/A2_cpu.cpp:20-134, src/Gourdon/C_cpu.cpp:20-78, restated in
+    oracle/oracle.c with the same OpenMP loops), on a bounded sample of the
+    workload with the reference alpha.  Two terms per query, not pi(x): the
+    reference's pi(x) through these terms is unfinished
+    (src/Gourdon/gourdonvariant.cpp:37-75 returns 0)."""
+    import oracle
+
+    nthreads = os.cpu_count() or 1
+    done, t0 = 0, time.perf_counter()
+    for x in xs:
+        y = oracle.default_y(x, *alpha_frac(x))
+        oracle.gourdon_A(x, y, nthreads)
+        oracle.gourdon_C(x, y, nthreads)
+        done += 1
+        if time.perf_counter() - t0 > budget_s:
+            break
+    dt = time.perf_counter() - t0
+    return {"value": done / dt, "unit": "queries/s (terms A and C only)", "cores": nthreads, "kind": "port",
+            "terms": "Gourdon A (src/Gourdon/A2_cpu.cpp:20-134) + C (src/Gourdon/C_cpu.cpp:20-78)",
+            "sample": f"first {done} of the {len(xs)} workload queries, oracle/oracle.c orc_gourdon_A + "
+                      f"orc_gourdon_C, OpenMP {nthreads} threads, {dt:.1f} s"}
 
 
 def alpha_frac(x):
@@ -290,7 +318,8 @@ def run_reference(args, world, rank):
             "warmup": args.warmup, "ms_per_step": 1000 * t / len(per_step), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "int64/int128", "data": "synthetic",
             "config": arm_config(args, world),
-            "cpu_baseline": {"value": v, "unit": UNIT, "cores": nthreads, "kind": "port", "sample": sample},
+            "cpu_baseline": {"value": v, "unit": UNIT, "cores": nthreads, "kind": "port", "sample": sample,
+                             "reference_terms": reference_terms_baseline(xs, args.ref_step_s / 4)},
             "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 

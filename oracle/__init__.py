@@ -60,6 +60,9 @@ def lib():
         L.orc_leaf_counts.argtypes = [U64, U64, U64, ctypes.c_uint32, ctypes.c_void_p]
         L.orc_pi_dr.restype = None
         L.orc_pi_dr.argtypes = [U64, U64, U64, ctypes.c_uint32, ctypes.c_int, ctypes.c_void_p]
+        for name in ("orc_gourdon_A", "orc_gourdon_C"):
+            getattr(L, name).restype = None
+            getattr(L, name).argtypes = [U64, U64, ctypes.c_int, ctypes.c_void_p]
         _lib = L
     return _lib
 
@@ -186,6 +189,22 @@ def pi_dr(x, y, c=6, nthreads=0):
     out = (U64 * 14)()
     lib().orc_pi_dr(*_split(x), y, c, nthreads, out)
     return {k: _s128(out[2 * i], out[2 * i + 1]) for i, k in enumerate(TERM_NAMES)}
+
+
+def gourdon_A(x, y, nthreads=0):
+    """Gourdon's A as the reference's OpenMP host code sums it
+    (src/Gourdon/A2_cpu.cpp:20-134): over primes x^(1/4) < p <= x^(1/3) and
+    p < q <= sqrt(x/p), chi(x/(pq)) pi(x/(pq)) with chi = 2 below y, else 1."""
+    assert 0 < x < 1 << 64
+    return _call128(lib().orc_gourdon_A, x, y, nthreads)
+
+
+def gourdon_C(x, y, nthreads=0):
+    """Gourdon's C as the reference's OpenMP host code sums it
+    (src/Gourdon/C_cpu.cpp:20-78): over primes sqrt(y) < p <= x^(1/4) and
+    x/p^3 < q <= y, pi(x/(pq)) - pi(p) + 2."""
+    assert 0 < x < 1 << 64
+    return _call128(lib().orc_gourdon_C, x, y, nthreads)
 
 
 def default_y(x, alpha_num=1, alpha_den=1):

@@ -968,6 +968,96 @@ void orc_pi_dr(uint64_t x_lo, uint64_t x_hi, uint64_t y, uint32_t c, int nthread
     if (nthreads > 0) omp_set_num_threads(saved);
 }
 
+/* ------------------------------------------ the reference's OpenMP terms */
+
+/* Gourdon's sums A and C as the reference computes them on the host with
+ * OpenMP.  They are the reference's only CPU term code (its pi(x) through
+ * Gourdon's terms, src/Gourdon/gourdonvariant.cpp:37-75, is unfinished and
+ * returns 0), restated here so that bench.py can time them on the host cores
+ * beside the GPU.  Same loop structure: a parallel loop over p with a dynamic
+ * schedule, an inner loop over the primes q, one pi-table lookup per (p, q).
+ *
+ *   A = sum_{x^(1/4) < p <= x^(1/3)} sum_{p < q <= sqrt(x/p)} chi(x/(pq)) pi(x/(pq)),
+ *       chi(n) = 2 if n < y else 1                 src/Gourdon/A2_cpu.cpp:20-134
+ *   C = sum_{sqrt(y) < p <= x^(1/4)} sum_{x/p^3 < q <= y} [pi(x/(pq)) - pi(p) + 2]
+ *                                                  src/Gourdon/C_cpu.cpp:20-78
+ *
+ * p and q run over primes; bounds are exact integer roots where the reference
+ * used doubles (A2_cpu.cpp:31,61; C_cpu.cpp:26-27).  The reference's C starts
+ * q above x/p^3 + 1 (C_cpu.cpp:53) and takes pi(p) from the index in its prime
+ * list (C_cpu.cpp:66); how both meet the sum depends on the range convention
+ * of its prime generator (CUDASieve, not vendored), so this restatement
+ * follows the sum.  C is then exactly the easy leaves (p, q) of the
+ * special-leaf sum with q prime and p > sqrt(y).  Both sums are positive;
+ * x < 2^64 as in the reference's GourdonVariant64. */
+void orc_gourdon_A(uint64_t x, uint64_t y, int nthreads, uint64_t *out)
+{
+    int saved = omp_get_max_threads();
+    if (nthreads > 0) omp_set_num_threads(nthreads);
+    const uint64_t sqrtx = isqrt128(x), cbrtx = icbrt128(x), qrtx = isqrt128(sqrtx);
+    /* q <= sqrt(x/p) < sqrt(x/qrtx): the list covers every q and every p */
+    uint64_t qmax = isqrt128(x / (qrtx + 1));
+    if (qmax < cbrtx) qmax = cbrtx;
+    uint64_t np;
+    uint32_t *P = primes_upto(qmax + 1, &np);
+    pitab_t tab = pitab_build(sqrtx + 1); /* x/(pq) < x/p^2 < sqrt(x) */
+    const uint64_t i0 = pitab_pi(&tab, qrtx), i1 = pitab_pi(&tab, cbrtx);
+    u128 s = 0;
+#pragma omp parallel
+    {
+        u128 ls = 0;
+#pragma omp for schedule(dynamic, 1)
+        for (uint64_t i = i0; i < i1; i++) {
+            const uint64_t p = P[i], xp = x / p, qhi = isqrt128(xp);
+            uint64_t t = 0;
+            for (uint64_t j = i + 1; j < np && P[j] <= qhi; j++) {
+                const uint64_t u = xp / P[j];
+                const uint64_t pu = pitab_pi(&tab, u);
+                t += u < y ? 2 * pu : pu;
+            }
+            ls += t;
+        }
+#pragma omp critical
+        s += ls;
+    }
+    put128((i128)s, out);
+    pitab_free(&tab);
+    free(P);
+    if (nthreads > 0) omp_set_num_threads(saved);
+}
+
+void orc_gourdon_C(uint64_t x, uint64_t y, int nthreads, uint64_t *out)
+{
+    int saved = omp_get_max_threads();
+    if (nthreads > 0) omp_set_num_threads(nthreads);
+    const uint64_t sqrtx = isqrt128(x), qrtx = isqrt128(sqrtx), sqrty = isqrt128(y);
+    uint64_t np;
+    uint32_t *P = primes_upto(y, &np);
+    pitab_t tab = pitab_build((y > sqrtx ? y : sqrtx) + 1); /* pi(q) for q <= y; x/(pq) < p^2 <= sqrt(x) */
+    const uint64_t i0 = pitab_pi(&tab, sqrty), i1 = pitab_pi(&tab, qrtx), jy = pitab_pi(&tab, y);
+    u128 s = 0;
+#pragma omp parallel
+    {
+        u128 ls = 0;
+#pragma omp for schedule(dynamic, 1)
+        for (uint64_t i = i0; i < i1; i++) {
+            const uint64_t p = P[i], xp = x / p, x3 = xp / p / p; /* floor(x / p^3) */
+            if (x3 >= y) continue;
+            const uint64_t b = i + 1; /* pi(p) */
+            uint64_t t = 0;
+            for (uint64_t j = pitab_pi(&tab, x3); j < jy; j++)
+                t += pitab_pi(&tab, xp / P[j]) + 2 - b;
+            ls += t;
+        }
+#pragma omp critical
+        s += ls;
+    }
+    put128((i128)s, out);
+    pitab_free(&tab);
+    free(P);
+    if (nthreads > 0) omp_set_num_threads(saved);
+}
+
 /* ------------------------------------------------------------------ Lehmer */
 
 uint64_t orc_pi_lehmer(uint64_t x)

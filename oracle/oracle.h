@@ -66,6 +66,12 @@ void orc_hard(uint64_t x_lo, uint64_t x_hi, uint64_t y, uint32_t c, uint64_t *ou
 void orc_pi_dr(uint64_t x_lo, uint64_t x_hi, uint64_t y, uint32_t c, int nthreads,
                uint64_t *terms);
 
+/* The reference's OpenMP host terms (Gourdon's A and C, src/Gourdon/A2_cpu.cpp,
+ * src/Gourdon/C_cpu.cpp), restated for the timed CPU baseline; x < 2^64.
+ * out[0..1] = the 128-bit sum (lo, hi).  nthreads <= 0 uses every host thread. */
+void orc_gourdon_A(uint64_t x, uint64_t y, int nthreads, uint64_t *out);
+void orc_gourdon_C(uint64_t x, uint64_t y, int nthreads, uint64_t *out);
+
 #ifdef __cplusplus
 }
 #endif

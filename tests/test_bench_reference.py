@@ -22,6 +22,8 @@ def test_reference_arm_json_line():
     assert line["value"] > 0 and line["higher_is_better"] is True
     assert line["e2e"]["value"] == line["value"] and line["e2e"]["h2d_bytes_per_step"] == 0
     assert line["cpu_baseline"]["kind"] == "port" and line["cpu_baseline"]["cores"] >= 1
+    rt = line["cpu_baseline"]["reference_terms"]
+    assert rt["value"] > 0 and "A2_cpu.cpp" in rt["terms"] and "C_cpu.cpp" in rt["terms"]
     sys.path.insert(0, ROOT)
     import bench
 
