@@ -60,6 +60,8 @@ def lib():
         L.orc_leaf_counts.argtypes = [U64, U64, U64, ctypes.c_uint32, ctypes.c_void_p]
         L.orc_pi_dr.restype = None
         L.orc_pi_dr.argtypes = [U64, U64, U64, ctypes.c_uint32, ctypes.c_int, ctypes.c_void_p]
+        L.orc_pi_gourdon.restype = None
+        L.orc_pi_gourdon.argtypes = [U64, U64, ctypes.c_uint32, ctypes.c_int, ctypes.c_void_p]
         for name in ("orc_gourdon_A", "orc_gourdon_C"):
             getattr(L, name).restype = None
             getattr(L, name).argtypes = [U64, U64, ctypes.c_int, ctypes.c_void_p]
@@ -205,6 +207,20 @@ def gourdon_C(x, y, nthreads=0):
     x/p^3 < q <= y, pi(x/(pq)) - pi(p) + 2."""
     assert 0 < x < 1 << 64
     return _call128(lib().orc_gourdon_C, x, y, nthreads)
+
+
+GOURDON_NAMES = ("A", "B", "C", "D", "phi0", "sigma", "pi")
+
+
+def pi_gourdon(x, y, c=6, nthreads=0):
+    """pi(x) through Gourdon's decomposition A - B + C + D + Phi0 + Sigma (the
+    term names of src/Gourdon/gourdonvariant.hpp:7-56), with
+    x* = max(x^(1/4), x/y^2); a second split of the leaves that the
+    Deleglise-Rivat identity sums.  x < 2^64."""
+    assert 0 < x < 1 << 64
+    out = (U64 * 14)()
+    lib().orc_pi_gourdon(x, y, c, nthreads, out)
+    return {k: _s128(out[2 * i], out[2 * i + 1]) for i, k in enumerate(GOURDON_NAMES)}
 
 
 def default_y(x, alpha_num=1, alpha_den=1):

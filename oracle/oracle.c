@@ -563,10 +563,12 @@ static i128 term_ordinary(const drctx_t *D, const int8_t *mu, const uint32_t *lp
     return s;
 }
 
-static i128 term_easy(const drctx_t *D, const int8_t *mu, const uint32_t *lpf)
+/* easy leaves of every p_b <= iroot4(x) and of iroot4(x) < p_b <= p_bmax
+ * (bmax = pi(cbrt x) gives all of them) */
+static i128 term_easy_upto(const drctx_t *D, const int8_t *mu, const uint32_t *lpf, uint64_t bmax)
 {
     i128 s = 0;
-    uint64_t blo = pitab_pi(&D->tab, D->qrtx) + 1, bhi = pitab_pi(&D->tab, D->cbrtx);
+    uint64_t blo = pitab_pi(&D->tab, D->qrtx) + 1, bhi = bmax;
     /* (ii) p_b <= iroot4(x): leaves with x/(p m) < p^2, i.e. m > x/p^3 */
     const uint64_t c = D->c;
 #pragma omp parallel
@@ -616,6 +618,11 @@ static i128 term_easy(const drctx_t *D, const int8_t *mu, const uint32_t *lpf)
         s += ls;
     }
     return s;
+}
+
+static i128 term_easy(const drctx_t *D, const int8_t *mu, const uint32_t *lpf)
+{
+    return term_easy_upto(D, mu, lpf, pitab_pi(&D->tab, D->cbrtx));
 }
 
 /* hard leaves by a segmented phi sieve over [0, z]; chunks of consecutive
@@ -990,6 +997,32 @@ void orc_pi_dr(uint64_t x_lo, uint64_t x_hi, uint64_t y, uint32_t c, int nthread
  * follows the sum.  C is then exactly the easy leaves (p, q) of the
  * special-leaf sum with q prime and p > sqrt(y).  Both sums are positive;
  * x < 2^64 as in the reference's GourdonVariant64. */
+/* A over the primes p = P[i], i0 <= i < i1; P holds every prime to
+ * sqrt(x / P[i0]) and tab covers sqrt(x) */
+static u128 gourdon_A_sum(uint64_t x, uint64_t y, const uint32_t *P, uint64_t np, const pitab_t *tab,
+                          uint64_t i0, uint64_t i1)
+{
+    u128 s = 0;
+#pragma omp parallel
+    {
+        u128 ls = 0;
+#pragma omp for schedule(dynamic, 1)
+        for (uint64_t i = i0; i < i1; i++) {
+            const uint64_t p = P[i], xp = x / p, qhi = isqrt128(xp);
+            uint64_t t = 0;
+            for (uint64_t j = i + 1; j < np && P[j] <= qhi; j++) {
+                const uint64_t u = xp / P[j];
+                const uint64_t pu = pitab_pi(tab, u);
+                t += u < y ? 2 * pu : pu;
+            }
+            ls += t;
+        }
+#pragma omp critical
+        s += ls;
+    }
+    return s;
+}
+
 void orc_gourdon_A(uint64_t x, uint64_t y, int nthreads, uint64_t *out)
 {
     int saved = omp_get_max_threads();
@@ -1002,25 +1035,7 @@ void orc_gourdon_A(uint64_t x, uint64_t y, int nthreads, uint64_t *out)
     uint32_t *P = primes_upto(qmax + 1, &np);
     pitab_t tab = pitab_build(sqrtx + 1); /* x/(pq) < x/p^2 < sqrt(x) */
     const uint64_t i0 = pitab_pi(&tab, qrtx), i1 = pitab_pi(&tab, cbrtx);
-    u128 s = 0;
-#pragma omp parallel
-    {
-        u128 ls = 0;
-#pragma omp for schedule(dynamic, 1)
-        for (uint64_t i = i0; i < i1; i++) {
-            const uint64_t p = P[i], xp = x / p, qhi = isqrt128(xp);
-            uint64_t t = 0;
-            for (uint64_t j = i + 1; j < np && P[j] <= qhi; j++) {
-                const uint64_t u = xp / P[j];
-                const uint64_t pu = pitab_pi(&tab, u);
-                t += u < y ? 2 * pu : pu;
-            }
-            ls += t;
-        }
-#pragma omp critical
-        s += ls;
-    }
-    put128((i128)s, out);
+    put128((i128)gourdon_A_sum(x, y, P, np, &tab, i0, i1), out);
     pitab_free(&tab);
     free(P);
     if (nthreads > 0) omp_set_num_threads(saved);
@@ -1055,6 +1070,103 @@ void orc_gourdon_C(uint64_t x, uint64_t y, int nthreads, uint64_t *out)
     put128((i128)s, out);
     pitab_free(&tab);
     free(P);
+    if (nthreads > 0) omp_set_num_threads(saved);
+}
+
+/* Gourdon's decomposition of pi(x), the second split of the same special-leaf
+ * sum, as the reference's Gourdon code names its terms:
+ *   pi(x) = A - B + C + D + Phi0 + Sigma0 + ... + Sigma6
+ * with a = pi(y), b3 = pi(cbrt x), bs = pi(sqrt x), cz = pi(sqrt z), z = x/y, and
+ * x* = min(max(iroot4(x), x/y^2), cbrt x), d = pi(x*), and cz = pi(sqrt z) held
+ * within [d, b3] (sqrt z splits the p of (x*, cbrt x]):
+ *   A      = sum_{x* < p <= cbrt x} sum_{p < q <= sqrt(x/p)} chi(x/pq) pi(x/pq)   (as orc_gourdon_A)
+ *   B      = sum_{y < p <= sqrt x} pi(x/p)                          src/Gourdon/B.cu:16-71
+ *   C      = the easy and trivial leaves (x/(p_b m) < p_b^2) of every p_b <= x*, b > c
+ *   D      = the hard leaves (p_b <= iroot4(x), x/(p_b m) >= p_b^2)  src/Gourdon/gourdonvariant.cpp:61
+ *   Phi0   = the ordinary leaves                                     src/Gourdon/phi_0.cpp:5-8
+ *   Sigma0 = a - 1 + bs(bs-1)/2 - a(a-1)/2                           src/Gourdon/sigma_cpu.cpp:36-43
+ *   Sigma1 = (a - b3)(a - b3 - 1)/2                                  :45-50
+ *   Sigma2 = a (b3 - cz - cz(cz-3)/2 + d(d-3)/2)                     :52-60
+ *   Sigma3 = b3(b3-1)(2b3-1)/6 - b3 - d(d-1)(2d-1)/6 + d             :62-71
+ *   Sigma4 = a sum_{x* < p <= sqrt z} pi(x/(p y))                    :73-96
+ *   Sigma5 = sum_{sqrt z < p <= cbrt x} pi(x/p^2)                    :98-119
+ *   Sigma6 = -sum_{x* < p <= cbrt x} pi(sqrt(x/p))^2                 :121-146
+ * The reference fixes x* = x^(1/4) (qrtx throughout its Gourdon code), which
+ * is exact only when sqrt(x/p) <= y for every p > x^(1/4), i.e. y >= ~x^(3/8);
+ * with x* = max(x^(1/4), x/y^2) every y of the Deleglise-Rivat domain works:
+ * for x^(1/4) < p <= x/y^2 no leaf is hard, so those p join C (with trivial
+ * leaves only when y < cbrt x, where x* stops at cbrt x).
+ * Derivation per p > x*: the easy leaves q in (p, min(y, x/p^2)] are summed
+ * as the pairs q <= sqrt(x/p) plus, by the hyperbola method, the pairs with
+ * q > sqrt(x/p) counted from the small side, which doubles pi(x/pq) where
+ * x/pq < y (chi) and leaves the closed forms above.  x < 2^64, as in the
+ * reference's GourdonVariant64.  terms[2k..2k+1] receives A, B, C, D, Phi0,
+ * Sigma (the sum of the seven) and pi(x) as signed 128-bit pairs. */
+void orc_pi_gourdon(uint64_t x, uint64_t y, uint32_t c, int nthreads, uint64_t *terms)
+{
+    int saved = omp_get_max_threads();
+    if (nthreads > 0) omp_set_num_threads(nthreads);
+    uint64_t len = y / 2 + 1;
+    int8_t *mu = (int8_t *)malloc(len);
+    uint32_t *lpf = (uint32_t *)malloc(len * 4);
+    orc_mu_lpf(0, 2 * len, mu, lpf);
+    drctx_t D;
+    dr_init(&D, x, y, c, tabmax_for(x, y));
+    const pitab_t *T = &D.tab;
+    const uint64_t xy2 = (uint64_t)((u128)x / ((u128)y * y));
+    uint64_t xs = D.qrtx > xy2 ? D.qrtx : xy2;
+    if (xs > D.cbrtx) xs = D.cbrtx;
+    const uint64_t sz = isqrt128(D.z);
+    const i128 a = pitab_pi(T, y), b3 = pitab_pi(T, D.cbrtx), bs = pitab_pi(T, D.sqrtx);
+    const i128 d = pitab_pi(T, xs), cz0 = pitab_pi(T, sz);
+    const i128 cz = cz0 < d ? d : (cz0 > b3 ? b3 : cz0); /* the split of (x*, cbrt x] at sqrt z */
+
+    const i128 A = (i128)gourdon_A_sum(x, y, D.P, D.np, T, (uint64_t)d, (uint64_t)b3);
+    i128 B = 0;
+#pragma omp parallel
+    {
+        i128 ls = 0;
+#pragma omp for schedule(static)
+        for (uint64_t i = (uint64_t)a; i < (uint64_t)bs; i++) ls += pitab_pi(T, x / D.P[i]);
+#pragma omp critical
+        B += ls;
+    }
+    i128 C = term_easy_upto(&D, mu, lpf, (uint64_t)d);
+    for (uint64_t i = pitab_pi(T, D.qrtx); i < (uint64_t)d; i++) {
+        /* trivial leaves q in (x/p^2, y] of a p <= x*: only where y < cbrt x */
+        const uint64_t v = x / D.P[i] / D.P[i];
+        if (v < y) C += a - (i128)pitab_pi(T, v);
+    }
+    const i128 Dh = term_hard(&D, mu, lpf);
+    const i128 phi0 = term_ordinary(&D, mu, lpf);
+
+    i128 sg[7];
+    sg[0] = a - 1 + bs * (bs - 1) / 2 - a * (a - 1) / 2;
+    sg[1] = (a - b3) * (a - b3 - 1) / 2;
+    sg[2] = a * (b3 - cz - cz * (cz - 3) / 2 + d * (d - 3) / 2);
+    sg[3] = b3 * (b3 - 1) * (2 * b3 - 1) / 6 - b3 - d * (d - 1) * (2 * d - 1) / 6 + d;
+    sg[4] = sg[5] = sg[6] = 0;
+    for (uint64_t i = (uint64_t)d; i < (uint64_t)b3; i++) {
+        const uint64_t p = D.P[i];
+        if (i < (uint64_t)cz) sg[4] += pitab_pi(T, x / p / y);
+        else sg[5] += pitab_pi(T, x / p / p);
+        const i128 r = pitab_pi(T, isqrt128(x / p));
+        sg[6] -= r * r;
+    }
+    sg[4] *= a;
+    i128 sigma = 0;
+    for (int k = 0; k < 7; k++) sigma += sg[k];
+
+    put128(A, terms + 0);
+    put128(B, terms + 2);
+    put128(C, terms + 4);
+    put128(Dh, terms + 6);
+    put128(phi0, terms + 8);
+    put128(sigma, terms + 10);
+    put128(A - B + C + Dh + phi0 + sigma, terms + 12);
+    dr_free(&D);
+    free(mu);
+    free(lpf);
     if (nthreads > 0) omp_set_num_threads(saved);
 }
 

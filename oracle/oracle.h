@@ -72,6 +72,11 @@ void orc_pi_dr(uint64_t x_lo, uint64_t x_hi, uint64_t y, uint32_t c, int nthread
 void orc_gourdon_A(uint64_t x, uint64_t y, int nthreads, uint64_t *out);
 void orc_gourdon_C(uint64_t x, uint64_t y, int nthreads, uint64_t *out);
 
+/* pi(x) through Gourdon's decomposition pi(x) = A - B + C + D + Phi0 + Sigma,
+ * a second split of the same leaves (x < 2^64).  terms[2k..2k+1] receives A,
+ * B, C, D, Phi0, Sigma, pi(x) as signed 128-bit pairs. */
+void orc_pi_gourdon(uint64_t x, uint64_t y, uint32_t c, int nthreads, uint64_t *terms);
+
 #ifdef __cplusplus
 }
 #endif

@@ -1,7 +1,10 @@
-"""The restatement of the reference's OpenMP host terms (Gourdon's A and C,
-src/Gourdon/A2_cpu.cpp:20-134 and src/Gourdon/C_cpu.cpp:20-78), which bench.py
-times as the reference's CPU path for those terms, against the sums written
-out from their definitions over a plain Python prime list.  CPU only."""
+"""Gourdon's decomposition in the oracle.  The restatement of the reference's
+OpenMP host terms (Gourdon's A and C, src/Gourdon/A2_cpu.cpp:20-134 and
+src/Gourdon/C_cpu.cpp:20-78), which bench.py times as the reference's CPU path
+for those terms, against the sums written out from their definitions over a
+plain Python prime list; and pi(x) through the whole decomposition
+A - B + C + D + Phi0 + Sigma against published and sympy values, a second
+split of the leaves beside the Deleglise-Rivat one.  CPU only."""
 import bisect
 import math
 
@@ -74,3 +77,41 @@ def test_gourdon_y_at_sqrt_edge(orc):
     A, C = _brute(x, y)
     assert orc.gourdon_A(x, y) == A
     assert orc.gourdon_C(x, y) == C
+
+
+@pytest.mark.parametrize("k", range(6, 16))
+def test_gourdon_pi_pow10(orc, golden, k):
+    # alpha 1 puts x/y^2 above x^(1/4) (x* = x/y^2), alpha 30 below it
+    x = 10**k
+    for alpha in (1, 4, 30):
+        y = orc.default_y(x, alpha)
+        assert orc.pi_gourdon(x, y)["pi"] == golden["pi_pow10"][str(k)], (k, alpha)
+
+
+def test_gourdon_pi_random(orc, golden):
+    for i, (x, p) in enumerate(golden["pi_random"]):
+        if x < 10**6:
+            continue
+        y = orc.default_y(x, (1, 3, 17)[i % 3])
+        assert orc.pi_gourdon(x, y)["pi"] == p, x
+
+
+def test_gourdon_terms_against_dr(orc):
+    # y >= x^(3/8): x* = x^(1/4), the reference's own setting
+    x = 10**12 + 39
+    y = orc.default_y(x, 20)
+    assert x // (y * y) <= math.isqrt(math.isqrt(x))
+    g = orc.pi_gourdon(x, y)
+    t = orc.pi_dr(x, y)
+    assert g["D"] == t["hard"] and g["phi0"] == t["ordinary"]
+    assert g["A"] == orc.gourdon_A(x, y)
+    assert g["pi"] == t["pi"]
+
+
+def test_gourdon_y_range_edges(orc):
+    # y = floor(cbrt x) below the real cube root (x* stops at cbrt x, sqrt z lies above it)
+    # and y just under sqrt x
+    for x in (387452, 7164126, 13091049675, 10**11 + 3):
+        p = orc.pi_lehmer(x)
+        for y in (orc.icbrt(x), orc.icbrt(x) + 1, orc.isqrt(x) - 1):
+            assert orc.pi_gourdon(x, y)["pi"] == p, (x, y)
