@@ -533,6 +533,7 @@ class PiTable:
         self._buf = None
         self._alloc()
         self.pi_base = None
+        self._pi_base_at = None  # the base that pi_base belongs to
 
     def _alloc(self):
         L = load()
@@ -556,16 +557,45 @@ class PiTable:
         return self.bottom
 
     def get_pi_base(self):
+        """pi(base - 1), counted on first use after the base changes
+        (src/pitable.cu:154-166)."""
         if self.base == 0:
             return 0
-        return count_primes(0, self.base, ctx=self.ctx)
+        if self._pi_base_at != self.base:
+            self.pi_base = count_primes(0, self.base, ctx=self.ctx)
+            self._pi_base_at = self.base
+        return self.pi_base
+
+    def set_pi_base(self, pi_base):
+        """A caller's pi(base - 1) (src/pitable.cu:175-179), kept until the base
+        changes; the next window fill replaces it by the exact count."""
+        self.pi_base = int(pi_base)
+        self._pi_base_at = self.base
 
     def set_base(self, base):
         self.base = int(base)
 
     def set_range(self, rng):
+        """Unlike the reference (src/pitable.cu:181-186), the buffer follows
+        the new range."""
         self.range = int(rng)
         self._alloc()
+
+    def allocate(self):
+        """Keeps an existing buffer (src/pitable.cu:63-68); contents are
+        written by the next getCurrent / getNextUp / getNextDown."""
+        if self._buf is None or not self._buf.ptr:
+            self._alloc()
+
+    def reallocate(self):
+        """A new buffer for the current range (src/pitable.cu:70-75)."""
+        self._alloc()
+
+    def setMaxRange(self):
+        """range = getMaxRange(), then reallocate (src/pitable.cu:56-61)."""
+        self.range = self.getMaxRange()
+        self._alloc()
+        return self.range
 
     def set_bottom(self, bottom):
         self.bottom = int(bottom)
@@ -574,6 +604,7 @@ class PiTable:
         pb = ctypes.c_uint64()
         self.ctx.call("cpx_pitable_window", self.base, self.range, self._buf.ptr, ctypes.byref(pb))
         self.pi_base = pb.value
+        self._pi_base_at = self.base
         return self._buf
 
     def getCurrent(self):

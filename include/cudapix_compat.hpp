@@ -157,6 +157,7 @@ inline void gen_d_mu_lpf(uint64_t bottom, uint64_t top, int8_t *d_mu, uint64_t *
 
 class PiTable {
     uint64_t base = 0, range = 0, bottom = 0, pi_base = 0;
+    bool pi_current = false;  // pi_base belongs to the current base
     uint32_t *d_pitable = nullptr;
 
     void alloc()
@@ -169,6 +170,7 @@ class PiTable {
     uint32_t *fill()
     {
         cudapix_compat::ok(cpx_pitable_window(cudapix_compat::ctx(), base, range, d_pitable, &pi_base));
+        pi_current = true;
         return d_pitable;
     }
 
@@ -187,8 +189,29 @@ class PiTable {
     uint64_t get_base() { return base; }
     uint64_t get_range() { return range; }
     uint64_t get_bottom() { return bottom; }
-    uint64_t get_pi_base() { return pi_base; }
-    void set_base(uint64_t b) { base = b; }
+    // pi(base - 1): counted on first use after the base changes (src/pitable.cu:154-166)
+    uint64_t get_pi_base()
+    {
+        if (base == 0) return 0;
+        if (!pi_current) {
+            cudapix_compat::ok(cpx_count_primes(cudapix_compat::ctx(), 0, base, &pi_base));
+            pi_current = true;
+        }
+        return pi_base;
+    }
+    // a caller's pi(base - 1), kept until the base changes (src/pitable.cu:175-179); the
+    // next window fill replaces it by the exact count
+    void set_pi_base(uint64_t v)
+    {
+        pi_base = v;
+        pi_current = true;
+    }
+    void set_base(uint64_t b)
+    {
+        base = b;
+        pi_current = false;
+    }
+    // unlike the reference (src/pitable.cu:181-186), the buffer follows the new range
     void set_range(uint64_t r)
     {
         range = r;
@@ -200,6 +223,19 @@ class PiTable {
         uint64_t f = 0, t = 0;
         cudapix_compat::ok(cpx_mem_info(cudapix_compat::ctx(), &f, &t));
         return (uint64_t)(f / 2.5);
+    }
+    // src/pitable.cu:56-75: allocate() keeps an existing buffer, reallocate() replaces it;
+    // the contents are written by the next getCurrent / getNextUp / getNextDown
+    void allocate()
+    {
+        if (!d_pitable) alloc();
+    }
+    void reallocate() { alloc(); }
+    uint64_t setMaxRange()
+    {
+        range = getMaxRange();
+        reallocate();
+        return range;
     }
     uint32_t *getCurrent() { return fill(); }
     uint32_t *getNextUp()

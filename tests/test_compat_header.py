@@ -19,6 +19,8 @@ int main() {
   uint32_t *lpf = gen_d_lpf<uint32_t>(0u, 1000u);
   uint32_t *pt = get_d_piTable(1000);
   PiTable w(1000000, 0, 4096); w.getCurrent(); w.getNextDown();
+  w.set_pi_base(w.get_pi_base()); w.allocate(); w.reallocate(); (void)w.getNextBaseDown();
+  PiTable big(1 << 20); (void)big.setMaxRange();
   Phi f(1000); uint64_t ph = f.phi(100000, 5);
   Phisieve s(1000, 1 << 16); s.firstSieve(6); s.markNext(); s.updateCount();
   uint64_t h = S2hardHost::S2hard(1000000000000ull, 100000, 6);

@@ -95,6 +95,23 @@ def test_pitable_walk(ctx, cpx, orc):
     assert t[77] + pt.pi_base == orc.pi_sieve(b0 + 153)
 
 
+def test_pitable_pi_base_and_buffers(ctx, cpx, orc):
+    pt = cpx.PiTable(2_000_000, 1_000_000, 100_000, ctx=ctx)
+    want = orc.pi_sieve(1_999_999)
+    assert pt.get_pi_base() == want  # counted before any window is filled
+    pt.set_pi_base(want)  # a caller's value is kept for this base
+    assert pt.get_pi_base() == want
+    pt.set_base(1_500_000)
+    assert pt.get_pi_base() == orc.pi_sieve(1_499_999)  # a new base is counted again
+    buf = pt._buf.ptr
+    pt.allocate()
+    assert pt._buf.ptr == buf  # allocate() keeps an existing buffer
+    pt.reallocate()
+    t = pt.getCurrent().to_host()
+    assert pt.pi_base == orc.pi_sieve(1_499_999)
+    assert t[7] + pt.pi_base == orc.pi_sieve(1_500_013)
+
+
 @pytest.mark.parametrize("lo,hi", [(0, 100), (0, 2), (2, 3), (90, 97), (10**9, 10**9 + 10**6), (10**13, 10**13 + 10**5)])
 def test_primes_and_counts(ctx, cpx, orc, lo, hi):
     p = cpx.get_device_primes(lo, hi, ctx=ctx).to_host()
