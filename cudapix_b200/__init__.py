@@ -21,6 +21,7 @@ Errors raise CpxError (the reference checked none).  Every value is an exact
 Python int; 64- and 128-bit overloads are chosen by the size of x.
 """
 import ctypes
+import math
 import os
 
 import numpy as np
@@ -640,6 +641,39 @@ class Phi:
         self.ctx = ctx or context()
         self.max = int(max_)
         self.p_max = p_max
+        self._lpf = None
+        self._primes = None
+
+    def get_d_lpf(self):
+        """lpf of the odd n in [0, max) (src/phi.cu:16), built on first use."""
+        if self._lpf is None:
+            self._lpf = gen_d_lpf(0, self.max, ctx=self.ctx)
+        return self._lpf
+
+    def get_h_primeList(self):
+        """The sieving primes after the 12 small primes 2 .. 37, up to p_max
+        (default isqrt(max)), as PrimeList::getSievingPrimes gives them
+        (src/phi.cu:20,30)."""
+        if self._primes is None:
+            top = self.p_max if self.p_max is not None else math.isqrt(self.max)
+            self._primes = get_device_primes(41, top + 1, ctx=self.ctx).to_host().astype(np.uint32)
+        return self._primes
+
+    def get_d_primeList(self):
+        h = self.get_h_primeList()
+        p = ctypes.c_void_p()
+        _check(None, load().cpx_device_alloc(max(1, h.size) * 4, ctypes.byref(p)))
+        arr = DeviceArray(p.value, h.size, "uint32")
+        if h.size:
+            _check(None, load().cpx_copy_to_device(p.value, h.ctypes.data, h.size * 4))
+        return arr
+
+    def get_primeListLength(self):
+        return int(self.get_h_primeList().size)
+
+    def makeModCache(self, pi_max):
+        """The reference fills a private cache that phi() never reads
+        (src/phi.cu:58-73); phi() here is exact without it."""
 
     def phi(self, x, a):
         return self.phi_std(x, a + 1)
@@ -685,6 +719,11 @@ class Phisieve:
         a = ctypes.c_uint32()
         self._c("cpx_phisieve_counts", None, ctypes.byref(a))
         return a.value
+
+    def set_a_current(self, a):
+        """The next markNext crosses off p_(a+1); the bitmap is left as it is
+        (include/sieve/phisieve_host.cuh:37)."""
+        self._c("cpx_phisieve_set_a", a)
 
     def getCountDevice(self):
         p, a = ctypes.c_void_p(), ctypes.c_uint32()

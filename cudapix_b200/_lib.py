@@ -211,6 +211,7 @@ _SIGS = {
     "cpx_phisieve_mark_next": (ctypes.c_int, [P]),
     "cpx_phisieve_update": (ctypes.c_int, [P]),
     "cpx_phisieve_counts": (ctypes.c_int, [P, PP, pu32]),
+    "cpx_phisieve_set_a": (ctypes.c_int, [P, ctypes.c_uint32]),
     "cpx_pi_batch": (ctypes.c_int, [P, pU, ctypes.c_size_t, ctypes.POINTER(Params), pU]),
     "cpx_terms_batch": (ctypes.c_int, [P, pU, pu64, ctypes.c_size_t, ctypes.POINTER(Params), ctypes.POINTER(Terms)]),
     "cpx_mem_info": (ctypes.c_int, [P, pu64, pu64]),

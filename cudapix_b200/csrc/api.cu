@@ -841,4 +841,12 @@ int cpx_phisieve_counts(cpx_phisieve *ps, uint32_t **d_counts, uint32_t *a_curre
     return CPX_OK;
 }
 
+// mark_next checks the value when it is used (a = 0, or p_{a+1} beyond 32 bits)
+int cpx_phisieve_set_a(cpx_phisieve *ps, uint32_t a_current)
+{
+    if (!ps) return CPX_EINVAL;
+    ps->a = a_current;
+    return CPX_OK;
+}
+
 }  // extern "C"

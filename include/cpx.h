@@ -220,6 +220,9 @@ int cpx_phisieve_first(cpx_phisieve *ps, uint16_t c);
 int cpx_phisieve_mark_next(cpx_phisieve *ps);
 int cpx_phisieve_update(cpx_phisieve *ps);
 int cpx_phisieve_counts(cpx_phisieve *ps, uint32_t **d_counts, uint32_t *a_current);
+/* Phisieve::set_a_current (include/sieve/phisieve_host.cuh:37): the next
+ * mark_next crosses off p_{a+1}; the bitmap is left as it is. */
+int cpx_phisieve_set_a(cpx_phisieve *ps, uint32_t a_current);
 
 /* ---- batched and served evaluation -------------------------------------- */
 /* cpx_params.flags */

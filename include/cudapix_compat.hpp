@@ -26,6 +26,7 @@
 // results are exact (the reference's easy + hard split was off by ~1 ppm).
 #pragma once
 #include <algorithm>
+#include <cmath>
 #include <cstdio>
 #include <cstdlib>
 #include <cstdint>
@@ -259,9 +260,72 @@ class PiTable {
 // phi(x, a) with the reference's prime index: a selects p = smallPrimes[a]
 // (0-based: a = 0 -> 2), i.e. the first a + 1 primes are excluded.
 class Phi {
+    uint32_t max_, p_max_;
+    uint32_t *d_lpf = nullptr, *d_primeList = nullptr, *h_primeList = nullptr, primeListLength = 0;
+
+    static uint32_t isqrt32(uint32_t m)
+    {
+        uint64_t r = (uint64_t)std::sqrt((double)m);
+        while (r * r > m) r--;
+        while ((r + 1) * (r + 1) <= m) r++;
+        return (uint32_t)r;
+    }
+    // the sieving primes after the 12 small primes 2 .. 37, up to p_max
+    // (PrimeList::getSievingPrimes in src/phi.cu:20,30), built on first use
+    void primes()
+    {
+        if (h_primeList) return;
+        uint64_t *d = nullptr, n = 0;
+        cudapix_compat::ok(cpx_primes(cudapix_compat::ctx(), 41, (uint64_t)p_max_ + 1, &d, &n));
+        std::vector<uint64_t> h(n);
+        if (n) cudapix_compat::ok(cpx_copy_to_host(h.data(), d, n * 8));
+        cpx_free(d);
+        h_primeList = (uint32_t *)std::malloc((n ? n : 1) * 4);
+        for (uint64_t i = 0; i < n; i++) h_primeList[i] = (uint32_t)h[i];
+        void *p = nullptr;
+        cudapix_compat::ok(cpx_device_alloc((n ? n : 1) * 4, &p));
+        d_primeList = (uint32_t *)p;
+        if (n) cudapix_compat::ok(cpx_copy_to_device(d_primeList, h_primeList, n * 4));
+        primeListLength = (uint32_t)n;
+    }
+
   public:
-    explicit Phi(uint32_t) {}
-    Phi(uint32_t, uint32_t) {}
+    explicit Phi(uint32_t max) : max_(max), p_max_(isqrt32(max)) {}
+    Phi(uint32_t max, uint32_t p_max) : max_(max), p_max_(p_max) {}
+    ~Phi()
+    {
+        if (d_lpf) cpx_free(d_lpf);
+        if (d_primeList) cpx_free(d_primeList);
+        std::free(h_primeList);
+    }
+    Phi(const Phi &) = delete;
+    Phi &operator=(const Phi &) = delete;
+
+    // lpf of the odd n in [0, max) (src/phi.cu:16), built on first use; owned by the Phi
+    uint32_t *get_d_lpf()
+    {
+        if (!d_lpf) d_lpf = gen_d_lpf<uint32_t>(0u, max_);
+        return d_lpf;
+    }
+    uint32_t *get_d_primeList()
+    {
+        primes();
+        return d_primeList;
+    }
+    uint32_t *get_h_primeList()
+    {
+        primes();
+        return h_primeList;
+    }
+    uint32_t get_primeListLength()
+    {
+        primes();
+        return primeListLength;
+    }
+    // The reference fills a private cache that phi() never reads (src/phi.cu:58-73);
+    // phi() here is exact without it, so there is nothing to build.
+    void makeModCache(uint32_t) {}
+
     uint64_t phi(uint32_t x, uint32_t a)
     {
         uint64_t r;
@@ -308,6 +372,7 @@ class Phisieve {
         cudapix_compat::ok(cpx_phisieve_counts(ps, nullptr, &a));
         return a;
     }
+    void set_a_current(uint32_t a) { cudapix_compat::ok(cpx_phisieve_set_a(ps, a)); }
 };
 
 struct S2hardHost {

@@ -22,7 +22,12 @@ int main() {
   w.set_pi_base(w.get_pi_base()); w.allocate(); w.reallocate(); (void)w.getNextBaseDown();
   PiTable big(1 << 20); (void)big.setMaxRange();
   Phi f(1000); uint64_t ph = f.phi(100000, 5);
+  f.makeModCache(8); uint32_t *fl = f.get_d_lpf(); uint32_t np = f.get_primeListLength();
+  uint32_t *hp = f.get_h_primeList(); uint32_t *dp = f.get_d_primeList();
+  Phi g(1 << 20, 2000); (void)g.get_h_primeList();
   Phisieve s(1000, 1 << 16); s.firstSieve(6); s.markNext(); s.updateCount();
+  s.set_a_current(s.get_a_current()); s.markNext();
+  (void)fl; (void)np; (void)hp; (void)dp;
   uint64_t h = S2hardHost::S2hard(1000000000000ull, 100000, 6);
   uint64_t p = deleglise_rivat64::pi_deleglise_rivat(1000000000000ull, 100000, 6);
   uint128_t q = deleglise_rivat128::pi_deleglise_rivat((uint128_t)1 << 70, 0, 6);

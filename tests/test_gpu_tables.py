@@ -147,6 +147,25 @@ def test_phi_range(ctx, cpx, orc):
         assert int(t[i]) == orc.phi(2 * i + 1, 6)
 
 
+def test_phi_getters_and_phisieve_set_a(ctx, cpx, orc):
+    ph = cpx.Phi(10**6, ctx=ctx)
+    _, lpf_o = orc.mu_lpf(0, 10**6)
+    assert np.array_equal(ph.get_d_lpf().to_host(), lpf_o)
+    pl = ph.get_h_primeList()  # primes 41 .. isqrt(10^6), after the 12 small primes
+    assert pl[0] == 41 and pl[-1] == 997 and ph.get_primeListLength() == 168 - 12
+    assert np.array_equal(ph.get_d_primeList().to_host(), pl)
+    ph.makeModCache(8)
+    assert ph.phi(10**5, 5) == orc.phi(10**5, 6)
+    ps = cpx.Phisieve(1000, 1 << 16, ctx=ctx)
+    ps.firstSieve(6)
+    ps.set_a_current(6)  # as it was: the next markNext crosses off p_7 = 17
+    ps.markNext()
+    ps.updateCount()
+    assert np.array_equal(ps.getCountHost(), orc.phisieve_counts(7, 1 << 16))
+    ps.set_a_current(3)
+    assert ps.get_a_current() == 3
+
+
 def test_phisieve(ctx, cpx, orc):
     ps = cpx.Phisieve(1000, 1 << 16, ctx=ctx)
     ps.firstSieve(6)
