@@ -263,7 +263,13 @@ def S2_easy(x, y, c=6, ctx=None):
     return o.value
 
 
-def S2hard(x, y, c=6, ctx=None):
+def S2hard(x, y, c=6, ctx=None, maxPrime=None):
+    """Hard leaves of the exact split (x/(p_b m) >= p_b^2, so p_b <= x^(1/4)).
+    maxPrime caps the sieving primes (include/sieve/S2_hard_host.cuh:36); as
+    hard leaves stop at x^(1/4), any cap >= x^(1/4) gives all of them and a
+    smaller one raises ValueError."""
+    if maxPrime is not None and maxPrime < math.isqrt(math.isqrt(x)):
+        raise ValueError("S2hard with maxPrime below x^(1/4) is not supported")
     ctx = ctx or context()
     if _wide(x):
         o = U128()

@@ -375,12 +375,29 @@ class Phisieve {
     void set_a_current(uint32_t a) { cudapix_compat::ok(cpx_phisieve_set_a(ps, a)); }
 };
 
+// The hard leaves of this library's exact split (x/(p_b m) >= p_b^2, so
+// p_b <= x^(1/4)); with S2_easy and the trivial leaves they give the
+// reference's S2 + S3 exactly (its own split between the two is off by ~1 ppm).
 struct S2hardHost {
     static uint64_t S2hard(uint64_t x, uint64_t y, uint16_t c)
     {
         int64_t r;
         cudapix_compat::ok(cpx_S2_hard_u64(cudapix_compat::ctx(), x, y, c, &r));
         return (uint64_t)r;
+    }
+    // maxPrime caps the sieving primes (include/sieve/S2_hard_host.cuh:36).  Hard
+    // leaves stop at x^(1/4), so any maxPrime >= x^(1/4) (the reference's one call
+    // with it, src/Gourdon/gourdonvariant.cpp:61, passes x^(1/4)) gives all of them;
+    // a smaller cap is refused.
+    static uint64_t S2hard(uint64_t x, uint64_t y, uint16_t c, uint64_t maxPrime)
+    {
+        uint64_t sx, cx, qx;
+        cudapix_compat::ok(cpx_iroots(cpx_u128{x, 0}, &sx, &cx, &qx));
+        if (maxPrime < qx) {
+            std::fprintf(stderr, "cudapix_b200: S2hard with maxPrime below x^(1/4) is not supported\n");
+            std::abort();
+        }
+        return S2hard(x, y, c);
     }
 };
 

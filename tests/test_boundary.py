@@ -4,6 +4,7 @@ GPU.  CPU only."""
 import ctypes
 
 import numpy as np
+import pytest
 
 
 def test_exports_every_declared_symbol():
@@ -75,3 +76,10 @@ def test_null_context_rejected():
     out = ctypes.c_uint64()
     assert L.cpx_P2_u64(None, 10**12, 10**5, ctypes.byref(out)) == _lib.CPX_EINVAL
     assert L.cpx_destroy(None) == _lib.CPX_EINVAL
+
+
+def test_s2hard_max_prime_below_quarter_root_refused():
+    import cudapix_b200 as cpx
+
+    with pytest.raises(ValueError):
+        cpx.S2hard(10**12, 10**5, 6, maxPrime=999)

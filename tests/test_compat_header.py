@@ -29,10 +29,11 @@ int main() {
   s.set_a_current(s.get_a_current()); s.markNext();
   (void)fl; (void)np; (void)hp; (void)dp;
   uint64_t h = S2hardHost::S2hard(1000000000000ull, 100000, 6);
+  uint64_t h4 = S2hardHost::S2hard(1000000000000ull, 100000, 6, 1000);
   uint64_t p = deleglise_rivat64::pi_deleglise_rivat(1000000000000ull, 100000, 6);
   uint128_t q = deleglise_rivat128::pi_deleglise_rivat((uint128_t)1 << 70, 0, 6);
   cpx_free(mu); cpx_free(lpf); cpx_free(pt);
-  return (int)(a + (uint64_t)b + t + o + (uint64_t)o2 + ph + h + p + (uint64_t)q + mutest(100));
+  return (int)(a + (uint64_t)b + t + o + (uint64_t)o2 + ph + h + h4 + p + (uint64_t)q + mutest(100));
 }
 """
 

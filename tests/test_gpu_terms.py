@@ -26,6 +26,7 @@ def test_single_term_entry_points(ctx, cpx, orc, x, y):
     assert cpx.Ordinary(x, y, 6, ctx=ctx) == orc.ordinary(x, y, 6)
     assert cpx.S2_easy(x, y, ctx=ctx) == orc.easy(x, y)
     assert cpx.S2hard(x, y, 6, ctx=ctx) == orc.hard(x, y, 6)
+    assert cpx.S2hard(x, y, 6, ctx=ctx, maxPrime=orc.iroot4(x)) == orc.hard(x, y, 6)
 
 
 @pytest.mark.parametrize("c", [1, 2, 3, 4, 5, 7, 8])
