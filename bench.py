@@ -120,14 +120,94 @@ def peaks():
         return 6650.0, "fallback"
 
 
-def profile_traffic():
-    """DRAM bytes per launch of the dominant kernel from the committed ncu summary."""
-    p = os.path.join(ROOT, "profiles", "traffic.json")
+PROFILE = os.path.join(ROOT, "profiles", "k_hard_shared_batch4096.json")
+
+
+def source_sha(files):
+    """sha256 over the kernel's source files, as the ncu summary records it."""
+    import hashlib
+
+    h = hashlib.sha256()
+    for f in files:
+        with open(os.path.join(ROOT, f), "rb") as fh:
+            h.update(fh.read())
+    return h.hexdigest()[:16]
+
+
+def kernel_profile():
+    """Per-launch counters of k_hard_shared on this workload from the committed
+    ncu capture (profiles/k_hard_shared_batch4096.json), and whether the
+    capture was taken of the current kernel source."""
     try:
-        with open(p) as f:
-            return json.load(f)
+        with open(PROFILE) as f:
+            pr = json.load(f)
+        pr["matches_source"] = source_sha(pr["source_files"]) == pr["source_sha"]
+        return pr
     except Exception:
         return None
+
+
+def golden_answers(name, xs):
+    """The oracle's answers for a workload (tests/golden/make_config_golden.py),
+    when the committed fixture holds exactly these queries."""
+    try:
+        with open(os.path.join(ROOT, "tests", "golden", name)) as f:
+            g = json.load(f)
+    except Exception:
+        return None
+    return g["pi"] if g["x"] == xs else None
+
+
+SMEM_BYTES_PER_CLK = 128  # shared-memory bandwidth of one SM per clock (32 banks x 4 B)
+ISSUE_PER_CLK = 4  # warp instructions an SM issues per clock (4 schedulers)
+
+
+def roofline(kern, hard_ms, hard_bytes, dev_ms, clocks, ctx):
+    """Roofline of the dominant kernel, k_hard_shared (the batch-shared
+    special-leaf phi sieve), which is bound by the integer ALU pipe.
+
+    achieved = ALU-pipe warp instructions of one launch (ncu, the committed
+    capture of this workload; `matches_source` says whether it was taken of
+    the current kernel source) / the launch's duration, measured live with
+    CUDA events on the context stream; peak = the ALU pipe's issue rate per
+    SM per clock (ncu's peak_sustained) x SMs x the median SM clock sampled
+    during the timed steps.  Beside it: all issued instructions against 4
+    per SM per clock, and the S2 rate (segment-bitmap bytes the sieve passes
+    over, one pass per level per segment, / duration of the hard-leaf
+    kernels) against the shared-memory bandwidth 128 B per SM per clock."""
+    pr = kernel_profile()
+    ks = statistics.median(k.get("k_hard_shared", 0.0) for k in kern) / 1000.0
+    mhz = clocks.get("sm_mhz") or 1965.0
+    sms = ctx.sm_count()
+    hs = statistics.median(hard_ms) / 1000.0
+    hb = hard_bytes[-1]
+    smem_peak = sms * SMEM_BYTES_PER_CLK * mhz * 1e6 / 1e9
+    s2 = (hb / hs) / 1e9 if hs else None
+    roof = {"bound": "alu", "kernel": "k_hard_shared (batch-shared special-leaf phi sieve)", "unit": "Ginst/s",
+            "achieved": None, "peak": None, "frac": None, "kernel_ms": ks * 1000.0, "traffic": None,
+            "peak_kind": f"derived: ALU-pipe warp instructions per SM per clock (ncu peak_sustained) x {sms} SMs x "
+                         f"{mhz:.0f} MHz (median sampled SM clock)",
+            "profile": os.path.relpath(PROFILE, ROOT), "profile_matches_source": None}
+    if pr and ks:
+        alu = pr["alu_warp_inst_per_launch"]
+        roof["achieved"] = alu / ks / 1e9
+        roof["peak"] = pr["alu_peak_warp_inst_per_sm_clk"] * sms * mhz * 1e6 / 1e9
+        roof["frac"] = roof["achieved"] / roof["peak"]
+        roof["traffic"] = pr["dram_bytes_per_launch"]
+        roof["profile_matches_source"] = pr["matches_source"]
+        issue_peak = ISSUE_PER_CLK * sms * mhz * 1e6 / 1e9
+        roof["issue_view"] = {"achieved": pr["warp_inst_per_launch"] / ks / 1e9, "peak": issue_peak,
+                              "unit": "Ginst/s", "frac": pr["warp_inst_per_launch"] / ks / 1e9 / issue_peak}
+    roof["smem_view"] = {"achieved": s2, "peak": smem_peak, "unit": "GB/s", "frac": s2 / smem_peak if s2 else None,
+                         "peak_kind": f"derived: {SMEM_BYTES_PER_CLK} B per SM per clock x {sms} SMs x {mhz:.0f} MHz",
+                         "what": "S2 bytes (one pass over the segment bitmap per level per segment) / hard-leaf "
+                                 "kernels' time; the kernel keeps chunk counters instead of sweeping, so this "
+                                 "counts work it does not do"}
+    tot = statistics.median(dev_ms)
+    names = sorted({n for k in kern for n in k})
+    shares = {n: {"ms": statistics.median(k.get(n, 0.0) for k in kern),
+                  "share": statistics.median(k.get(n, 0.0) for k in kern) / tot} for n in names}
+    return roof, shares
 
 
 def cpu_baseline(xs, budget_s):
@@ -174,11 +254,11 @@ def reference_terms_baseline(xs, budget_s):
 
 
 def alpha_frac(x):
-    # the library's default alpha (reference alpha(x), src/main.cpp:128-194), as num/den
-    import cudapix_b200 as cpx
-    from cudapix_b200 import _lib
+    # the reference's alpha(x) (src/main.cpp:128-194) from the oracle, as num/den;
+    # the CPU arms load no product library
+    import oracle
 
-    return _lib.load().cpx_alpha_milli(_lib.U128.of(x)), 1000
+    return oracle.alpha_milli(x), 1000
 
 
 def target_ratio(cpx, ctx, args):
@@ -186,6 +266,8 @@ def target_ratio(cpx, ctx, args):
     queries, numpy default_rng(0)); the plain path on the first 128."""
     xs = workload(1024, seed=0, lo=10.0, hi=15.0)
     ref = cpx.pi_batch(xs, ctx=ctx)
+    want = golden_answers("batch_1e10_1e15.json", xs)
+    assert want is None or ref == want, "batch answers differ from the oracle's"
     dev = []
     for _ in range(3):
         ctx.flush_l2()
@@ -202,7 +284,7 @@ def target_ratio(cpx, ctx, args):
     b = len(xs) / (statistics.median(dev) / 1000.0)
     p = len(lat) / (sum(lat) / 1000.0)
     return {"workload": "1024 x = floor(10^e), e ~ U[10,15], default_rng(0); plain on the first 128",
-            "batch_e2e_qps": b, "plain_qps": p, "ratio": b / p}
+            "checked_against_oracle": want is not None, "batch_e2e_qps": b, "plain_qps": p, "ratio": b / p}
 
 
 def serve_sweep(cpx, ctx, args):
@@ -299,18 +381,22 @@ def run_reference(args, world, rank):
 
     per_step = []
     sample = None
+    # each step a bounded sample of the workload: the whole run stays within a
+    # few minutes whatever --steps / --warmup ask for
+    step_s = args.ref_step_s or max(2.0, min(20.0, 150.0 / (args.warmup + args.steps)))
     for k in range(args.warmup + args.steps):
         t0 = time.perf_counter()
         done = 0
         for x in xs:
             oracle.pi_dr(x, oracle.default_y(x, *alpha_frac(x)), 6, nthreads)
             done += 1
-            if time.perf_counter() - t0 > args.ref_step_s:
+            if time.perf_counter() - t0 > step_s:
                 break
         dt = time.perf_counter() - t0
         if k >= args.warmup:
             per_step.append((done, dt))
-        sample = f"per step the first {done} of the {len(xs)} workload queries, oracle/oracle.c orc_pi_dr, OpenMP {nthreads} threads"
+        sample = (f"per step the first {done} of the {len(xs)} workload queries ({step_s:.1f} s), "
+                  f"oracle/oracle.c orc_pi_dr, OpenMP {nthreads} threads")
     q = sum(d for d, _ in per_step)
     t = sum(s for _, s in per_step)
     v = q / t
@@ -319,7 +405,7 @@ def run_reference(args, world, rank):
             "scaling": "weak", "vs_baseline": None, "dtype": "int64/int128", "data": "synthetic",
             "config": arm_config(args, world),
             "cpu_baseline": {"value": v, "unit": UNIT, "cores": nthreads, "kind": "port", "sample": sample,
-                             "reference_terms": reference_terms_baseline(xs, args.ref_step_s / 4)},
+                             "reference_terms": reference_terms_baseline(xs, step_s)},
             "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
@@ -372,7 +458,8 @@ def main():
     ap.add_argument("--queries", type=int, default=4096)
     ap.add_argument("--plain", type=int, default=256, help="queries timed through the plain per-query path")
     ap.add_argument("--cpu-budget", type=float, default=15.0)
-    ap.add_argument("--ref-step-s", type=float, default=20.0)
+    ap.add_argument("--ref-step-s", type=float, default=0.0,
+                    help="seconds of CPU work per reference step (0: 150 s over all steps, 2..20 s each)")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--graph", type=int, default=1, help="also time the batch as one CUDA graph launch")
     ap.add_argument("--serve", type=int, default=1, help="serving sweep and the [1e10,1e15] target check")
@@ -395,12 +482,13 @@ def main():
     ctx = tuned_context(cpx, local)
     ctx.set_timing(True)
     xs = workload(args.queries, seed=0)
-    ref = None
+    ref = golden_answers("batch_seed0.json", xs)  # the oracle's answers, when committed for these queries
+    checked = ref is not None
     for _ in range(max(args.warmup, 3)):
         out = cpx.pi_batch(xs, ctx=ctx)
         if ref is None:
             ref = out
-        assert out == ref, "batch results changed between runs"
+        assert out == ref, "batch answers differ from the oracle's" if checked else "batch results changed between runs"
 
     # plain path: one full launch sequence per query, on a fixed subsample (before the
     # clock sampler of the timed batches starts polling the driver)
@@ -420,7 +508,7 @@ def main():
                  "p50_ms": lat[len(lat) // 2], "p99_ms": lat[min(len(lat) - 1, int(len(lat) * 0.99))]}
 
     launches0 = ctx.launches
-    dev_ms, e2e_ms, hard_ms, hard_bytes, host_stats = [], [], [], [], []
+    dev_ms, e2e_ms, hard_ms, hard_bytes, host_stats, kern = [], [], [], [], [], []
     barrier(world)
     with Clocks(local) as clk:
         for _ in range(args.steps):
@@ -433,6 +521,7 @@ def main():
             hard_ms.append(hm)
             hard_bytes.append(hb)
             host_stats.append(ctx.last_batch_stats())
+            kern.append(ctx.last_kernel_ms())
             assert out == ref
     barrier(world)
     import ctypes
@@ -470,25 +559,15 @@ def main():
         serving = serve_sweep(cpx, ctx, args)
     if rank != 0:
         return
-    hbm, kind = peaks()
-    hb = hard_bytes[-1]
-    hs = statistics.median(hard_ms) / 1000.0
-    tr = profile_traffic()
-    roof = {"bound": "hbm", "kernel": "k_hard_shared (batch-shared special-leaf phi sieve)",
-            "achieved": (hb / hs) / 1e9 if hs else None,
-            "peak": hbm, "unit": "GB/s", "frac": ((hb / hs) / 1e9) / hbm if hs else None,
-            "peak_kind": kind, "traffic": tr.get("dram_bytes_per_launch") if tr else None,
-            "alu_pipe_frac_ncu": tr.get("alu_pipe_frac") if tr else None,
-            "note": "achieved = segment-bitmap bytes the sieve passes over (the counting sweep and every group "
-                    "unit: one pass per level per segment) / duration of the hard-leaf kernels (CUDA events); "
-                    "the passes run in shared memory and the kernel is integer-ALU bound (alu_pipe_frac_ncu, "
-                    "profiles/k_hard_shared_batch4096.md), so the HBM fraction is a proxy"}
+    clocks = clk.summary()
+    roof, shares = roofline(kern, hard_ms, hard_bytes, dev_ms, clocks, ctx)
     cpu = None if args.no_cpu else cpu_baseline(xs, args.cpu_budget)
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": max(args.warmup, 3), "ms_per_step": 1000 * t_dev / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "int64/int128", "data": "synthetic",
         "config": arm_config(args, world),
+        "checked_against_oracle": checked,
         "e2e": {"value": nq / t_e2e, "unit": UNIT, "h2d_bytes_per_step": io[0], "d2h_bytes_per_step": io[1]},
         "gpu_launches": int(launches),
         "host_ms": {k: round(statistics.median(h[k] for h in host_stats), 3)
@@ -499,10 +578,11 @@ def main():
         "plain": plain,
         "batched_over_plain": (value / plain["value"]) if plain else None,
         "e2e_over_plain": ((nq / t_e2e) / plain["value"]) if plain else None,
-        "s2_gbs": (hb / hs) / 1e9 if hs else None,
+        "s2_gbs": roof["smem_view"]["achieved"],
+        "kernel_ms": shares,
         "roofline": roof,
         "cpu_baseline": cpu,
-        "clocks": clk.summary(),
+        "clocks": clocks,
     }
     print(json.dumps(line), flush=True)
     if world > 1:

@@ -26,7 +26,8 @@ import os
 
 import numpy as np
 
-from ._lib import (BatchStats, CpxError, ExtensionMissing, LeafCounts, Params, ServeConfig, ServeCounters, Terms, TuneEntry,  # noqa: F401
+from ._lib import (BatchStats, CpxError, ExtensionMissing, GourdonTerms, LeafCounts, Params, ServeConfig, ServeCounters,  # noqa: F401
+                   Terms, TuneEntry,
                    U128,
                    header_symbols, load)
 
@@ -154,6 +155,23 @@ class Context:
         ms, by = ctypes.c_float(), ctypes.c_double()
         self.call("cpx_last_hard_stats", ctypes.byref(ms), ctypes.byref(by))
         return ms.value, by.value
+
+    def sm_count(self):
+        return self.L.cpx_sm_count(self.h)
+
+    def last_kernel_ms(self):
+        """{kernel: device ms} of the timed kernel launches of the last batch
+        (timing on, not a graph); launches of the same kernel are summed."""
+        out = {}
+        i = 0
+        while True:
+            name, ms = ctypes.c_char_p(), ctypes.c_float()
+            if self.L.cpx_last_kernel_span(self.h, i, ctypes.byref(name), ctypes.byref(ms)) != 0:
+                break
+            k = name.value.decode()
+            out[k] = out.get(k, 0.0) + ms.value
+            i += 1
+        return out
 
     def last_batch_ms(self):
         ms = ctypes.c_float()
@@ -290,6 +308,18 @@ def pi_terms(x, y=0, c=6, ctx=None):
     else:
         o = ctypes.c_uint64()
         ctx.call("cpx_pi_u64", x, y, c, ctypes.byref(o), ctypes.byref(t))
+    return t.as_dict()
+
+
+def pi_gourdon(x, y=0, c=6, ctx=None):
+    """pi(x) through Gourdon's decomposition, every term as a dict (A, B, C,
+    D, phi0, sigma, pi, x, y): the terms of the reference's GourdonVariant64
+    (include/Gourdon/gourdonvariant.hpp:7-56).  x < 2^64."""
+    ctx = ctx or context()
+    if _wide(x):
+        raise ValueError("Gourdon's decomposition here takes x < 2^64 (as GourdonVariant64)")
+    t = GourdonTerms()
+    ctx.call("cpx_gourdon_u64", x, y, c, ctypes.byref(t))
     return t.as_dict()
 
 

@@ -66,6 +66,16 @@ class Terms(ctypes.Structure):
         return d
 
 
+class GourdonTerms(ctypes.Structure):
+    _fields_ = [(k, U128) for k in ("A", "B", "C", "D", "phi0", "sigma", "pi")] + [
+        ("x", ctypes.c_uint64), ("y", ctypes.c_uint64)]
+
+    def as_dict(self):
+        d = {k: getattr(self, k).value(signed=True) for k in ("A", "B", "C", "D", "phi0", "sigma", "pi")}
+        d.update(x=self.x, y=self.y)
+        return d
+
+
 class BatchStats(ctypes.Structure):
     _fields_ = [
         ("roots_ms", ctypes.c_double),
@@ -149,6 +159,7 @@ _SIGS = {
     "cpx_version": (ctypes.c_char_p, []),
     "cpx_stream": (P, [P]),
     "cpx_launch_count": (u64, [P]),
+    "cpx_sm_count": (ctypes.c_int, [P]),
     "cpx_free": (ctypes.c_int, [P]),
     "cpx_device_alloc": (ctypes.c_int, [ctypes.c_size_t, PP]),
     "cpx_copy_to_host": (ctypes.c_int, [P, P, ctypes.c_size_t]),
@@ -169,6 +180,8 @@ _SIGS = {
     "cpx_tune_clear": (ctypes.c_int, [P]),
     "cpx_leaf_count": (ctypes.c_int, [P, U128, u64, u16, ctypes.POINTER(LeafCounts)]),
     "cpx_last_hard_stats": (ctypes.c_int, [P, ctypes.POINTER(ctypes.c_float), ctypes.POINTER(ctypes.c_double)]),
+    "cpx_last_kernel_span": (ctypes.c_int, [P, ctypes.c_int, ctypes.POINTER(ctypes.c_char_p),
+                                            ctypes.POINTER(ctypes.c_float)]),
     "cpx_set_timing": (ctypes.c_int, [P, ctypes.c_int]),
     "cpx_last_batch_ms": (ctypes.c_int, [P, ctypes.POINTER(ctypes.c_float)]),
     "cpx_timer_start": (ctypes.c_int, [P]),
@@ -190,6 +203,7 @@ _SIGS = {
     "cpx_S2_hard_u64": (ctypes.c_int, [P, u64, u64, u16, pi64]),
     "cpx_S2_hard_u128": (ctypes.c_int, [P, U128, u64, u16, pU]),
     "cpx_pi_u64": (ctypes.c_int, [P, u64, u64, u16, pu64, ctypes.POINTER(Terms)]),
+    "cpx_gourdon_u64": (ctypes.c_int, [P, u64, u64, u16, ctypes.POINTER(GourdonTerms)]),
     "cpx_pi_u128": (ctypes.c_int, [P, U128, u64, u16, pU, ctypes.POINTER(Terms)]),
     "cpx_gen_d_mu": (ctypes.c_int, [P, u64, u64, PP]),
     "cpx_gen_d_lpf32": (ctypes.c_int, [P, u64, u64, PP]),

@@ -22,8 +22,8 @@ template <class F> int guarded(cpx_ctx *ctx, F &&f)
         return CPX_ESTATE;
     }
     try {
-        cudaError_t e = cudaSetDevice(ctx->device);
-        if (e != cudaSuccess) fail(CPX_ECUDA, std::string("cudaSetDevice: ") + cudaGetErrorString(e));
+        DeviceGuard dg(ctx->device);
+        if (dg.err != cudaSuccess) fail(CPX_ECUDA, std::string("cudaSetDevice: ") + cudaGetErrorString(dg.err));
         f();
         ctx->last_error.clear();
         return CPX_OK;
@@ -70,7 +70,8 @@ template <class F> static void each_buf(cpx_ctx *ctx, F &&f)
 int init_context(cpx_ctx *ctx, int device)
 {
     ctx->device = device;
-    cudaError_t e = cudaSetDevice(device);
+    DeviceGuard dg(device);
+    cudaError_t e = dg.err;
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking);
     if (e == cudaSuccess) e = cudaDeviceGetAttribute(&ctx->sm_count, cudaDevAttrMultiProcessorCount, device);
     int optin = 0;
@@ -89,7 +90,7 @@ int init_context(cpx_ctx *ctx, int device)
 void release_context(cpx_ctx *ctx)
 {
     std::lock_guard<std::recursive_mutex> lk(ctx->mu);
-    cudaSetDevice(ctx->device);
+    DeviceGuard dg(ctx->device);
     if (ctx->stream) cudaStreamSynchronize(ctx->stream);
     Tables &tb = ctx->tab;
     if (!ctx->tables_borrowed) {
@@ -107,6 +108,10 @@ void release_context(cpx_ctx *ctx)
     for (cudaEvent_t *ev : {&ctx->ev_hard0, &ctx->ev_hard1, &ctx->ev_b0, &ctx->ev_b1, &ctx->ev_t0, &ctx->ev_t1}) {
         if (*ev) cudaEventDestroy(*ev);
         *ev = nullptr;
+    }
+    for (cudaEvent_t &ev : ctx->span_ev) {
+        if (ev) cudaEventDestroy(ev);
+        ev = nullptr;
     }
     if (ctx->stream) cudaStreamDestroy(ctx->stream);
     ctx->stream = nullptr;
@@ -146,6 +151,7 @@ int cpx_destroy(cpx_ctx *ctx)
 const char *cpx_last_error(cpx_ctx *ctx) { return ctx ? ctx->last_error.c_str() : "null context"; }
 void *cpx_stream(cpx_ctx *ctx) { return ctx ? (void *)ctx->stream : nullptr; }
 uint64_t cpx_launch_count(cpx_ctx *ctx) { return ctx ? ctx->launches : 0; }
+int cpx_sm_count(cpx_ctx *ctx) { return ctx ? ctx->sm_count : 0; }
 int cpx_free(void *p) { return cudaFree(p) == cudaSuccess ? CPX_OK : CPX_ECUDA; }
 
 int cpx_device_alloc(size_t bytes, void **p)
@@ -403,6 +409,15 @@ int cpx_timer_stop(cpx_ctx *ctx, float *ms)
     });
 }
 
+int cpx_last_kernel_span(cpx_ctx *ctx, int i, const char **name, float *ms)
+{
+    return guarded(ctx, [&] {
+        if (i < 0 || i >= ctx->n_span) fail(CPX_ERANGE, "no such kernel span");
+        if (name) *name = ctx->span_name[i];
+        if (ms) *ms = ctx->span_ms[i];
+    });
+}
+
 int cpx_last_hard_stats(cpx_ctx *ctx, float *ms, double *bytes)
 {
     return guarded(ctx, [&] {
@@ -537,6 +552,20 @@ int cpx_pi_u64(cpx_ctx *ctx, uint64_t x, uint64_t y, uint16_t c, uint64_t *pi, c
         one(ctx, x, y, c ? c : 6, TERM_PI, t, &yu);
         if (pi) *pi = (uint64_t)t[6];
         if (terms) fill_terms(terms, x, yu, c ? c : 6, t);
+    });
+}
+
+int cpx_gourdon_u64(cpx_ctx *ctx, uint64_t x, uint64_t y, uint16_t c, cpx_gourdon_terms *out)
+{
+    return guarded(ctx, [&] {
+        if (!out) fail(CPX_EINVAL, "null output");
+        const uint64_t yu = y ? y : default_y(x, 0, 0);
+        i128 t[7];
+        gourdon_terms(ctx, x, yu, c ? c : 6, t);
+        cpx_u128 *o[7] = {&out->A, &out->B, &out->C, &out->D, &out->phi0, &out->sigma, &out->pi};
+        for (int k = 0; k < 7; k++) *o[k] = C128s(t[k]);
+        out->x = x;
+        out->y = yu;
     });
 }
 

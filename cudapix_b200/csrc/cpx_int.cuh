@@ -78,6 +78,56 @@ CPX_HD uint64_t cpx_icbrt(u128 x)
 
 CPX_HD uint64_t cpx_iroot4(u128 x) { return cpx_isqrt((u128)cpx_isqrt(x)); }
 
+// ------------------------------------------------ 128-by-64-bit division
+// floor(n / d) for d >= 1 and a quotient below 2^64 (n < d 2^64): the x/p,
+// x/n and x/(p m) of x >= 2^64.  Division by Newton-Raphson reciprocal
+// refinement with exact integer correction (Brent and Zimmermann, Modern
+// Computer Arithmetic, sections 1.4.1 and 3.4.1):
+//   r0 = 1/d rounded to float; one Newton step in double,
+//   rd = r0 + r0 (1 - d r0), relative error below 2^-46;
+//   q0 = trunc(n * rd), within 2^18 of n/d since n/d < 2^64;
+//   the remainder r = n - q0 d is exact in 128 bits (|r| < 2^18 d + d);
+//   t = floor(r * rd) is within 1 of floor(r/d) (|r/d| < 2^19), and
+//   q0 + t corrected by the sign and size of r - t d is the quotient.
+// Every step is an IEEE-rounded operation, so the host and device forms
+// return the same value; the host form is checked against the compiler's
+// 128-bit division on random and edge operands.
+CPX_HD uint64_t cpx_udiv_2by1(u128 n, uint64_t d)
+{
+    const uint64_t nh = (uint64_t)(n >> 64), nl = (uint64_t)n;
+    constexpr double k2p64 = 18446744073709551616.0;
+#if defined(__CUDA_ARCH__)
+    const double dd = __ull2double_rn(d);
+    const double r0 = (double)__frcp_rn(__ull2float_rn(d));
+    const double rd = __fma_rn(r0, __fma_rn(-dd, r0, 1.0), r0);
+    const double qd = __dmul_rn(__fma_rn(__ull2double_rn(nh), k2p64, __ull2double_rn(nl)), rd);
+#else
+    const double dd = (double)d;
+    const double r0 = (double)(1.0f / (float)d);
+    const double rd = std::fma(r0, std::fma(-dd, r0, 1.0), r0);
+    const double qd = std::fma((double)nh, k2p64, (double)nl) * rd;
+#endif
+    uint64_t q = qd >= k2p64 ? ~0ull : (uint64_t)qd;  // truncation
+    i128 r = (i128)(n - (u128)q * d);
+    const double rr = (double)(int64_t)(uint64_t)((u128)r >> 64) * k2p64 + (double)(uint64_t)r;
+#if defined(__CUDA_ARCH__)
+    const int64_t t = __double2ll_rd(__dmul_rn(rr, rd));
+#else
+    const int64_t t = (int64_t)std::floor(rr * rd);
+#endif
+    q += (uint64_t)t;
+    r -= (i128)t * (i128)d;
+    while (r < 0) {
+        q--;
+        r += d;
+    }
+    while (r >= (i128)d) {
+        q++;
+        r -= d;
+    }
+    return q;
+}
+
 // --------------------------------------------------------- table lookups
 // Compressed prime table: entry w covers the odd numbers 128w+1 .. 128w+127,
 // .x = bitmap (bit j <-> 128w + 2j + 1 is prime), .y = number of odd primes
@@ -146,11 +196,15 @@ __device__ __forceinline__ uint64_t cpx_udiv_leaf(uint64_t n, uint64_t d)
 }
 __device__ __forceinline__ uint64_t cpx_qdiv(uint64_t n, uint64_t d) { return cpx_udiv_leaf(n, d); }
 // 128-bit dividend: x/p is below 2^64 for x < 2^64 p, so most leaf
-// quotients of the 128-bit path take the 64-bit route as well
+// quotients of the 128-bit path take the 64-bit route; a wider dividend with
+// a quotient below 2^64 takes cpx_udiv_2by1, and only quotients of 2^64 or
+// more the compiler's 128-bit division
 static __device__ __noinline__ u128 cpx_udiv128_slow(u128 n, uint64_t d) { return n / (u128)d; }
 __device__ __forceinline__ u128 cpx_qdiv(u128 n, uint64_t d)
 {
-    if (!(n >> 64)) return (u128)cpx_udiv_leaf((uint64_t)n, d);
+    const uint64_t nh = (uint64_t)(n >> 64);
+    if (!nh) return (u128)cpx_udiv_leaf((uint64_t)n, d);
+    if (nh < d) return (u128)cpx_udiv_2by1(n, d);
     return cpx_udiv128_slow(n, d);
 }
 

@@ -131,6 +131,14 @@ struct cpx_ctx {
     cpx_batch_stats last_stats = {};      // host phases of the last batch
     double last_hard_bytes = 0.0;
     uint64_t launches = 0;  // kernels launched by this context
+    void *noalloc_scratch = nullptr;  // device address of cpx_mutest_noalloc's static array (first call)
+    // per-kernel CUDA-event spans of the last timed batch (timing on, not a graph)
+    static constexpr int kMaxSpans = 16;
+    cudaEvent_t span_ev[2 * kMaxSpans] = {};
+    const char *span_name[kMaxSpans] = {};
+    float span_ms[kMaxSpans] = {};
+    int n_span = 0;
+    bool span_on = false;  // spans are being recorded for the current batch
 };
 
 namespace cpx {
@@ -165,5 +173,57 @@ void release_context(cpx_ctx *ctx);
 
 // counts launched kernels for the gpu_launches report
 inline void note_launch(cpx_ctx *ctx, uint64_t n = 1) { ctx->launches += n; }
+
+// Brackets one kernel launch with CUDA events on the context stream when the
+// batch records spans (ctx->span_on); the durations are read once the batch
+// has synchronised (finish_spans).
+struct KSpan {
+    cpx_ctx *c;
+    int i = -1;
+    KSpan(cpx_ctx *ctx, const char *name) : c(ctx)
+    {
+        if (!c->span_on || c->n_span >= cpx_ctx::kMaxSpans) return;
+        i = c->n_span++;
+        c->span_name[i] = name;
+        if (!c->span_ev[2 * i]) {
+            cudaEventCreate(&c->span_ev[2 * i]);
+            cudaEventCreate(&c->span_ev[2 * i + 1]);
+        }
+        cudaEventRecord(c->span_ev[2 * i], c->stream);
+    }
+    ~KSpan()
+    {
+        if (i >= 0) cudaEventRecord(c->span_ev[2 * i + 1], c->stream);
+    }
+    KSpan(const KSpan &) = delete;
+    KSpan &operator=(const KSpan &) = delete;
+};
+inline void finish_spans(cpx_ctx *c)
+{
+    for (int i = 0; i < c->n_span; i++) {
+        c->span_ms[i] = 0.f;
+        cudaEventElapsedTime(&c->span_ms[i], c->span_ev[2 * i], c->span_ev[2 * i + 1]);
+    }
+    c->span_on = false;
+}
+
+// Makes a device current for the lifetime of the guard and gives the caller's
+// current device back afterwards (entry points leave the caller's device as
+// they found it).
+struct DeviceGuard {
+    int prev = -1;
+    cudaError_t err;
+    explicit DeviceGuard(int dev)
+    {
+        if (cudaGetDevice(&prev) != cudaSuccess) prev = -1;
+        err = cudaSetDevice(dev);
+    }
+    ~DeviceGuard()
+    {
+        if (prev >= 0) cudaSetDevice(prev);
+    }
+    DeviceGuard(const DeviceGuard &) = delete;
+    DeviceGuard &operator=(const DeviceGuard &) = delete;
+};
 
 }  // namespace cpx

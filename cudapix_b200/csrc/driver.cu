@@ -696,7 +696,9 @@ replan:  // again without the batch alpha when its shared sieve would not fit (b
                 if (mask & TERM_ORD) n_ord = ((d.y + 1) / 2 + 3) / 4;
                 if ((mask & TERM_P2) && d.sx > d.y && !d.p2win) n_p2 = ((d.sx - 1) >> 7) - (d.y >> 7) + 1;
                 if (mask & TERM_TRIV) n_triv = (d.cx > d.tx) ? ((d.cx - 1) >> 7) - (d.tx >> 7) + 1 : 1;
-                if ((mask & TERM_EASY) && d.cx > pc) n_easy = host_pi(hP, d.cx) - c;  // primes p_c < p <= icbrt(x)
+                // primes p_c < p <= icbrt(x) (or <= easy_pmax)
+                const uint64_t pe = rq.easy_pmax ? std::min<uint64_t>(d.cx, rq.easy_pmax) : d.cx;
+                if ((mask & TERM_EASY) && pe > pc) n_easy = host_pi(hP, pe) - c;
                 if (mask & TERM_EASY) {
                     // composite easy leaves: levels b with p_b <= iroot4(x), p_b^2 < y and
                     // max(y/p_b, x/p_b^3) < y
@@ -967,6 +969,8 @@ replan:  // again without the batch alpha when its shared sieve would not fit (b
         }
         if (!any_p2win) launch_finalize(ctx, pl, d_out, mask == TERM_PI);
     };
+    ctx->n_span = 0;
+    ctx->span_on = ctx->timing && !rq.graph;
     if (ctx->timing) CPX_CUDA(cudaEventRecord(ctx->ev_b0, ctx->stream));
     if (rq.graph && !any_p2win) launch_as_graph(ctx, launch_all);
     else launch_all();
@@ -1007,6 +1011,7 @@ replan:  // again without the batch alpha when its shared sieve would not fit (b
         CPX_CUDA(cudaMemcpy(rq.hard_levels, pl.hard_levels, n_levels * sizeof(HardLevel), cudaMemcpyDeviceToHost));
     }
     if (ctx->timing) CPX_CUDA(cudaEventElapsedTime(&ctx->last_batch_ms, ctx->ev_b0, ctx->ev_b1));
+    finish_spans(ctx);
     if (pl.time_hard && (pl.n_seg || pl.n_gunits)) {
         float ms = 0.f;
         CPX_CUDA(cudaEventElapsedTime(&ms, ctx->ev_hard0, ctx->ev_hard1));

@@ -33,6 +33,7 @@ struct BatchReq {
     const TuneEntry *tune = nullptr;  // per-decade alpha scale when alpha_num = alpha_scale = 0
     uint64_t seg_lo = 0, seg_hi = 0;  // one query's hard-leaf segments [seg_lo, seg_hi) (0, 0: all)
     HardLevel *hard_levels = nullptr; // per-level records of that part (host, nb - c entries)
+    uint64_t easy_pmax = 0;           // easy leaves of the p <= easy_pmax only (0: every p <= icbrt x)
     bool wide = false;   // 128-bit kernels even when every x < 2^64
     bool graph = false;  // one CUDA graph launch for the batch's kernels
 };
@@ -63,6 +64,8 @@ void tune_load(cpx_ctx *ctx, const char *path);
 // exact special-leaf counts of one query: hard, easy (composite m), easy (prime m), trivial
 void leaf_counts(cpx_ctx *ctx, u128 x, uint64_t y, uint32_t c, uint64_t out[4]);
 uint64_t default_y(u128 x, uint32_t num, uint32_t den);
+// pi(x) through Gourdon's decomposition (gourdon.cu): A, B, C, D, Phi0, Sigma, pi
+void gourdon_terms(cpx_ctx *ctx, uint64_t x, uint64_t y, uint32_t c, i128 out[7]);
 uint32_t alpha_milli(u128 x);
 bool dr_domain_ok(u128 x, uint64_t y, uint32_t c);
 

@@ -564,10 +564,13 @@ template <class XT> static void hard_go(cpx_ctx *ctx, const Plan &pl)
         CPX_CUDA(cudaMemsetAsync(pl.njobs, 0, sizeof(unsigned int), ctx->stream));
         CPX_CUDA(cudaMemsetAsync(pl.job_units, 0, (pl.max_jobs + 1) * sizeof(uint64_t), ctx->stream));
     }
-    k_hard<XT><<<(unsigned)pl.n_seg, pl.hard_threads, smem, ctx->stream>>>(
-        pl.qd, pl.Q, pl.pre_seg, pl.n_seg, pl.seg_B, pl.seg_off, tb.P, tb.MU, tb.T, pl.hard_cnt, pl.hard_ms,
-        pl.hard_entries, pl.acc, pl.lbits_max, pl.jobs, pl.njobs, pl.job_units, pl.snap, pl.max_jobs, lbits_sub,
-        (uint32_t)std::min<uint64_t>(pl.offload_min, 0xFFFFFFFFull));
+    {
+        KSpan ks(ctx, "k_hard");
+        k_hard<XT><<<(unsigned)pl.n_seg, pl.hard_threads, smem, ctx->stream>>>(
+            pl.qd, pl.Q, pl.pre_seg, pl.n_seg, pl.seg_B, pl.seg_off, tb.P, tb.MU, tb.T, pl.hard_cnt, pl.hard_ms,
+            pl.hard_entries, pl.acc, pl.lbits_max, pl.jobs, pl.njobs, pl.job_units, pl.snap, pl.max_jobs, lbits_sub,
+            (uint32_t)std::min<uint64_t>(pl.offload_min, 0xFFFFFFFFull));
+    }
     CPX_LAUNCH("k_hard");
     note_launch(ctx);
     if (pl.max_jobs) launch_hard_leaves(ctx, pl, lbits_sub);

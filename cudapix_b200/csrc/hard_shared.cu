@@ -267,8 +267,11 @@ static __device__ __noinline__ bool offload_sets(bool off_j, uint32_t lane, uint
 // Sum(-mu) for the query of its last leaf and adds them into the warp's
 // per-query slots when the query changes; at the end of the level lane j
 // folds slot j into its total as sum + carry * Sum(-mu).
-template <class XT>
-__global__ void __launch_bounds__(1024, 1)
+// LB is the launch bound: blocks of 1024 threads (32 warps per SM) leave 64
+// registers a thread, blocks of up to 512 threads leave up to 128, which the
+// level loop uses without spilling.
+template <class XT, int LB>
+__global__ void __launch_bounds__(LB, 1)
     k_hard_shared(const QD *__restrict__ qd, const HardGroup *__restrict__ grp, const uint64_t *__restrict__ pre_grp,
                   uint32_t ngrp, uint64_t total, uint32_t lbits, uint32_t c, const uint32_t *__restrict__ P,
                   uint32_t np, const int32_t *__restrict__ MU, const cpx_pient *__restrict__ Tpi,
@@ -584,9 +587,12 @@ template <class XT> static void shared_go(cpx_ctx *ctx, const Plan &pl)
     const uint32_t lbits_sub = pl.sh_lbits - (uint32_t)(__builtin_ctz(T) - 5);
     if (pl.time_hard) CPX_CUDA(cudaEventRecord(ctx->ev_hard0, ctx->stream));
     if (pl.sh_nlv) {
-        k_sieve_counts<<<(unsigned)pl.sh_nseg, T, counts_smem(pl.sh_lbits), ctx->stream>>>(
-            pl.sh_nseg, pl.sh_lbits, pl.sh_xmax, pl.sh_r4max, pl.c, tb.P, (uint32_t)tb.prm_n, pl.lvl_off, pl.sh_nlv,
-            pl.carry);
+        {
+            KSpan ks(ctx, "k_sieve_counts");
+            k_sieve_counts<<<(unsigned)pl.sh_nseg, T, counts_smem(pl.sh_lbits), ctx->stream>>>(
+                pl.sh_nseg, pl.sh_lbits, pl.sh_xmax, pl.sh_r4max, pl.c, tb.P, (uint32_t)tb.prm_n, pl.lvl_off,
+                pl.sh_nlv, pl.carry);
+        }
         CPX_LAUNCH("k_sieve_counts");
         k_carry_scan<<<pl.sh_nlv, 1024, 0, ctx->stream>>>(pl.sh_nlv, pl.c, 2ull << pl.sh_lbits, tb.P, tb.T, pl.lvl_off,
                                                            pl.carry);
@@ -605,10 +611,17 @@ template <class XT> static void shared_go(cpx_ctx *ctx, const Plan &pl)
         CPX_LAUNCH("k_group_levels");
         note_launch(ctx);
     }
-    k_hard_shared<XT><<<(unsigned)pl.n_gunits, T, shared_smem(pl.sh_lbits, T), ctx->stream>>>(
-        pl.qd, pl.grp, pl.pre_grp, pl.n_grp, pl.n_gunits, pl.sh_lbits, pl.c, tb.P, (uint32_t)tb.prm_n, tb.MU, tb.T,
-        pl.lvl_off, pl.sh_nlv, pl.carry, pl.acc, pl.jobs, pl.njobs, pl.job_units, pl.snap, pl.nsnap, pl.max_jobs,
-        lbits_sub, (uint32_t)std::min<uint64_t>(pl.offload_min, 0xFFFFFFFFull), gxp, pl.gae);
+    {
+        KSpan ks(ctx, "k_hard_shared");
+        auto go = [&](auto kern) {
+            kern<<<(unsigned)pl.n_gunits, T, shared_smem(pl.sh_lbits, T), ctx->stream>>>(
+                pl.qd, pl.grp, pl.pre_grp, pl.n_grp, pl.n_gunits, pl.sh_lbits, pl.c, tb.P, (uint32_t)tb.prm_n, tb.MU,
+                tb.T, pl.lvl_off, pl.sh_nlv, pl.carry, pl.acc, pl.jobs, pl.njobs, pl.job_units, pl.snap, pl.nsnap,
+                pl.max_jobs, lbits_sub, (uint32_t)std::min<uint64_t>(pl.offload_min, 0xFFFFFFFFull), gxp, pl.gae);
+        };
+        if (T > 512) go(k_hard_shared<XT, 1024>);
+        else go(k_hard_shared<XT, 512>);
+    }
     CPX_LAUNCH("k_hard_shared");
     note_launch(ctx);
     if (pl.max_jobs) launch_hard_leaves(ctx, pl, lbits_sub);
@@ -636,8 +649,13 @@ void prepare_hard_shared(cpx_ctx *ctx, const Plan &pl)
     const int w = pl.wide ? 1 : 0;
     if (done_dev[w] == ctx->device) return;
     raise_dyn_smem(k_sieve_counts, ctx->smem_optin);
-    if (pl.wide) raise_dyn_smem(k_hard_shared<u128>, ctx->smem_optin);
-    else raise_dyn_smem(k_hard_shared<uint64_t>, ctx->smem_optin);
+    if (pl.wide) {
+        raise_dyn_smem(k_hard_shared<u128, 1024>, ctx->smem_optin);
+        raise_dyn_smem(k_hard_shared<u128, 512>, ctx->smem_optin);
+    } else {
+        raise_dyn_smem(k_hard_shared<uint64_t, 1024>, ctx->smem_optin);
+        raise_dyn_smem(k_hard_shared<uint64_t, 512>, ctx->smem_optin);
+    }
     done_dev[w] = ctx->device;
 }
 

@@ -20,13 +20,15 @@
 //
 // In host code the name g_noalloc_scratch is only a host-side stand-in for the
 // device array: a kernel given it would fault or, where the GPU can reach host
-// memory, silently use the wrong memory.  So on the first call on each device,
-// with that device current, the entry point asks the runtime for the array's
-// device address (cudaGetSymbolAddress) and passes that address to the kernels.
-// That first call on a device does this set-up, so make it before any stream
-// capture on that device.
+// memory, silently use the wrong memory.  So the first call on each context,
+// with the context's device current, asks the runtime for the array's device
+// address (cudaGetSymbolAddress), keeps it in the context and passes it to the
+// kernels.  Make that first call on a context before any stream capture.
+// cudaDeviceReset destroys every context's stream and tables along with the
+// array: destroy the contexts before a reset and create new ones after it (a
+// new context looks the address up again).  The caller's current device is
+// left as it was.
 #include <algorithm>
-#include <mutex>
 
 #include "misc.h"
 
@@ -48,10 +50,6 @@ constexpr uint64_t kMaxTop = 2 * kMaxOdd;  // 33554432
 constexpr size_t kScratchBytes = kMuOff + kMaxOdd;
 
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kScratchBytes];
-
-constexpr int kMaxDevices = 64;
-std::mutex g_setup_mu;
-void *g_scratch_addr[kMaxDevices] = {};
 
 // primes below 8192, ascending, by trial division in one CTA of 1024 threads
 // (4 odd candidates per thread, block scan for the output positions)
@@ -99,20 +97,17 @@ extern "C" int cpx_mutest_noalloc(cpx_ctx *ctx, uint64_t top, int64_t *out)
     };
     if (top > kMaxTop)
         return err(CPX_ERANGE, "cpx_mutest_noalloc: top must be <= 33554432 (the 16 MiB static scratch)");
-    if (cudaSetDevice(ctx->device) != cudaSuccess) return err(CPX_ECUDA, "cudaSetDevice failed");
-    if (ctx->device < 0 || ctx->device >= kMaxDevices) return err(CPX_EINVAL, "device index out of range");
-    unsigned char *base = nullptr;
-    {
-        std::lock_guard<std::mutex> g(g_setup_mu);
-        if (!g_scratch_addr[ctx->device]) {
-            void *p = nullptr;
-            const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-            if (e != cudaSuccess || !p)
-                return err(CPX_ECUDA, std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e));
-            g_scratch_addr[ctx->device] = p;
-        }
-        base = static_cast<unsigned char *>(g_scratch_addr[ctx->device]);
+    DeviceGuard dg(ctx->device);
+    if (dg.err != cudaSuccess)
+        return err(CPX_ECUDA, std::string("cudaSetDevice: ") + cudaGetErrorString(dg.err));
+    if (!ctx->noalloc_scratch) {
+        void *p = nullptr;
+        const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+        if (e != cudaSuccess || !p)
+            return err(CPX_ECUDA, std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e));
+        ctx->noalloc_scratch = p;
     }
+    unsigned char *base = static_cast<unsigned char *>(ctx->noalloc_scratch);
     *out = 0;
     if (top <= 1) {
         ctx->last_error.clear();

@@ -334,7 +334,8 @@ int cpx_serve_create(cpx_ctx *ctx, const cpx_serve_config *cfg, cpx_server **out
     try {
         std::lock_guard<std::recursive_mutex> g(ctx->mu);
         if (ctx->server_attached) fail(CPX_ESTATE, "the context already serves another server");
-        CPX_CUDA(cudaSetDevice(ctx->device));
+        DeviceGuard dg(ctx->device);
+        CPX_CUDA(dg.err);
         if (cfg) S->cfg = *cfg;
         if (!S->cfg.lanes) S->cfg.lanes = 4;
         if (!S->cfg.max_batch) S->cfg.max_batch = 4096;

@@ -64,8 +64,16 @@ __global__ void __launch_bounds__(kThreads) k_ordinary(const QD *__restrict__ qd
                 if (n > y || v == 0) continue;
                 if ((v > 0 ? v : -v) <= Wh::PC) continue;
                 const XT m = cpx_qdiv(x, n);
-                const XT qw = m / (XT)Wh::W;
-                const uint32_t r = (uint32_t)(m - qw * (XT)Wh::W);
+                XT qw;
+                uint32_t r;
+                if ((u128)m >> 64) {
+                    qw = m / (XT)Wh::W;
+                    r = (uint32_t)(m - qw * (XT)Wh::W);
+                } else {  // below 2^64 (every n > x / 2^64): 64-bit division by the constant
+                    const uint64_t m64 = (uint64_t)m, q64 = m64 / Wh::W;
+                    qw = (XT)q64;
+                    r = (uint32_t)(m64 - q64 * Wh::W);
+                }
                 const i128 ph = (i128)qw * (i128)Wh::TOT + (i128)__ldg(WH + ((r + 1) >> 1));
                 a.v += (v > 0) ? ph : -ph;
             }
@@ -555,6 +563,7 @@ template <class XT> static void ord_dispatch(cpx_ctx *ctx, const Plan &pl)
 void launch_ordinary(cpx_ctx *ctx, const Plan &pl)
 {
     if (!pl.n_ord) return;
+    KSpan ks(ctx, "k_ordinary");
     if (pl.wide) ord_dispatch<u128>(ctx, pl);
     else ord_dispatch<uint64_t>(ctx, pl);
     CPX_LAUNCH("k_ordinary");
@@ -564,6 +573,7 @@ void launch_ordinary(cpx_ctx *ctx, const Plan &pl)
 void launch_p2(cpx_ctx *ctx, const Plan &pl)
 {
     if (!pl.n_p2) return;
+    KSpan ks(ctx, "k_p2");
     if (pl.wide)
         k_p2<u128><<<grid_for(ctx, pl.n_p2), kThreads, 0, ctx->stream>>>(pl.qd, pl.Q, pl.pre_p2, pl.n_p2,
                                                                          ctx->tab.T, pl.acc);
@@ -603,6 +613,7 @@ void launch_easy(cpx_ctx *ctx, const Plan &pl)
     note_launch(ctx);
     scan_u64(ctx, off, pl.n_easy + 1);
     const unsigned grid = (unsigned)ctx->sm_count * 8;
+    KSpan ks(ctx, "k_easy");
     if (pl.wide)
         k_easy<u128><<<grid, kThreads, 0, ctx->stream>>>(pl.qd, pl.Q, pl.pre_easy, pl.n_easy, off, tb.P, tb.prm_max,
                                                          tb.T, pl.acc);
@@ -618,6 +629,7 @@ void launch_easy_comp(cpx_ctx *ctx, const Plan &pl)
     if (!pl.n_ecomp) return;
     const unsigned grid = (unsigned)std::max<uint64_t>(
         1, std::min<uint64_t>((pl.n_ecomp + (kThreads / 32) - 1) / (kThreads / 32), (uint64_t)ctx->sm_count * 16));
+    KSpan ks(ctx, "k_easy_comp");
     if (pl.wide)
         k_easy_comp<u128><<<grid, kThreads, 0, ctx->stream>>>(pl.qd, pl.elv, pl.n_elv, pl.n_ecomp, ctx->tab.MU,
                                                               ctx->tab.T, pl.acc);

@@ -70,6 +70,8 @@ const char *cpx_version(void);
 void *cpx_stream(cpx_ctx *ctx);
 /* kernels launched by this context since creation */
 uint64_t cpx_launch_count(cpx_ctx *ctx);
+/* streaming multiprocessors of the context's device (0 for a null context) */
+int cpx_sm_count(cpx_ctx *ctx);
 int cpx_free(void *device_ptr);
 /* plain device memory helpers for callers without their own CUDA runtime */
 int cpx_device_alloc(size_t bytes, void **device_ptr);
@@ -102,6 +104,12 @@ int cpx_set_p2_window(cpx_ctx *ctx, uint64_t limit);
  * its algorithmic byte count (one pass over the segment bitmap per active
  * prime per segment). */
 int cpx_last_hard_stats(cpx_ctx *ctx, float *ms, double *bytes);
+/* Device time of the i-th timed kernel launch of the last batch run with
+ * timing on (cpx_set_timing) and not as a graph: *name is the kernel (a
+ * static string), *ms its CUDA-event duration on the context stream.  The
+ * timed kernels are the dominant ones (k_hard_shared, k_hard, k_easy,
+ * k_easy_comp, k_p2, k_sieve_counts, k_ordinary).  CPX_ERANGE past the last. */
+int cpx_last_kernel_span(cpx_ctx *ctx, int i, const char **name, float *ms);
 int cpx_set_timing(cpx_ctx *ctx, int enable);
 /* device time of the last batch's kernels (first launch to last, CUDA events
  * on the context stream); valid when timing is enabled */
@@ -167,6 +175,18 @@ int cpx_S2_hard_u128(cpx_ctx *ctx, cpx_u128 x, uint64_t y, uint16_t c, cpx_u128 
  * directly.                   (src/Deleglise-Rivat/deleglise-rivat.cpp:50-80) */
 int cpx_pi_u64(cpx_ctx *ctx, uint64_t x, uint64_t y, uint16_t c, uint64_t *pi, cpx_terms *terms);
 int cpx_pi_u128(cpx_ctx *ctx, cpx_u128 x, uint64_t y, uint16_t c, cpx_u128 *pi, cpx_terms *terms);
+/* pi(x) through Gourdon's decomposition, the terms of the reference's
+ * GourdonVariant64 (include/Gourdon/gourdonvariant.hpp:7-56; A: src/Gourdon/A2.cu,
+ * B: B.cu, C: C.cu, D = S2hard (gourdonvariant.cpp:61), Phi0: phi_0.cpp,
+ * Sigma: sigma_cpu.cpp): pi = A - B + C + D + phi0 + sigma, every term signed
+ * 128-bit (two's complement).  x < 2^64; y = 0 picks the default y rule; the
+ * domain is icbrt(x) <= y < isqrt(x).  x* = max(iroot4(x), x/y^2) (the
+ * reference's x* = iroot4(x) is exact only for y >= ~x^(3/8)). */
+typedef struct {
+    cpx_u128 A, B, C, D, phi0, sigma, pi;
+    uint64_t x, y;
+} cpx_gourdon_terms;
+int cpx_gourdon_u64(cpx_ctx *ctx, uint64_t x, uint64_t y, uint16_t c, cpx_gourdon_terms *out);
 
 /* ---- sieves and tables -------------------------------------------------- */
 /* mu(n) and lpf(n) for odd n = lo + 2i + 1, i < (hi - lo) / 2, lo even.
@@ -187,9 +207,12 @@ int cpx_mutest(cpx_ctx *ctx, uint64_t top, int64_t *out);
  * synchronise a latency-critical path).  Scratch lives in one file-scope
  * static device array of 16 MiB + 16 KiB that every GPU loading the library
  * holds until exit; top must be <= 33554432 (CPX_ERANGE otherwise).  The
- * first call on a device looks up the array's device address, so make it
- * before any stream capture on that device.  Calls share the array: calls
- * that overlap on the GPU race.  Uses the context's stream and device. */
+ * first call on a context looks up the array's device address and keeps it
+ * in the context, so make it before any stream capture on that context; after
+ * a cudaDeviceReset, create new contexts (a reset also destroys their streams
+ * and tables).  Calls share the array: calls that overlap on the GPU race.
+ * Uses the context's stream and device; the caller's current device is left
+ * as it was. */
 int cpx_mutest_noalloc(cpx_ctx *ctx, uint64_t top, int64_t *out);
 /* dense pi table of get_d_piTable: out[k] = pi(2k - 1), k < hi / 2, hi < 2^32
  *                                                          (src/pitable.cu:10) */

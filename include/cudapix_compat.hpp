@@ -17,6 +17,8 @@
 //   gen_d_lpf / gen_h_lpf / gen_d_mu / gen_h_mu / gen_d_mu_lpf
 //                                                     include/sieve/lpf_mu.cuh:12-24
 //   S2hardHost::S2hard(x, y, c)                       include/sieve/S2_hard_host.cuh:35
+//   GourdonVariant64 (piGourdon, pi, A, B, C, sigma, phi_0)
+//                                                     include/Gourdon/gourdonvariant.hpp:7-56
 //   deleglise_rivat64/128::pi_deleglise_rivat(x, y, c)
 //                                                     include/Deleglise-Rivat/deleglise-rivat.hpp:28,64
 //
@@ -417,4 +419,26 @@ struct deleglise_rivat128 {
         cudapix_compat::ok(cpx_pi_u128(cudapix_compat::ctx(), cudapix_compat::to(x), y, c, &r, nullptr));
         return cudapix_compat::from(r);
     }
+};
+
+// Gourdon's decomposition (include/Gourdon/gourdonvariant.hpp:7-56): the
+// terms are computed once, on construction; pi() = A - B + C + D + phi_0 + sigma
+// with D = S2hardHost::S2hard(x, y, c, x^(1/4)) (gourdonvariant.cpp:61).
+class GourdonVariant64 {
+    cpx_gourdon_terms t_;
+    static int64_t s64(cpx_u128 v) { return (int64_t)v.lo; }
+
+  public:
+    GourdonVariant64(uint64_t x, uint64_t y, uint16_t c)
+    {
+        cudapix_compat::ok(cpx_gourdon_u64(cudapix_compat::ctx(), x, y, c, &t_));
+    }
+    static uint64_t piGourdon(uint64_t x, uint64_t y, uint16_t c) { return GourdonVariant64(x, y, c).pi(); }
+    uint64_t pi() { return t_.pi.lo; }
+    uint64_t A() { return t_.A.lo; }
+    uint64_t B() { return t_.B.lo; }
+    uint64_t C() { return t_.C.lo; }
+    uint64_t D() { return (uint64_t)s64(t_.D); }
+    int64_t sigma() { return s64(t_.sigma); }
+    uint64_t phi_0() { return (uint64_t)s64(t_.phi0); }
 };

@@ -32,6 +32,8 @@ def lib():
         for name in ("orc_isqrt", "orc_icbrt", "orc_iroot4"):
             getattr(L, name).restype = U64
             getattr(L, name).argtypes = [U64, U64]
+        L.orc_alpha_milli.restype = ctypes.c_uint32
+        L.orc_alpha_milli.argtypes = [U64, U64]
         L.orc_pi_sieve.restype = U64
         L.orc_pi_sieve.argtypes = [U64]
         L.orc_pi_lehmer.restype = U64
@@ -94,6 +96,11 @@ def icbrt(x):
 
 def iroot4(x):
     return lib().orc_iroot4(*_split(x))
+
+
+def alpha_milli(x):
+    """The reference's alpha(x) (src/main.cpp:128-194) in per mille."""
+    return lib().orc_alpha_milli(*_split(x))
 
 
 def pi_sieve(x):

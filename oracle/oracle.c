@@ -82,6 +82,24 @@ uint64_t orc_isqrt(uint64_t lo, uint64_t hi) { return isqrt128(mk128(lo, hi)); }
 uint64_t orc_icbrt(uint64_t lo, uint64_t hi) { return icbrt128(mk128(lo, hi)); }
 uint64_t orc_iroot4(uint64_t lo, uint64_t hi) { return isqrt128(isqrt128(mk128(lo, hi))); }
 
+/* alpha(x) of src/main.cpp:128-194 in per mille: the reference's cubic in
+ * log x (one set of coefficients up to 1e21, another above), at least 1.
+ * It only chooses y = alpha * icbrt(x); no count depends on it. */
+uint32_t orc_alpha_milli(uint64_t lo, uint64_t hi)
+{
+    const double xd = (double)lo + ldexp((double)hi, 64);
+    const double lx = log(xd);
+    double a, b, c, d;
+    if (xd <= 1e21) {
+        a = 0.000711339; b = -0.0160586; c = 0.123034; d = 0.802942;
+    } else {
+        a = 0.00149066; b = -0.0375705; c = 0.282139; d = 0.591972;
+    }
+    double al = a * lx * lx * lx + b * lx * lx + c * lx + d;
+    if (al < 1.0) al = 1.0;
+    return (uint32_t)lround(al * 1000.0);
+}
+
 /* ----------------------------------------------------------- small primes */
 
 /* all primes <= n (n < 2^32), ascending; *cnt receives the count */

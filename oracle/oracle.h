@@ -26,6 +26,8 @@ extern "C" {
 uint64_t orc_isqrt(uint64_t lo, uint64_t hi);
 uint64_t orc_icbrt(uint64_t lo, uint64_t hi);
 uint64_t orc_iroot4(uint64_t lo, uint64_t hi);
+/* alpha(x) of src/main.cpp:128-194 in per mille (chooses y only). */
+uint32_t orc_alpha_milli(uint64_t lo, uint64_t hi);
 
 /* pi(x) by an OpenMP segmented sieve of Eratosthenes (independent count). */
 uint64_t orc_pi_sieve(uint64_t x);
