@@ -76,6 +76,8 @@ int init_context(cpx_ctx *ctx, int device)
     if (e == cudaSuccess) e = cudaDeviceGetAttribute(&ctx->sm_count, cudaDevAttrMultiProcessorCount, device);
     int optin = 0;
     if (e == cudaSuccess) e = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device);
+    int per_sm = 0;
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&per_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, device);
     for (cudaEvent_t *ev : {&ctx->ev_hard0, &ctx->ev_hard1, &ctx->ev_b0, &ctx->ev_b1, &ctx->ev_t0, &ctx->ev_t1})
         if (e == cudaSuccess) e = cudaEventCreate(ev);
     if (e != cudaSuccess) {
@@ -83,6 +85,7 @@ int init_context(cpx_ctx *ctx, int device)
         return CPX_ECUDA;
     }
     ctx->smem_optin = (size_t)optin;
+    ctx->smem_per_sm = (size_t)per_sm;
     each_buf(ctx, [&](DevBuf &b) { b.stream = ctx->stream; });
     return CPX_OK;
 }
@@ -193,6 +196,7 @@ int cpx_set_hard_params(cpx_ctx *ctx, uint32_t log2_bits, uint32_t threads)
         if ((1u << log2_bits) < 128u * threads) fail(CPX_EINVAL, "segment smaller than 128 bits per thread");
         ctx->hard_log2_bits = log2_bits;
         ctx->hard_threads = threads;
+        ctx->hard_params_set = true;
     });
 }
 

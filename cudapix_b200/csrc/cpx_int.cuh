@@ -208,6 +208,34 @@ __device__ __forceinline__ u128 cpx_qdiv(u128 n, uint64_t d)
     return cpx_udiv128_slow(n, d);
 }
 
+// floor(n / d) for n < 2^40 and d < 2^32, with nd = n as a double.  The
+// reciprocal estimate comes from the hardware approximation (relative error
+// at most 2^-22); one Newton-Raphson step in double brings it below 2^-43, so
+// trunc(n rd) is within 1 of the quotient (< 2^40), and the sign and size of
+// n - q d fix it without a branch.
+__device__ __forceinline__ uint64_t cpx_quot40(uint64_t n, double nd, uint32_t d)
+{
+    float rf;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(rf) : "f"(__uint2float_rn(d)));
+    const double r = (double)rf;
+    const double rd = __fma_rn(r, __fma_rn(-(double)d, r, 1.0), r);
+    const uint64_t u = __double2ull_rz(__dmul_rn(nd, rd));
+    const int64_t rem = (int64_t)(n - u * d);
+    return u + (rem >= (int64_t)d) - (rem < 0);
+}
+
+// pi(floor(n / d)) of an easy leaf whose dividend n = x/p is below 2^40 and
+// whose quotient u is below 2^32 (u < sqrt(x) for x < 2^64), by cpx_quot40.
+// u >= 2; pi(u) = 1 + entry prefix + bits 0..j of the entry's bitmap,
+// j = ((u - 1) mod 128) / 2.
+__device__ __forceinline__ uint64_t cpx_pi_quot40(const cpx_pient *__restrict__ T, uint64_t n, double nd, uint32_t d)
+{
+    const uint32_t m = (uint32_t)cpx_quot40(n, nd, d) - 1;
+    const ulonglong2 e = __ldg(reinterpret_cast<const ulonglong2 *>(T) + (m >> 7));
+    const uint32_t j = (m & 127u) >> 1;
+    return 1 + e.y + (uint64_t)__popcll(e.x << (63 - j));
+}
+
 // ------------------------------------------------ 128-bit atomic accumulate
 // Two 64-bit atomics; the carry out of the low word is added to the high word
 // by the same thread, which makes the final 128-bit total exact in any order.

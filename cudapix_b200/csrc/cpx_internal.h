@@ -107,9 +107,11 @@ struct cpx_ctx {
     bool server_attached = false;  // the context's tables serve a cpx_server
     int sm_count = 148;
     size_t smem_optin = 0;
+    size_t smem_per_sm = 0;
     // tuning
     uint32_t hard_log2_bits = 18;  // hard-leaf segment size (odd numbers, bits)
     uint32_t hard_threads = 256;
+    bool hard_params_set = false;      // cpx_set_hard_params was called (no size rule then)
     uint32_t hard_offload_min = 1024;  // candidates of a (sub-segment, level) sent to k_hard_leaves
     uint32_t hard_shared = 1;          // batch-shared sieve: 0 never, 1 batches, 2 always
     uint64_t hard_offload_bytes = 4ull << 30;  // snapshot pool budget of one batch

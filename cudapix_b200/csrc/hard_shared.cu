@@ -92,7 +92,7 @@ __global__ void __launch_bounds__(1024, 1) k_sieve_counts(uint64_t nseg, uint32_
             const uint32_t b = gb + k;
             const uint32_t p = __shfl_sync(FULL, lp, k);
             if (lane == 0) {
-                const uint64_t first = ((uint64_t)p * p) / span;
+                const uint64_t first = ((uint64_t)p * p) >> (lbits + 1);  // / span
                 const uint64_t idx = lvl_off[b - c - 1] + (w - first * NW);
                 if (idx < lvl_off[b - c]) cnt[idx] = tot;
             }
@@ -267,11 +267,12 @@ static __device__ __noinline__ bool offload_sets(bool off_j, uint32_t lane, uint
 // Sum(-mu) for the query of its last leaf and adds them into the warp's
 // per-query slots when the query changes; at the end of the level lane j
 // folds slot j into its total as sum + carry * Sum(-mu).
-// LB is the launch bound: blocks of 1024 threads (32 warps per SM) leave 64
-// registers a thread, blocks of up to 512 threads leave up to 128, which the
-// level loop uses without spilling.
-template <class XT, int LB>
-__global__ void __launch_bounds__(LB, 1)
+// The launch bounds (at most TMAX threads, at least MINB blocks per SM) set
+// the register budget: 65536 / (TMAX MINB) a thread, 64 when 32 warps share
+// an SM and 128 (no spills) when 16 do.  The launch takes the variant whose
+// MINB blocks fit the SM's shared memory with this segment size.
+template <class XT, int TMAX, int MINB>
+__global__ void __launch_bounds__(TMAX, MINB)
     k_hard_shared(const QD *__restrict__ qd, const HardGroup *__restrict__ grp, const uint64_t *__restrict__ pre_grp,
                   uint32_t ngrp, uint64_t total, uint32_t lbits, uint32_t c, const uint32_t *__restrict__ P,
                   uint32_t np, const int32_t *__restrict__ MU, const cpx_pient *__restrict__ Tpi,
@@ -321,13 +322,17 @@ __global__ void __launch_bounds__(LB, 1)
     // this lane's query
     const uint32_t nq = G.n;
     const uint32_t qj = lane < nq ? G.q[lane] : 0xFFFFFFFFu;
-    XT xj = 0;
-    uint64_t yj = 0, zj = 0;
+    // the lane's query has leaves in the warp's sub-segment at level b only
+    // if lo_w <= z, p^2 < hi_w and x / (p hi_w) < y, i.e. p > pthr =
+    // floor(x / (y hi_w)); y < 2^31
+    bool qin = false;
+    uint32_t yj = 0, pthr = 0xFFFFFFFFu;
     if (lane < nq) {
         const QD &d = qd[qj];
-        xj = xload<XT>(d);
-        yj = d.y;
-        zj = d.z;
+        yj = (uint32_t)d.y;
+        qin = lo_w <= d.z;
+        const u128 t = (u128)xload<XT>(d) / ((u128)d.y * hi_w);
+        pthr = t < 0xFFFFFFFFull ? (uint32_t)t : 0xFFFFFFFFu;
     }
     i128 accq = 0;  // this lane's query: its hard sum over the CTA's part of the segment
 
@@ -336,15 +341,28 @@ __global__ void __launch_bounds__(LB, 1)
     __syncwarp();
     const uint64_t w = seg * NW + warp;
     auto sub_count = [&](uint64_t uu) -> uint32_t { return sub_survivors(uu, lo_w, wl, cnt8, bm, CPT, s, warp); };
+    // the leaf quotient x/(p m): cpx_quot40 when x < 2^64 and x/p < 2^40 (xpd = x/p as a double)
+    auto hq = [&](XT xv, double xvd, uint64_t m) -> uint64_t {
+        if (sizeof(XT) == 8 && (uint64_t)xv < (1ull << 40)) return cpx_quot40((uint64_t)xv, xvd, (uint32_t)m);
+        return (uint64_t)cpx_qdiv(xv, m);
+    };
     const Recip r_lo{lo_w, lo_w ? 1.0 / (double)lo_w : 0.0}, r_hi{hi_w, 1.0 / (double)hi_w};
     const size_t gbase = (size_t)g * nlv * 32 + lane;  // this lane's slot in the group's level table
 
     for (uint32_t gb = c + 1; gb <= B; gb += 32) {
         const uint32_t nl = min(32u, B - gb + 1);
+        // per lane k, level gb + k: its prime, crossing-off start and the
+        // carry of the warp's sub-segment (survivors of level b - 1 below it,
+        // row b of the counting sweep), all loaded at once
         uint32_t lp = 0, lr0 = 0, li0 = 0xFFFFFFFFu;
+        uint64_t lC = 0;
         if (lane < nl) {
-            lp = P[gb + lane - 1];
+            const uint32_t bl = gb + lane;
+            lp = P[bl - 1];
             cross_params(lp, lo_w, hi_w, lr0, li0);
+            const uint64_t first = ((uint64_t)lp * lp) >> (lbits + 1);  // / span
+            const uint64_t ci = lvl_off[bl - c - 1] + (w - first * NW);
+            if (ci < lvl_off[bl - c]) lC = __ldg(carry + ci);
         }
         for (uint32_t k = 0; k < nl; k++) {
             const uint32_t b = gb + k;
@@ -356,7 +374,7 @@ __global__ void __launch_bounds__(LB, 1)
             XT xp = 0;
             uint32_t mlo = 0, mhi = 0;
             bool act = false;
-            if (lane < nq && lo_w <= zj && hi_w > pp && (u128)p * yj * hi_w > (u128)xj) {
+            if (qin && hi_w > pp && p > pthr) {
                 const size_t gi = gbase + (size_t)(b - c - 1) * 32;
                 xp = gxp[gi];
                 const uint2 ae = gae[gi];  // y/p, min(y, x/p^3)
@@ -380,9 +398,7 @@ __global__ void __launch_bounds__(LB, 1)
                 wl[lane] = off0;
                 if (act) s_xp[lane] = xp;
                 __syncwarp();
-                const uint64_t first = pp / span;
-                const uint64_t ci = lvl_off[b - c - 1] + (w - first * NW);
-                const uint64_t C = ci < lvl_off[b - c] ? __ldg(carry + ci) : 0;  // survivors below the sub-segment
+                const uint64_t C = __shfl_sync(FULL, lC, k);  // survivors below the sub-segment
                 const bool prime_j = pp > yj;  // m must be a prime q > max(mlo, p)
                 const uint32_t qa_j = mlo > p ? mlo : p;
                 uint64_t work = 0;
@@ -406,13 +422,14 @@ __global__ void __launch_bounds__(LB, 1)
                     // answers its own query's candidates
                     int64_t sv = 0;
                     int32_t sm = 0;
+                    const double xpd = (double)(uint64_t)xp;
                     for (uint32_t k2 = 0; k2 < nw_j; k2++) {
                         const uint64_t wq = (qa_j >> 7) + k2;
                         uint64_t qb = __ldg(reinterpret_cast<const ulonglong2 *>(Tpi) + wq).x & range_mask(wq, qa_j, mhi);
                         while (qb) {
                             const int jb = __ffsll((long long)qb) - 1;
                             qb &= qb - 1;
-                            sv += sub_count((uint64_t)cpx_qdiv(xp, 128 * wq + 2 * jb + 1));  // mu(q) = -1
+                            sv += sub_count(hq(xp, xpd, 128 * wq + 2 * jb + 1));  // mu(q) = -1
                             sm += 1;
                         }
                     }
@@ -425,7 +442,7 @@ __global__ void __launch_bounds__(LB, 1)
                         while (vm) {
                             const int kq = __ffs(vm) - 1;
                             vm &= vm - 1;
-                            const uint32_t cv = sub_count((uint64_t)cpx_qdiv(xp, 2 * (4 * g4 + kq) + 1));
+                            const uint32_t cv = sub_count(hq(xp, xpd, 2 * (4 * g4 + kq) + 1));
                             if ((neg >> kq) & 1u) {
                                 sv += cv;
                                 sm += 1;
@@ -466,7 +483,8 @@ __global__ void __launch_bounds__(LB, 1)
                     for (uint32_t jj = lane; jj < nbuf; jj += 32) {
                         const uint2 e = lbuf[jj];
                         const uint32_t key = e.y & 31u;
-                        put(key, sub_count((uint64_t)cpx_qdiv(s_xp[key], (uint64_t)e.x)), (e.y >> 31) != 0);
+                        const XT xk = s_xp[key];
+                        put(key, sub_count(hq(xk, (double)(uint64_t)xk, e.x)), (e.y >> 31) != 0);
                     }
                     __syncwarp();
                     nbuf = 0;
@@ -502,7 +520,7 @@ __global__ void __launch_bounds__(LB, 1)
                             while (qb) {
                                 const int jb = __ffsll((long long)qb) - 1;
                                 qb &= qb - 1;
-                                put(jq, sub_count((uint64_t)cpx_qdiv(xq, 128 * wq + 2 * jb + 1)), true);  // mu(q) = -1
+                                put(jq, sub_count(hq(xq, (double)(uint64_t)xq, 128 * wq + 2 * jb + 1)), true);  // mu(q) = -1
                             }
                             continue;
                         }
@@ -580,6 +598,14 @@ __global__ void __launch_bounds__(LB, 1)
 
 size_t hard_shared_smem_bytes(uint32_t lbits, uint32_t threads) { return shared_smem(lbits, threads); }
 
+// blocks of k_hard_shared one SM's shared memory holds (1 KB of each is the
+// runtime's reservation)
+static int shared_blocks_per_sm(const cpx_ctx *ctx, uint32_t lbits, uint32_t threads)
+{
+    const size_t per = shared_smem(lbits, threads) + 1024;
+    return (int)std::max<size_t>(1, (ctx->smem_per_sm ? ctx->smem_per_sm : 233472) / per);
+}
+
 template <class XT> static void shared_go(cpx_ctx *ctx, const Plan &pl)
 {
     const Tables &tb = ctx->tab;
@@ -619,8 +645,10 @@ template <class XT> static void shared_go(cpx_ctx *ctx, const Plan &pl)
                 tb.T, pl.lvl_off, pl.sh_nlv, pl.carry, pl.acc, pl.jobs, pl.njobs, pl.job_units, pl.snap, pl.nsnap,
                 pl.max_jobs, lbits_sub, (uint32_t)std::min<uint64_t>(pl.offload_min, 0xFFFFFFFFull), gxp, pl.gae);
         };
-        if (T > 512) go(k_hard_shared<XT, 1024>);
-        else go(k_hard_shared<XT, 512>);
+        const int fit = shared_blocks_per_sm(ctx, pl.sh_lbits, T);
+        if (T > 512) go(k_hard_shared<XT, 1024, 1>);
+        else if (T > 256) fit >= 2 ? go(k_hard_shared<XT, 512, 2>) : go(k_hard_shared<XT, 512, 1>);
+        else fit >= 4 ? go(k_hard_shared<XT, 256, 4>) : go(k_hard_shared<XT, 256, 2>);
     }
     CPX_LAUNCH("k_hard_shared");
     note_launch(ctx);
@@ -649,13 +677,16 @@ void prepare_hard_shared(cpx_ctx *ctx, const Plan &pl)
     const int w = pl.wide ? 1 : 0;
     if (done_dev[w] == ctx->device) return;
     raise_dyn_smem(k_sieve_counts, ctx->smem_optin);
-    if (pl.wide) {
-        raise_dyn_smem(k_hard_shared<u128, 1024>, ctx->smem_optin);
-        raise_dyn_smem(k_hard_shared<u128, 512>, ctx->smem_optin);
-    } else {
-        raise_dyn_smem(k_hard_shared<uint64_t, 1024>, ctx->smem_optin);
-        raise_dyn_smem(k_hard_shared<uint64_t, 512>, ctx->smem_optin);
-    }
+    auto raise_all = [&](auto xt) {
+        using XT = decltype(xt);
+        raise_dyn_smem(k_hard_shared<XT, 1024, 1>, ctx->smem_optin);
+        raise_dyn_smem(k_hard_shared<XT, 512, 1>, ctx->smem_optin);
+        raise_dyn_smem(k_hard_shared<XT, 512, 2>, ctx->smem_optin);
+        raise_dyn_smem(k_hard_shared<XT, 256, 2>, ctx->smem_optin);
+        raise_dyn_smem(k_hard_shared<XT, 256, 4>, ctx->smem_optin);
+    };
+    if (pl.wide) raise_all(u128());
+    else raise_all(uint64_t());
     done_dev[w] = ctx->device;
 }
 

@@ -488,30 +488,32 @@ uint64_t extract_primes_u64(cpx_ctx *ctx, uint64_t lo, uint64_t hi, uint64_t *d_
 
 // ----------------------------------------------------------- mu / lpf sieve
 
-// odd numbers per CTA: 12 bytes of shared state each for 32-bit words, 20 for 64-bit
+// odd numbers per CTA: 8 bytes of shared state each for 32-bit words, 12 for 64-bit
 template <class W> struct MuSeg { static constexpr uint32_t N = sizeof(W) == 4 ? 4096 : 2048; };
 
-// multiply a shared-memory word by p (compare-and-swap loop)
-__device__ __forceinline__ void atomic_mul_shared(unsigned int *a, unsigned int p)
+// Mitchell's approximation of log2(v), v >= 1, in units of 2^-16: the bit
+// position of the leading one plus the next 16 bits read as a fraction.  It
+// never exceeds log2(v) and falls short of it by less than 0.0861 + 2^-16.
+__device__ __forceinline__ uint32_t mitchell_log2_q16(uint64_t v)
 {
-    unsigned int old = *a, assumed;
-    do {
-        assumed = old;
-        old = atomicCAS(a, assumed, assumed * p);
-    } while (old != assumed);
-}
-__device__ __forceinline__ void atomic_mul_shared(unsigned long long *a, unsigned long long p)
-{
-    unsigned long long old = *a, assumed;
-    do {
-        assumed = old;
-        old = atomicCAS(a, assumed, assumed * p);
-    } while (old != assumed);
+    const int e = 63 - __clzll((long long)v);
+    const uint64_t frac = ((v << (63 - e)) << 1) >> 48;
+    return ((uint32_t)e << 16) | (uint32_t)frac;
 }
 
-// Per odd n of the segment: smallest prime factor found (atomicMin), product
-// of distinct prime factors <= sqrt(hi) (CAS multiply), their count and a
-// square flag.  A remaining cofactor > 1 is one prime above sqrt(hi).
+// Per odd n of the segment (sieving primes p with p^2 < hi):
+//   s_lpf: the smallest prime factor found (atomicMin);
+//   s_acc: bits 0..23 the sum of mitchell_log2_q16(p) over the distinct
+//          prime factors found, bits 24..29 their count, bit 31 a square
+//          factor (one atomicAdd and, for multiples of p^2, one atomicOr).
+// An odd n < hi has at most one prime factor q that is not found (q^2 >= hi),
+// and only then is the log sum short of mitchell_log2_q16(n) by log2(q) > 1.49
+// less the approximation errors; without it the sum exceeds the log of n by at
+// most 15 x 0.0862 < 1.3 (an odd n < 2^64 has at most 15 distinct prime
+// factors).  So "cofactor" is exactly: log of n minus the sum > 1.4.
+// The reference multiplies the prime factors into a word with a
+// compare-and-swap loop (src/sieve/lpf_mu.cu:89-108); the log sum needs none.
+constexpr uint32_t kCofactorQ16 = 91750;  // 1.4 in units of 2^-16
 template <class W>
 __global__ void __launch_bounds__(kThreads) k_mulpf(uint64_t lo0, uint64_t hi_all, const uint32_t *__restrict__ P,
                                                     uint32_t np, uint32_t nsmall, int8_t *__restrict__ mu,
@@ -520,54 +522,48 @@ __global__ void __launch_bounds__(kThreads) k_mulpf(uint64_t lo0, uint64_t hi_al
 {
     constexpr uint32_t kMuSeg = MuSeg<W>::N;
     __shared__ W s_lpf[kMuSeg];
-    __shared__ W s_prod[kMuSeg];
-    __shared__ uint32_t s_cnt[kMuSeg];
+    __shared__ uint32_t s_acc[kMuSeg];
     const uint32_t tid = threadIdx.x;
     const uint64_t lo = lo0 + (uint64_t)blockIdx.x * 2 * kMuSeg;
     const uint64_t hi = lo + 2 * kMuSeg;  // exclusive
     for (uint32_t i = tid; i < kMuSeg; i += kThreads) {
         s_lpf[i] = (W)~(W)0;
-        s_prod[i] = 1;
-        s_cnt[i] = 0;
+        s_acc[i] = 0;
     }
     __syncthreads();
+    auto square_flags = [&](uint64_t p, uint32_t t0, uint32_t step) {
+        const uint64_t p2 = p * p;
+        if (p2 >= hi) return;
+        uint64_t r = (lo + 1) % p2;
+        uint64_t m = lo + 1 + (r ? p2 - r : 0);
+        if ((m & 1) == 0) m += p2;
+        for (m += (uint64_t)t0 * 2 * p2; m < hi; m += (uint64_t)step * 2 * p2)
+            atomicOr(&s_acc[(m - lo - 1) >> 1], 0x80000000u);
+    };
     // primes from P[1] (3) while p^2 < hi; the first nsmall by all threads
     for (uint32_t k = 1; k < np && k <= nsmall; k++) {
         const uint64_t p = P[k];
         if (p * p >= hi) break;
         uint32_t i0 = first_odd_multiple_idx(lo, hi, p, false);
         if (i0 == 0xFFFFFFFFu) continue;
+        const uint32_t add = mitchell_log2_q16(p) + (1u << 24);
         for (uint32_t i = i0 + tid * (uint32_t)p; i < kMuSeg; i += kThreads * (uint32_t)p) {
             atomicMin(&s_lpf[i], (W)p);
-            atomic_mul_shared(&s_prod[i], (W)p);
-            atomicAdd(&s_cnt[i], 1u);
+            atomicAdd(&s_acc[i], add);
         }
-        const uint64_t p2 = p * p;
-        if (p2 < hi) {
-            uint64_t r = (lo + 1) % p2;
-            uint64_t m = lo + 1 + (r ? p2 - r : 0);
-            if ((m & 1) == 0) m += p2;
-            for (m += tid * 2 * p2; m < hi; m += (uint64_t)kThreads * 2 * p2)
-                atomicOr(&s_cnt[(m - lo - 1) >> 1], 0x80000000u);
-        }
+        square_flags(p, tid, kThreads);
     }
     for (uint32_t k = nsmall + 1 + tid; k < np; k += kThreads) {
         const uint64_t p = P[k];
         if (p * p >= hi) break;
         uint32_t i0 = first_odd_multiple_idx(lo, hi, p, false);
         if (i0 == 0xFFFFFFFFu) continue;
+        const uint32_t add = mitchell_log2_q16(p) + (1u << 24);
         for (uint32_t i = i0; i < kMuSeg; i += (uint32_t)p) {
             atomicMin(&s_lpf[i], (W)p);
-            atomic_mul_shared(&s_prod[i], (W)p);
-            atomicAdd(&s_cnt[i], 1u);
+            atomicAdd(&s_acc[i], add);
         }
-        const uint64_t p2 = p * p;
-        if (p2 < hi) {
-            uint64_t r = (lo + 1) % p2;
-            uint64_t m = lo + 1 + (r ? p2 - r : 0);
-            if ((m & 1) == 0) m += p2;
-            for (; m < hi; m += 2 * p2) atomicOr(&s_cnt[(m - lo - 1) >> 1], 0x80000000u);
-        }
+        square_flags(p, 0, 1);
     }
     __syncthreads();
     for (uint32_t i = tid; i < kMuSeg; i += kThreads) {
@@ -580,12 +576,12 @@ __global__ void __launch_bounds__(kThreads) k_mulpf(uint64_t lo0, uint64_t hi_al
             m = 1;
             l = 0xFFFFFFFFull;
         } else {
-            const uint32_t cnt = s_cnt[i];
-            const W pr = s_prod[i];
+            const uint32_t a = s_acc[i];
             l = (s_lpf[i] == (W)~(W)0) ? n : (uint64_t)s_lpf[i];
-            if (cnt & 0x80000000u) m = 0;
+            if (a & 0x80000000u) m = 0;
             else {
-                uint32_t k = (cnt & 0xFFFFu) + ((uint64_t)pr < n ? 1u : 0u);
+                const bool cofactor = mitchell_log2_q16(n) > (a & 0xFFFFFFu) + kCofactorQ16;
+                const uint32_t k = ((a >> 24) & 0x3Fu) + (cofactor ? 1u : 0u);
                 m = (k & 1) ? -1 : 1;
             }
         }

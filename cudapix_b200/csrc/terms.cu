@@ -389,12 +389,16 @@ __global__ void __launch_bounds__(kThreads) k_easy(const QD *__restrict__ qd, ui
             const uint64_t w_end = min(w_beg + kEasyChunk, ((e.q1 - 1) >> 7) + 1);
             uint64_t ps = 0, cnt = 0;
             uint32_t nbuf = 0;
+            // x < 2^64 and x/p < 2^40: every quotient below 2^32, taken by cpx_pi_quot40
+            const bool fast = sizeof(XT) == 8 && (uint64_t)xp < (1ull << 40);
+            const double xpd = (double)(uint64_t)xp;
+            auto leaf = [&](uint32_t q) -> uint64_t {
+                return fast ? cpx_pi_quot40(T, (uint64_t)xp, xpd, q) : cpx_pi_dev(T, (uint64_t)cpx_qdiv(xp, (uint64_t)q));
+            };
             auto flush = [&] {
                 __syncwarp();
-                for (uint32_t jj = lane; jj < nbuf; jj += 32) {
-                    ps += cpx_pi_dev(T, (uint64_t)cpx_qdiv(xp, (uint64_t)qbuf[jj]));
-                    cnt++;
-                }
+                if (lane < nbuf) cnt += (nbuf - lane + 31) / 32;
+                for (uint32_t jj = lane; jj < nbuf; jj += 32) ps += leaf(qbuf[jj]);
                 __syncwarp();
                 nbuf = 0;
             };
@@ -414,7 +418,7 @@ __global__ void __launch_bounds__(kThreads) k_easy(const QD *__restrict__ qd, ui
                     while (qb) {
                         const int j2 = __ffsll((long long)qb) - 1;
                         qb &= qb - 1;
-                        ps += cpx_pi_dev(T, (uint64_t)cpx_qdiv(xp, 128 * wq + 2 * j2 + 1));
+                        ps += leaf((uint32_t)(128 * wq + 2 * j2 + 1));
                         cnt++;
                     }
                     continue;

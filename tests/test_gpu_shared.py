@@ -144,16 +144,24 @@ def test_batch_alpha_only_for_queries_with_companions(own, cpx):
     assert cpx.terms_batch(xs, ctx=own) == got
 
 
-def test_shared_sieve_over_budget_replans_without_batch_alpha(own, cpx):
-    """Seventeen queries near 1e18 have companions, but the batch alpha would
-    give the shared sieve's counting sweep 22.5 GB of carry rows, above the
-    16 GiB budget: the batch is planned again with each decade's alpha (y as
-    for the query alone; 6.6 GB of rows, so the sieve is still shared) and
-    the answers are exact."""
+def test_shared_sieve_over_budget_replans_without_batch_alpha(own, cpx, tmp_path):
+    """Seventeen queries near 1e18 have companions, but with 1024-thread
+    blocks over 2^20-bit segments the batch alpha would give the shared
+    sieve's counting sweep 22.5 GB of carry rows, above the 16 GiB budget: the
+    batch is planned again with each decade's alpha (y as for the query alone;
+    6.6 GB of rows, so the sieve is still shared) and the answers are exact."""
+    import json
     import os
 
     root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
-    own.tune_load(os.path.join(root, "cudapix_b200", "tuning", "b200.json"))
+    with open(os.path.join(root, "cudapix_b200", "tuning", "b200.json")) as f:
+        tune = json.load(f)
+    for e in tune["entries"]:
+        if e["decade"] == 99:
+            e["threads"], e["log2_bits"] = 1024, 20
+    path = tmp_path / "tune.json"
+    path.write_text(json.dumps(tune))
+    own.tune_load(str(path))
     xs = [10**18 + k * 3 * 10**16 + 1 for k in range(17)]
     got = cpx.terms_batch(xs, ctx=own)
     assert own.last_batch_stats()["shared_groups"] >= 1
