@@ -254,10 +254,17 @@ static __device__ __noinline__ bool offload_sets(bool off_j, uint32_t lane, uint
     return off_j;
 }
 
+// Candidate entries (pi-table words or 4-m groups) a lane answers itself;
+// above it on any lane the warp gathers the level's leaves (on the B200 the
+// 4096-query batch took 49.0 / 46.0 / 41.4 / 40.9 ms of this kernel with 8 /
+// 16 / 32 / 64)
+constexpr uint32_t kLaneEntries = 64;
+
 // (3) One CTA per (group, segment).  Per level, the lanes hold one query
 // each: its x/p and candidate range in the warp's sub-segment.  When no query
-// has more than 8 candidate table entries (most levels: about one leaf per
-// query), each lane answers its own query's leaves into its 128-bit total.
+// has more than kLaneEntries candidate table entries (98% of the visits of
+// the 4096-query batch, with about 1.3 entries a query), each lane answers
+// its own query's leaves into its 128-bit total.
 // Otherwise the warp walks the candidates of all the group's queries as one
 // sequence (pi-table words of the prime-only levels, then 4-m groups of
 // packed mu*lpf of the others), 32 words at a time, each lane finding its
@@ -416,10 +423,10 @@ __global__ void __launch_bounds__(TMAX, MINB)
                 uint32_t ng_j = 0;
                 if (act && !off_j && !prime_j)
                     ng_j = (uint32_t)(((((uint64_t)mhi - 1) >> 1) >> 2) - ((((uint64_t)mlo + 1) >> 1) >> 2) + 1);
-                if (!__any_sync(FULL, nw_j > 8 || ng_j > 8)) {
+                if (!__any_sync(FULL, nw_j > kLaneEntries || ng_j > kLaneEntries)) {
                     // a sparse level (the common case: about one leaf per query;
-                    // at most 8 table entries or 4-m groups each): each lane
-                    // answers its own query's candidates
+                    // at most kLaneEntries table entries or 4-m groups each):
+                    // each lane answers its own query's candidates
                     int64_t sv = 0;
                     int32_t sm = 0;
                     const double xpd = (double)(uint64_t)xp;

@@ -310,14 +310,28 @@ __device__ __forceinline__ uint32_t sub_survivors(uint64_t uu, uint64_t lo_w, co
     const uint32_t jb = kk - 1, w = jb >> 5;
     const uint32_t chs = w >> 2, ow = chs >> s;  // chunk in the sub-segment, owning lane
     const uint32_t ch = chs + CPT * 32 * warp;   // chunk in the segment
-    uint32_t cv = wl[ow] + counter_sum(cnt8 + ch - (chs - ow * CPT), chs - ow * CPT);
+    const uint32_t n = chs - ow * CPT;           // the owner's counters before the chunk
+    uint32_t cv = wl[ow];
+    if (CPT >= 4) {
+        // the owner's counters as CPT/4 aligned words (CPT is a power of two);
+        // a trip count uniform over the warp, the counters before the chunk
+        // selected by a byte mask
+        const uint32_t *cw = reinterpret_cast<const uint32_t *>(cnt8 + ch - n);
+        for (uint32_t i = 0; i < (CPT >> 2); i++) {
+            const int r = (int)n - 4 * (int)i;
+            const uint32_t sel = r >= 4 ? 0x01010101u : (r <= 0 ? 0u : (0x01010101u & ((1u << (8 * r)) - 1u)));
+            cv = __dp4a(cw[i], sel, cv);
+        }
+    } else {
+        for (uint32_t i = 0; i < n; i++) cv += cnt8[ch - n + i];
+    }
     const uint4 v4 = reinterpret_cast<const uint4 *>(bm)[swz(ch, s)];
     const uint32_t wi = w & 3, msk = (2u << (jb & 31)) - 1u;
-    if (wi == 0) cv += __popc(v4.x & msk);
-    else if (wi == 1) cv += __popc(v4.x) + __popc(v4.y & msk);
-    else if (wi == 2) cv += __popc(v4.x) + __popc(v4.y) + __popc(v4.z & msk);
-    else cv += __popc(v4.x) + __popc(v4.y) + __popc(v4.z) + __popc(v4.w & msk);
-    return cv;
+    const uint32_t m0 = wi > 0 ? ~0u : msk;
+    const uint32_t m1 = wi > 1 ? ~0u : (wi == 1 ? msk : 0u);
+    const uint32_t m2 = wi > 2 ? ~0u : (wi == 2 ? msk : 0u);
+    const uint32_t m3 = wi == 3 ? msk : 0u;
+    return cv + __popc(v4.x & m0) + __popc(v4.y & m1) + __popc(v4.z & m2) + __popc(v4.w & m3);
 }
 
 // B(seg) = pi(min(r4, isqrt((x - 1) / lo), isqrt(hi - 1))): the levels b a

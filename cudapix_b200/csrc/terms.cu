@@ -398,7 +398,13 @@ __global__ void __launch_bounds__(kThreads) k_easy(const QD *__restrict__ qd, ui
             auto flush = [&] {
                 __syncwarp();
                 if (lane < nbuf) cnt += (nbuf - lane + 31) / 32;
-                for (uint32_t jj = lane; jj < nbuf; jj += 32) ps += leaf(qbuf[jj]);
+                // two leaves a lane at a time: their quotients and table gathers overlap
+                uint32_t jj = lane;
+                for (; jj + 32 < nbuf; jj += 64) {
+                    const uint32_t qa = qbuf[jj], qb2 = qbuf[jj + 32];
+                    ps += leaf(qa) + leaf(qb2);
+                }
+                if (jj < nbuf) ps += leaf(qbuf[jj]);
                 __syncwarp();
                 nbuf = 0;
             };
