@@ -114,6 +114,7 @@ struct cpx_ctx {
     bool hard_params_set = false;      // cpx_set_hard_params was called (no size rule then)
     uint32_t hard_offload_min = 1024;  // candidates of a (sub-segment, level) sent to k_hard_leaves
     uint32_t hard_shared = 1;          // batch-shared sieve: 0 never, 1 batches, 2 always
+    uint32_t hard_persist = 1;         // shared sieve as a persistent launch over a unit queue
     uint64_t hard_offload_bytes = 4ull << 30;  // snapshot pool budget of one batch
     uint64_t p2_table_limit = 1ull << 36;      // z beyond this: P2 by pi-table windows
     cpx::TuneEntry tune[cpx::kTuneDecades] = {};  // per decade (batches of up to 4 queries)

@@ -861,7 +861,9 @@ replan:  // again without the batch alpha when its shared sieve would not fit (b
     const size_t elv_bytes = elv.size() * sizeof(EasyLvl);
     const size_t grp_bytes = groups.size() * sizeof(HardGroup);
     const size_t pg_bytes = (pre_grp.size() * 8 + 15) & ~size_t(15), lo_bytes = (lvl_off.size() * 8 + 15) & ~size_t(15);
-    const size_t stage_bytes = qd_bytes + pre_bytes + elv_bytes + grp_bytes + pg_bytes + lo_bytes;
+    const bool persist = shared && ctx->hard_persist && pre_grp.back() <= 0xFFFFFFFFull;
+    const size_t ord_bytes = persist ? ((pre_grp.back() * 4 + 15) & ~size_t(15)) : 0;
+    const size_t stage_bytes = qd_bytes + pre_bytes + elv_bytes + grp_bytes + pg_bytes + lo_bytes + ord_bytes;
     const size_t acc_words = (size_t)Q * kAccStride;
     unsigned char *dbuf = (unsigned char *)ctx->b_work[0].get(stage_bytes + acc_words * 8 + 64);
     QD *d_qd = reinterpret_cast<QD *>(dbuf);
@@ -894,6 +896,10 @@ replan:  // again without the batch alpha when its shared sieve would not fit (b
         pl.grp = reinterpret_cast<const HardGroup *>(d_sh);
         pl.pre_grp = reinterpret_cast<const uint64_t *>(d_sh + grp_bytes);
         pl.lvl_off = reinterpret_cast<const uint64_t *>(d_sh + grp_bytes + pg_bytes);
+        if (persist) {
+            pl.unit_order = reinterpret_cast<const uint32_t *>(d_sh + grp_bytes + pg_bytes + lo_bytes);
+            pl.unit_next = d_acc + acc_words;  // zeroed with the accumulators
+        }
         pl.carry = ctx->b_work[4].as<uint64_t>(pl.n_carry + 1);
         const size_t ntab = groups.size() * (size_t)sh_nlv * 32, xb = wide ? 16 : 8;
         unsigned char *tab = static_cast<unsigned char *>(ctx->b_work[5].get(ntab * (xb + 8) + 64));
@@ -968,9 +974,18 @@ replan:  // again without the batch alpha when its shared sieve would not fit (b
         memcpy(h_sh, groups.data(), grp_bytes);
         memcpy(h_sh + grp_bytes, pre_grp.data(), pre_grp.size() * 8);
         memcpy(h_sh + grp_bytes + pg_bytes, lvl_off.data(), lvl_off.size() * 8);
+        if (persist) {
+            // segment-major: every group's segment 0, then segment 1, ... (the
+            // early segments of a group hold most of its leaves)
+            uint32_t *ord = reinterpret_cast<uint32_t *>(h_sh + grp_bytes + pg_bytes + lo_bytes);
+            size_t k = 0;
+            for (uint64_t sg = 0; sg < sh_nseg; sg++)
+                for (size_t g = 0; g < groups.size(); g++)
+                    if (sg < groups[g].nseg) ord[k++] = (uint32_t)(pre_grp[g] + sg);
+        }
     }
     CPX_CUDA(cudaMemcpyAsync(dbuf, stage.data(), stage.size(), cudaMemcpyHostToDevice, ctx->stream));
-    CPX_CUDA(cudaMemsetAsync(d_acc, 0, acc_words * 8, ctx->stream));
+    CPX_CUDA(cudaMemsetAsync(d_acc, 0, acc_words * 8 + 8, ctx->stream));  // and the unit counter
 
     // ---- kernels
     auto launch_all = [&] {

@@ -181,11 +181,12 @@ __global__ void __launch_bounds__(512, 2) k_hard(const QD *__restrict__ qd, uint
                     // so that a lane with many candidates does not hold up the others.
                     int32_t msl = 0;
                     uint32_t nbuf = 0;
+                    const double xpd = (double)(uint64_t)xp;
                     auto flush = [&] {
                         __syncwarp();
                         for (uint32_t jj = lane; jj < nbuf; jj += 32) {
                             const uint32_t e = lbuf[jj];
-                            const uint32_t cv = sub_count((uint64_t)cpx_qdiv(xp, (uint64_t)(e & 0x7FFFFFFFu)));
+                            const uint32_t cv = sub_count(leaf_quot(xp, xpd, e & 0x7FFFFFFFu));
                             if (e >> 31) {
                                 S += cv;
                                 msl += 1;
@@ -213,7 +214,7 @@ __global__ void __launch_bounds__(512, 2) k_hard(const QD *__restrict__ qd, uint
                                     while (qb) {
                                         const int j = __ffsll((long long)qb) - 1;
                                         qb &= qb - 1;
-                                        S += sub_count((uint64_t)cpx_qdiv(xp, 128 * wq + 2 * j + 1));  // mu(q) = -1
+                                        S += sub_count(leaf_quot(xp, xpd, 128 * wq + 2 * j + 1));  // mu(q) = -1
                                         msl += 1;
                                     }
                                     continue;
@@ -324,20 +325,14 @@ __global__ void __launch_bounds__(kThreads) k_hard_leaves(const HardJob *__restr
         const uint4 *sb = reinterpret_cast<const uint4 *>(snap + (size_t)J.snap * stride);
         const uint32_t *spre = reinterpret_cast<const uint32_t *>(sb + ncmax);
         const XT xp = (XT)J.xp;
+        const double xpd = (double)(uint64_t)xp;
         const uint64_t lo = J.lo;
         // survivors of the sub-segment with n <= uu (the carry is added per unit)
         auto count = [&](uint64_t uu) -> uint32_t {
             const uint32_t kk = (uint32_t)((uu - lo + 1) >> 1);
             if (!kk) return 0u;  // u = lo: no number of the sub-segment is <= u
             const uint32_t jb = kk - 1, w = jb >> 5, ch = w >> 2;
-            uint32_t cv = __ldg(spre + ch);
-            const uint4 v4 = __ldg(sb + ch);
-            const uint32_t wi = w & 3, msk = (2u << (jb & 31)) - 1u;
-            if (wi == 0) cv += __popc(v4.x & msk);
-            else if (wi == 1) cv += __popc(v4.x) + __popc(v4.y & msk);
-            else if (wi == 2) cv += __popc(v4.x) + __popc(v4.y) + __popc(v4.z & msk);
-            else cv += __popc(v4.x) + __popc(v4.y) + __popc(v4.z) + __popc(v4.w & msk);
-            return cv;
+            return __ldg(spre + ch) + chunk_survivors(__ldg(sb + ch), jb);
         };
         int64_t S = 0;
         int32_t ms = 0;
@@ -348,7 +343,7 @@ __global__ void __launch_bounds__(kThreads) k_hard_leaves(const HardJob *__restr
             __syncwarp();
             for (uint32_t jj = lane; jj < nbuf; jj += 32) {
                 const uint32_t e = lbuf[jj];
-                const uint32_t cv = count((uint64_t)cpx_qdiv(xp, (uint64_t)(e & 0x7FFFFFFFu)));
+                const uint32_t cv = count(leaf_quot(xp, xpd, e & 0x7FFFFFFFu));
                 if (e >> 31) {
                     S += cv;
                     ms += 1;
@@ -384,7 +379,7 @@ __global__ void __launch_bounds__(kThreads) k_hard_leaves(const HardJob *__restr
                     while (qb) {
                         const int j = __ffsll((long long)qb) - 1;
                         qb &= qb - 1;
-                        S += count((uint64_t)cpx_qdiv(xp, 128 * wq + 2 * j + 1));  // mu(q) = -1
+                        S += count(leaf_quot(xp, xpd, 128 * wq + 2 * j + 1));  // mu(q) = -1
                         ms += 1;
                     }
                     continue;

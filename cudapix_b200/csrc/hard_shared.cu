@@ -278,21 +278,23 @@ constexpr uint32_t kLaneEntries = 64;
 // the register budget: 65536 / (TMAX MINB) a thread, 64 when 32 warps share
 // an SM and 128 (no spills) when 16 do.  The launch takes the variant whose
 // MINB blocks fit the SM's shared memory with this segment size.
-template <class XT, int TMAX, int MINB>
-__global__ void __launch_bounds__(TMAX, MINB)
-    k_hard_shared(const QD *__restrict__ qd, const HardGroup *__restrict__ grp, const uint64_t *__restrict__ pre_grp,
-                  uint32_t ngrp, uint64_t total, uint32_t lbits, uint32_t c, const uint32_t *__restrict__ P,
-                  uint32_t np, const int32_t *__restrict__ MU, const cpx_pient *__restrict__ Tpi,
-                  const uint64_t *__restrict__ lvl_off, uint32_t nlv, const uint64_t *__restrict__ carry,
-                  unsigned long long *__restrict__ acc, HardJob *__restrict__ jobs, unsigned int *__restrict__ njobs,
-                  uint64_t *__restrict__ job_units, unsigned char *__restrict__ snap, unsigned int *__restrict__ nsnap,
-                  uint32_t max_jobs, uint32_t lbits_sub, uint32_t offload_min, const XT *__restrict__ gxp,
-                  const uint2 *__restrict__ gae)
+#define CPX_HS_PARAMS                                                                                          \
+    const QD *__restrict__ qd, const HardGroup *__restrict__ grp, const uint64_t *__restrict__ pre_grp,          \
+        uint32_t ngrp, uint64_t total, uint32_t lbits, uint32_t c, const uint32_t *__restrict__ P, uint32_t np, \
+        const int32_t *__restrict__ MU, const cpx_pient *__restrict__ Tpi, const uint64_t *__restrict__ lvl_off, \
+        uint32_t nlv, const uint64_t *__restrict__ carry, unsigned long long *__restrict__ acc,                   \
+        HardJob *__restrict__ jobs, unsigned int *__restrict__ njobs, uint64_t *__restrict__ job_units,          \
+        unsigned char *__restrict__ snap, unsigned int *__restrict__ nsnap, uint32_t max_jobs, uint32_t lbits_sub, \
+        uint32_t offload_min, const XT *__restrict__ gxp, const uint2 *__restrict__ gae
+#define CPX_HS_ARGS                                                                                             \
+    qd, grp, pre_grp, ngrp, total, lbits, c, P, np, MU, Tpi, lvl_off, nlv, carry, acc, jobs, njobs, job_units, snap, \
+        nsnap, max_jobs, lbits_sub, offload_min, gxp, gae
+
+// one (group, segment) unit of the shared sieve, by one CTA
+template <class XT> __device__ __forceinline__ void hard_shared_unit(uint64_t unit, CPX_HS_PARAMS)
 {
     extern __shared__ uint4 smem4[];
     __shared__ uint32_t s_B;
-    const uint64_t unit = blockIdx.x;
-    if (unit >= total) return;
     const uint32_t g = find_q(pre_grp, ngrp, unit);
     const HardGroup &G = grp[g];
     const uint64_t seg = unit - pre_grp[g];
@@ -601,6 +603,29 @@ __global__ void __launch_bounds__(TMAX, MINB)
     }
 }
 
+// The kernel: one CTA per unit (unit_order null), or a persistent grid whose
+// CTAs take units from the device counter `next` in the order unit_order
+// gives, so that the heaviest units start first and no CTA waits at the end
+// for a late wave.
+template <class XT, int TMAX, int MINB>
+__global__ void __launch_bounds__(TMAX, MINB)
+    k_hard_shared(const uint32_t *__restrict__ unit_order, unsigned long long *__restrict__ next, CPX_HS_PARAMS)
+{
+    if (!unit_order) {
+        if (blockIdx.x < total) hard_shared_unit<XT>(blockIdx.x, CPX_HS_ARGS);
+        return;
+    }
+    __shared__ unsigned long long s_k;
+    for (;;) {
+        __syncthreads();  // every thread is done with the previous unit's shared memory
+        if (threadIdx.x == 0) s_k = atomicAdd(next, 1ull);
+        __syncthreads();
+        const unsigned long long k = s_k;
+        if (k >= total) return;
+        hard_shared_unit<XT>(unit_order[k], CPX_HS_ARGS);
+    }
+}
+
 // ------------------------------------------------------------------ launchers
 
 size_t hard_shared_smem_bytes(uint32_t lbits, uint32_t threads) { return shared_smem(lbits, threads); }
@@ -646,16 +671,22 @@ template <class XT> static void shared_go(cpx_ctx *ctx, const Plan &pl)
     }
     {
         KSpan ks(ctx, "k_hard_shared");
-        auto go = [&](auto kern) {
-            kern<<<(unsigned)pl.n_gunits, T, shared_smem(pl.sh_lbits, T), ctx->stream>>>(
-                pl.qd, pl.grp, pl.pre_grp, pl.n_grp, pl.n_gunits, pl.sh_lbits, pl.c, tb.P, (uint32_t)tb.prm_n, tb.MU,
-                tb.T, pl.lvl_off, pl.sh_nlv, pl.carry, pl.acc, pl.jobs, pl.njobs, pl.job_units, pl.snap, pl.nsnap,
-                pl.max_jobs, lbits_sub, (uint32_t)std::min<uint64_t>(pl.offload_min, 0xFFFFFFFFull), gxp, pl.gae);
+        // minb: the variant's resident blocks per SM (its launch bound; the
+        // shared memory fits them), the persistent grid's CTAs per SM
+        auto go = [&](auto kern, int minb) {
+            const size_t smem = shared_smem(pl.sh_lbits, T);
+            unsigned grid = (unsigned)pl.n_gunits;
+            if (pl.unit_order) grid = (unsigned)std::min<uint64_t>(pl.n_gunits, (uint64_t)minb * ctx->sm_count);
+            kern<<<grid, T, smem, ctx->stream>>>(
+                pl.unit_order, pl.unit_next, pl.qd, pl.grp, pl.pre_grp, pl.n_grp, pl.n_gunits, pl.sh_lbits, pl.c, tb.P,
+                (uint32_t)tb.prm_n, tb.MU, tb.T, pl.lvl_off, pl.sh_nlv, pl.carry, pl.acc, pl.jobs, pl.njobs,
+                pl.job_units, pl.snap, pl.nsnap, pl.max_jobs, lbits_sub,
+                (uint32_t)std::min<uint64_t>(pl.offload_min, 0xFFFFFFFFull), gxp, pl.gae);
         };
         const int fit = shared_blocks_per_sm(ctx, pl.sh_lbits, T);
-        if (T > 512) go(k_hard_shared<XT, 1024, 1>);
-        else if (T > 256) fit >= 2 ? go(k_hard_shared<XT, 512, 2>) : go(k_hard_shared<XT, 512, 1>);
-        else fit >= 4 ? go(k_hard_shared<XT, 256, 4>) : go(k_hard_shared<XT, 256, 2>);
+        if (T > 512) go(k_hard_shared<XT, 1024, 1>, 1);
+        else if (T > 256) fit >= 2 ? go(k_hard_shared<XT, 512, 2>, 2) : go(k_hard_shared<XT, 512, 1>, 1);
+        else fit >= 4 ? go(k_hard_shared<XT, 256, 4>, 4) : go(k_hard_shared<XT, 256, 2>, std::min(fit, 2));
     }
     CPX_LAUNCH("k_hard_shared");
     note_launch(ctx);

@@ -299,6 +299,25 @@ __device__ __forceinline__ uint32_t cross_off(uint32_t *bm, uint8_t *cnt8, uint3
     return cleared;
 }
 
+// A leaf quotient x/(p m) = xp / m: cpx_quot40 when x < 2^64 and xp < 2^40
+// (xpd = xp as a double), else cpx_qdiv.
+template <class XT> __device__ __forceinline__ uint64_t leaf_quot(XT xp, double xpd, uint64_t m)
+{
+    if (sizeof(XT) == 8 && (uint64_t)xp < (1ull << 40)) return cpx_quot40((uint64_t)xp, xpd, (uint32_t)m);
+    return (uint64_t)cpx_qdiv(xp, m);
+}
+
+// Survivors among bits 0..jb of one 16-byte bitmap chunk, without a branch.
+__device__ __forceinline__ uint32_t chunk_survivors(uint4 v4, uint32_t jb)
+{
+    const uint32_t wi = (jb >> 5) & 3, msk = (2u << (jb & 31)) - 1u;
+    const uint32_t m0 = wi > 0 ? ~0u : msk;
+    const uint32_t m1 = wi > 1 ? ~0u : (wi == 1 ? msk : 0u);
+    const uint32_t m2 = wi > 2 ? ~0u : (wi == 2 ? msk : 0u);
+    const uint32_t m3 = wi == 3 ? msk : 0u;
+    return __popc(v4.x & m0) + __popc(v4.y & m1) + __popc(v4.z & m2) + __popc(v4.w & m3);
+}
+
 // Survivors of a warp's sub-segment [lo_w, lo_w + 2 Lw) with n <= uu, uu in
 // [lo_w, hi_w), from the lane prefixes wl[] of the sub-segment, the chunk
 // counters and the chunk's popcounts.
@@ -325,13 +344,7 @@ __device__ __forceinline__ uint32_t sub_survivors(uint64_t uu, uint64_t lo_w, co
     } else {
         for (uint32_t i = 0; i < n; i++) cv += cnt8[ch - n + i];
     }
-    const uint4 v4 = reinterpret_cast<const uint4 *>(bm)[swz(ch, s)];
-    const uint32_t wi = w & 3, msk = (2u << (jb & 31)) - 1u;
-    const uint32_t m0 = wi > 0 ? ~0u : msk;
-    const uint32_t m1 = wi > 1 ? ~0u : (wi == 1 ? msk : 0u);
-    const uint32_t m2 = wi > 2 ? ~0u : (wi == 2 ? msk : 0u);
-    const uint32_t m3 = wi == 3 ? msk : 0u;
-    return cv + __popc(v4.x & m0) + __popc(v4.y & m1) + __popc(v4.z & m2) + __popc(v4.w & m3);
+    return cv + chunk_survivors(reinterpret_cast<const uint4 *>(bm)[swz(ch, s)], jb);
 }
 
 // B(seg) = pi(min(r4, isqrt((x - 1) / lo), isqrt(hi - 1))): the levels b a

@@ -115,6 +115,11 @@ struct Plan {
     unsigned int *nsnap = nullptr;      // device counter of snapshot slots
     void *gxp = nullptr;                // x/p per (group, level, slot): uint64 or u128 (wide)
     uint2 *gae = nullptr;               // y/p and min(y, x/p^3) per (group, level, slot)
+    // persistent launch of the shared sieve: its units in the order they are
+    // taken (segment-major: every group's segment 0 first, the heaviest) and
+    // the device counter that hands them out (null: one CTA per unit)
+    const uint32_t *unit_order = nullptr;
+    unsigned long long *unit_next = nullptr;
 };
 
 void launch_ordinary(cpx_ctx *ctx, const Plan &pl);
