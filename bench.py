@@ -463,7 +463,7 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--graph", type=int, default=1, help="also time the batch as one CUDA graph launch")
     ap.add_argument("--serve", type=int, default=1, help="serving sweep and the [1e10,1e15] target check")
-    ap.add_argument("--serve-lanes", type=int, default=4)
+    ap.add_argument("--serve-lanes", type=int, default=1)
     args = ap.parse_args()
     world, rank, local = dist_setup()
     # no collector passes inside the timed host-driven launch sequences (a

@@ -396,7 +396,7 @@ class Server:
     context answers no other call."""
 
     def __init__(self, ctx, lanes=4, max_batch=4096, admit_fraction=0.5, reserve_x=0, alpha=None, c=6,
-                 hard_log2_bits=0, hard_threads=0, graph=False):
+                 hard_log2_bits=0, hard_threads=0, graph=False, fill_target=0, window_us=0):
         self.ctx = ctx
         self.L = ctx.L
         cfg = ServeConfig()
@@ -405,6 +405,8 @@ class Server:
         cfg.admit_fraction = admit_fraction
         cfg.reserve_x = U128.of(reserve_x)
         cfg.params = _params(alpha, c, hard_log2_bits, hard_threads, False, graph)
+        cfg.fill_target = fill_target
+        cfg.window_us = window_us
         h = ctypes.c_void_p()
         rc = self.L.cpx_serve_create(ctx.h, ctypes.byref(cfg), ctypes.byref(h))
         if rc != 0:

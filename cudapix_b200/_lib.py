@@ -127,6 +127,8 @@ class ServeConfig(ctypes.Structure):
         ("admit_fraction", ctypes.c_double),
         ("reserve_x", U128),
         ("params", Params),
+        ("fill_target", ctypes.c_uint32),
+        ("window_us", ctypes.c_uint32),
     ]
 
 

@@ -327,10 +327,15 @@ int cpx_tune_load(cpx_ctx *ctx, const char *path)
 int cpx_tune_get(cpx_ctx *ctx, uint32_t decade, cpx_tune_entry *out)
 {
     return guarded(ctx, [&] {
-        if (!out || (decade >= kTuneDecades && decade != kBatchEntry)) fail(CPX_EINVAL, "bad decade or null output");
-        const bool b = decade == kBatchEntry;
-        const TuneEntry &t = b ? ctx->batch_tune : ctx->tune[decade];
-        const bool on = b ? ctx->batch_tuned : ctx->tuned;
+        const bool bd = decade >= kBatchDecade0 && decade < kBatchDecade0 + kTuneDecades;
+        if (!out || (decade >= kTuneDecades && decade != kBatchEntry && !bd)) fail(CPX_EINVAL, "bad decade or null output");
+        const bool b = decade == kBatchEntry || bd;
+        TuneEntry t = b ? ctx->batch_tune : ctx->tune[decade];
+        bool on = b ? ctx->batch_tuned : ctx->tuned;
+        if (bd) {
+            t.alpha_milli = ctx->batch_alpha_dec[decade - kBatchDecade0];
+            on = on && t.alpha_milli;
+        }
         *out = cpx_tune_entry{decade, t.alpha_milli, t.lbits, on ? t.threads : 0, t.offload, t.ms};
     });
 }
@@ -342,6 +347,7 @@ int cpx_tune_clear(cpx_ctx *ctx)
         ctx->tuned = false;
         ctx->batch_tune = TuneEntry{};
         ctx->batch_tuned = false;
+        for (uint32_t &a : ctx->batch_alpha_dec) a = 0;
     });
 }
 

@@ -184,7 +184,15 @@ void tune_save(const cpx_ctx *ctx, const char *path)
     if (ctx->tuned)
         for (uint32_t e = 0; e < kTuneDecades; e++)
             if (ctx->tune[e].threads) put_entry(f, first, e, ctx->tune[e]);
-    if (ctx->batch_tuned) put_entry(f, first, kBatchEntry, ctx->batch_tune);
+    if (ctx->batch_tuned) {
+        put_entry(f, first, kBatchEntry, ctx->batch_tune);
+        for (uint32_t e = 0; e < kTuneDecades; e++)
+            if (ctx->batch_alpha_dec[e]) {
+                TuneEntry t = ctx->batch_tune;
+                t.alpha_milli = ctx->batch_alpha_dec[e];
+                put_entry(f, first, kBatchDecade0 + e, t);
+            }
+    }
     fprintf(f, "\n]}\n");
     fclose(f);
 }
@@ -195,6 +203,7 @@ void tune_load(cpx_ctx *ctx, const char *path)
     FILE *f = fopen(path, "r");
     if (!f) fail(CPX_EINVAL, std::string("cannot read ") + path);
     TuneEntry tab[kTuneDecades] = {}, batch = {};
+    uint32_t bdec[kTuneDecades] = {};
     bool any = false, have_batch = false, fmt = false;
     char line[512];
     while (fgets(line, sizeof line, f)) {
@@ -207,7 +216,8 @@ void tune_load(cpx_ctx *ctx, const char *path)
                    "\"decade\": %u, \"alpha_scale_milli\": %u, \"log2_bits\": %u, \"threads\": %u, "
                    "\"offload_min\": %u, \"ms\": %lf",
                    &e, &am, &lb, &th, &off, &ms) != 6 ||
-            (e >= kTuneDecades && e != kBatchEntry) || (th != 128 && th != 256 && th != 512 && th != 1024) ||
+            (e >= kTuneDecades && e != kBatchEntry && (e < kBatchDecade0 || e >= kBatchDecade0 + kTuneDecades)) ||
+            (th != 128 && th != 256 && th != 512 && th != 1024) ||
             (lb && (lb < 15 || lb > 20))) {
             fclose(f);
             fail(CPX_EINVAL, std::string("malformed tuning entry in ") + path);
@@ -216,6 +226,8 @@ void tune_load(cpx_ctx *ctx, const char *path)
         if (e == kBatchEntry) {
             batch = t;
             have_batch = true;
+        } else if (e >= kBatchDecade0) {
+            bdec[e - kBatchDecade0] = am;
         } else {
             tab[e] = t;
             any = true;
@@ -227,6 +239,7 @@ void tune_load(cpx_ctx *ctx, const char *path)
     ctx->tuned = any;
     ctx->batch_tune = batch;
     ctx->batch_tuned = have_batch;
+    for (uint32_t e = 0; e < kTuneDecades; e++) ctx->batch_alpha_dec[e] = have_batch ? bdec[e] : 0;
 }
 
 }  // namespace cpx

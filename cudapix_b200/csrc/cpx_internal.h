@@ -74,6 +74,7 @@ struct TuneEntry {
 };
 constexpr uint32_t kTuneDecades = 40;
 constexpr uint32_t kBatchEntry = 99;  // decade number of the batch entry in the JSON file
+constexpr uint32_t kBatchDecade0 = 100;  // entries 100 + e: the batch alpha scale of the queries of decade e
 
 struct Timer {
     cudaEvent_t a = nullptr, b = nullptr;
@@ -121,6 +122,9 @@ struct cpx_ctx {
     bool tuned = false;
     cpx::TuneEntry batch_tune = {};               // larger batches
     bool batch_tuned = false;
+    // alpha scale of a batch's queries by decade of x (0: the batch entry's);
+    // the tuning file's entries 100 + e
+    uint32_t batch_alpha_dec[cpx::kTuneDecades] = {};
     // kernel timing (CUDA events around the hard-leaf sieve)
     bool timing = false;
     cudaEvent_t ev_hard0 = nullptr, ev_hard1 = nullptr;

@@ -247,8 +247,12 @@ static uint32_t choose_shared(cpx_ctx *ctx, const std::vector<QD> &qd, const std
 // sample batch) pays off for queries that share their sieve with others; a
 // query with fewer than 16 companions within half a decade of x sieves
 // mostly alone and takes its decade's tuned scale (the reference alpha when
-// untuned).
-static std::vector<uint32_t> batch_alpha_scales(const u128 *xs, uint32_t Q, uint32_t batch_sc, const TuneEntry *tune)
+// untuned).  Larger x share less (their easy leaves, which no query shares,
+// grow as pi(y)^2), so a decade may carry a batch scale of its own (bdec):
+// on the B200, batches of 64 queries in [1e16, 1e17) and [1e17, 1e18) ran
+// fastest at 1/4 and 1/2 of the reference alpha, against 1/8 below 1e16.
+static std::vector<uint32_t> batch_alpha_scales(const u128 *xs, uint32_t Q, uint32_t batch_sc, const TuneEntry *tune,
+                                                const uint32_t *bdec)
 {
     std::vector<std::pair<double, uint32_t>> lx(Q);
     for (uint32_t i = 0; i < Q; i++) lx[i] = {std::log10((double)xs[i]), i};
@@ -259,6 +263,10 @@ static std::vector<uint32_t> batch_alpha_scales(const u128 *xs, uint32_t Q, uint
         while (lx[k].first - lx[a].first > 0.5) a++;
         while (b < Q && lx[b].first - lx[k].first <= 0.5) b++;
         uint32_t v = batch_sc;
+        {
+            const uint32_t e = decade_of(xs[lx[k].second]);
+            if (bdec && e < kTuneDecades && bdec[e]) v = bdec[e];  // the batch scale of the decade
+        }
         if (b - a < 17) {
             const uint32_t e = decade_of(xs[lx[k].second]);
             v = (tune && e < kTuneDecades && tune[e].alpha_milli) ? tune[e].alpha_milli : 1000;
@@ -601,7 +609,8 @@ replan:  // again without the batch alpha when its shared sieve would not fit (b
         r2.p2_table_limit = ctx->p2_table_limit;
         r2.tune = tune;
         if (batch_alpha) {
-            ascale = batch_alpha_scales(rq.xs, Q, btune->alpha_milli, ctx->tuned ? ctx->tune : nullptr);
+            ascale = batch_alpha_scales(rq.xs, Q, btune->alpha_milli, ctx->tuned ? ctx->tune : nullptr,
+                                        ctx->batch_alpha_dec);
             r2.alpha_scales = ascale.data();
         }
         compute_needs(r2, qd, need, wide);

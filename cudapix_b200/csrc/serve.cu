@@ -148,6 +148,14 @@ static void run_lane(cpx_server *S, size_t li)
                 S->cv_work.notify_all();
                 continue;
             }
+            // batch window: under load (another lane busy) wait for a fuller batch
+            if (S->busy > 0 && S->cfg.fill_target > 1 && S->pending.size() < S->cfg.fill_target) {
+                const auto deadline = S->pending.front().t_arrive + std::chrono::microseconds(S->cfg.window_us);
+                S->cv_work.wait_until(lk, deadline, [&] {
+                    return S->stop || S->growing || S->busy == 0 || S->pending.size() >= S->cfg.fill_target;
+                });
+                if (S->pending.empty() || S->growing) continue;
+            }
             uint64_t foot = 0;
             while (!S->pending.empty() && batch.size() < S->cfg.max_batch) {
                 const Req &r = S->pending.front();
@@ -268,7 +276,7 @@ static uint64_t submit(cpx_server *S, u128 x, Clock::time_point t)
     r.ticket = S->next_ticket++;
     S->pending.push_back(r);
     S->st.submitted++;
-    S->cv_work.notify_one();
+    S->cv_work.notify_all();  // a lane in its batch window counts the arrivals
     return r.ticket;
 }
 
@@ -340,6 +348,8 @@ int cpx_serve_create(cpx_ctx *ctx, const cpx_serve_config *cfg, cpx_server **out
         if (!S->cfg.lanes) S->cfg.lanes = 4;
         if (!S->cfg.max_batch) S->cfg.max_batch = 4096;
         if (!(S->cfg.admit_fraction > 0.0)) S->cfg.admit_fraction = 0.5;
+        if (!S->cfg.fill_target) S->cfg.fill_target = 64;
+        if (!S->cfg.window_us) S->cfg.window_us = 5000;
         if (S->cfg.lanes > 16) fail(CPX_EINVAL, "lanes must be in 1..16");
         if (S->cfg.admit_fraction > 0.95) fail(CPX_EINVAL, "admit_fraction must be in (0, 0.95]");
         if (S->cfg.params.flags & ~(CPX_BATCH_WIDE | CPX_BATCH_GRAPH)) fail(CPX_EINVAL, "unknown cpx_params flag");

@@ -354,6 +354,13 @@ typedef struct {
     double admit_fraction;  /* share of free HBM for batch buffers, (0, 0.95]; 0 = 0.5 */
     cpx_u128 reserve_x;     /* grow the tables for x up to this at creation (0: on demand) */
     cpx_params params;      /* y rule, c, hard-leaf tuning, CPX_BATCH_* flags */
+    /* Batch window: a lane that frees up while other lanes still run batches
+     * waits until fill_target requests are pending, or until the oldest has
+     * waited window_us, so that requests arriving under load share a batch
+     * (and its hard-leaf sieve); with every lane idle it starts at once.
+     * fill_target 0 = 64; window_us 0 = 5000; fill_target 1 = no window. */
+    uint32_t fill_target;
+    uint32_t window_us;
 } cpx_serve_config;
 typedef struct {
     uint64_t submitted, completed, failed, pending;
