@@ -236,6 +236,29 @@ __device__ __forceinline__ uint64_t cpx_pi_quot40(const cpx_pient *__restrict__ 
     return 1 + e.y + (uint64_t)__popcll(e.x << (63 - j));
 }
 
+// floor(n / d) for n < 2^53 and a quotient below 2^44, d < 2^32, nd = n as a
+// double: the reciprocal rounded to nearest (relative error 2^-24) and one
+// Newton-Raphson step give an error below 2^-46, so trunc(n rd) is within 1
+// of the quotient; the remainder's sign and size fix it without a branch.
+// The easy leaves of x >= 2^64 (x/p < 2^53 for p > x^(1/4) when x < 2^106).
+__device__ __forceinline__ uint64_t cpx_quot53(uint64_t n, double nd, uint32_t d)
+{
+    const double r = (double)__frcp_rn(__uint2float_rn(d));
+    const double rd = __fma_rn(r, __fma_rn(-(double)d, r, 1.0), r);
+    const uint64_t u = __double2ull_rz(__dmul_rn(nd, rd));
+    const int64_t rem = (int64_t)(n - u * d);
+    return u + (rem >= (int64_t)d) - (rem < 0);
+}
+
+// pi(u) for 2 <= u from the compressed table, without the small-u test
+__device__ __forceinline__ uint64_t cpx_pi_ge2(const cpx_pient *__restrict__ T, uint64_t u)
+{
+    const uint64_t m = u - 1;
+    const ulonglong2 e = __ldg(reinterpret_cast<const ulonglong2 *>(T) + (m >> 7));
+    const uint32_t j = ((uint32_t)m & 127u) >> 1;
+    return 1 + e.y + (uint64_t)__popcll(e.x << (63 - j));
+}
+
 // ------------------------------------------------ 128-bit atomic accumulate
 // Two 64-bit atomics; the carry out of the low word is added to the high word
 // by the same thread, which makes the final 128-bit total exact in any order.

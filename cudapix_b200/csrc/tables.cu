@@ -168,8 +168,9 @@ __device__ __forceinline__ uint32_t first_odd_multiple_idx(uint64_t lo, uint64_t
                                                             bool from_square)
 {
     // bit index of the first odd multiple m of p with m >= lo + 1 (and, for
-    // prime sieving, m >= p^2); 0xFFFFFFFF if none below hi.
-    uint64_t r = (lo + 1) % p;
+    // prime sieving, m >= p^2); 0xFFFFFFFF if none below hi.  (lo + 1) mod p
+    // by the reciprocal quotient (p < 2^32), not the 64-bit division routine
+    uint64_t r = (lo + 1) - cpx_udiv_leaf(lo + 1, p) * p;
     uint64_t m = lo + 1 + (r ? p - r : 0);
     if ((m & 1) == 0) m += p;
     if (from_square && m < p * p) m = p * p;

@@ -389,11 +389,15 @@ __global__ void __launch_bounds__(kThreads) k_easy(const QD *__restrict__ qd, ui
             const uint64_t w_end = min(w_beg + kEasyChunk, ((e.q1 - 1) >> 7) + 1);
             uint64_t ps = 0, cnt = 0;
             uint32_t nbuf = 0;
-            // x < 2^64 and x/p < 2^40: every quotient below 2^32, taken by cpx_pi_quot40
+            // x < 2^64 and x/p < 2^40: every quotient below 2^32, taken by
+            // cpx_pi_quot40; else x/p < 2^53 and x/p^2 < 2^44 (q > p): cpx_quot53
             const bool fast = sizeof(XT) == 8 && (uint64_t)xp < (1ull << 40);
+            const bool fast53 = !fast && xp < ((XT)1 << 53) && ((uint64_t)xp >> 44) < e.qlo;
             const double xpd = (double)(uint64_t)xp;
             auto leaf = [&](uint32_t q) -> uint64_t {
-                return fast ? cpx_pi_quot40(T, (uint64_t)xp, xpd, q) : cpx_pi_dev(T, (uint64_t)cpx_qdiv(xp, (uint64_t)q));
+                if (fast) return cpx_pi_quot40(T, (uint64_t)xp, xpd, q);
+                if (fast53) return cpx_pi_ge2(T, cpx_quot53((uint64_t)xp, xpd, q));
+                return cpx_pi_dev(T, (uint64_t)cpx_qdiv(xp, (uint64_t)q));
             };
             auto flush = [&] {
                 __syncwarp();
