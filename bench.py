@@ -120,7 +120,7 @@ def peaks():
         return 6650.0, "fallback"
 
 
-PROFILE = os.path.join(ROOT, "profiles", "k_hard_shared_batch4096.json")
+PROFILES = {k: os.path.join(ROOT, "profiles", f"{k}_batch4096.json") for k in ("k_hard_shared", "k_easy")}
 
 
 def source_sha(files):
@@ -134,12 +134,12 @@ def source_sha(files):
     return h.hexdigest()[:16]
 
 
-def kernel_profile():
-    """Per-launch counters of k_hard_shared on this workload from the committed
-    ncu capture (profiles/k_hard_shared_batch4096.json), and whether the
-    capture was taken of the current kernel source."""
+def kernel_profile(name):
+    """Per-launch counters of one of the batch's two dominant kernels on this
+    workload from its committed ncu capture (profiles/<kernel>_batch4096.json),
+    and whether the capture was taken of the current kernel source."""
     try:
-        with open(PROFILE) as f:
+        with open(PROFILES[name]) as f:
             pr = json.load(f)
         pr["matches_source"] = source_sha(pr["source_files"]) == pr["source_sha"]
         return pr
@@ -163,46 +163,56 @@ ISSUE_PER_CLK = 4  # warp instructions an SM issues per clock (4 schedulers)
 
 
 def roofline(kern, hard_ms, hard_bytes, dev_ms, clocks, ctx):
-    """Roofline of the dominant kernel, k_hard_shared (the batch-shared
-    special-leaf phi sieve), which is bound by the integer ALU pipe.
+    """Roofline of the batch's dominant kernel (k_easy or k_hard_shared,
+    whichever took longer in the timed steps), both bound by the integer ALU
+    pipe; the other one beside it.
 
     achieved = ALU-pipe warp instructions of one launch (ncu, the committed
-    capture of this workload; `matches_source` says whether it was taken of
-    the current kernel source) / the launch's duration, measured live with
-    CUDA events on the context stream; peak = the ALU pipe's issue rate per
-    SM per clock (ncu's peak_sustained) x SMs x the median SM clock sampled
-    during the timed steps.  Beside it: all issued instructions against 4
-    per SM per clock, and the S2 rate (segment-bitmap bytes the sieve passes
-    over, one pass per level per segment, / duration of the hard-leaf
-    kernels) against the shared-memory bandwidth 128 B per SM per clock."""
-    pr = kernel_profile()
-    ks = statistics.median(k.get("k_hard_shared", 0.0) for k in kern) / 1000.0
+    capture of this workload; `profile_matches_source` says whether it was
+    taken of the current kernel source) / the launch's duration, measured
+    live with CUDA events on the context stream; peak = the ALU pipe's issue
+    rate per SM per clock (2, ncu's peak_sustained) x SMs x the median SM
+    clock sampled during the timed steps.  Beside it: all issued
+    instructions against 4 per SM per clock, and for the phi sieve the S2
+    rate (segment-bitmap bytes it passes over, one pass per level per
+    segment, / duration of the hard-leaf kernels) against the shared-memory
+    bandwidth 128 B per SM per clock."""
     mhz = clocks.get("sm_mhz") or 1965.0
     sms = ctx.sm_count()
+
+    def one(name, what):
+        ks = statistics.median(k.get(name, 0.0) for k in kern) / 1000.0
+        pr = kernel_profile(name)
+        r = {"bound": "alu", "kernel": f"{name} ({what})", "unit": "Ginst/s", "achieved": None, "peak": None,
+             "frac": None, "kernel_ms": ks * 1000.0, "traffic": None,
+             "peak_kind": f"derived: ALU-pipe warp instructions per SM per clock (ncu peak_sustained) x {sms} SMs "
+                          f"x {mhz:.0f} MHz (median sampled SM clock), of measured clocks",
+             "profile": os.path.relpath(PROFILES[name], ROOT), "profile_matches_source": None}
+        if pr and ks:
+            r["achieved"] = pr["alu_warp_inst_per_launch"] / ks / 1e9
+            r["peak"] = pr["alu_peak_warp_inst_per_sm_clk"] * sms * mhz * 1e6 / 1e9
+            r["frac"] = r["achieved"] / r["peak"]
+            r["traffic"] = pr["dram_bytes_per_launch"]
+            r["profile_matches_source"] = pr["matches_source"]
+            issue_peak = ISSUE_PER_CLK * sms * mhz * 1e6 / 1e9
+            r["issue_view"] = {"achieved": pr["warp_inst_per_launch"] / ks / 1e9, "peak": issue_peak,
+                               "unit": "Ginst/s", "frac": pr["warp_inst_per_launch"] / ks / 1e9 / issue_peak}
+        return r
+
+    rows = {"k_hard_shared": one("k_hard_shared", "batch-shared special-leaf phi sieve"),
+            "k_easy": one("k_easy", "easy special leaves, one quotient and one pi-table gather each")}
     hs = statistics.median(hard_ms) / 1000.0
     hb = hard_bytes[-1]
     smem_peak = sms * SMEM_BYTES_PER_CLK * mhz * 1e6 / 1e9
     s2 = (hb / hs) / 1e9 if hs else None
-    roof = {"bound": "alu", "kernel": "k_hard_shared (batch-shared special-leaf phi sieve)", "unit": "Ginst/s",
-            "achieved": None, "peak": None, "frac": None, "kernel_ms": ks * 1000.0, "traffic": None,
-            "peak_kind": f"derived: ALU-pipe warp instructions per SM per clock (ncu peak_sustained) x {sms} SMs x "
-                         f"{mhz:.0f} MHz (median sampled SM clock)",
-            "profile": os.path.relpath(PROFILE, ROOT), "profile_matches_source": None}
-    if pr and ks:
-        alu = pr["alu_warp_inst_per_launch"]
-        roof["achieved"] = alu / ks / 1e9
-        roof["peak"] = pr["alu_peak_warp_inst_per_sm_clk"] * sms * mhz * 1e6 / 1e9
-        roof["frac"] = roof["achieved"] / roof["peak"]
-        roof["traffic"] = pr["dram_bytes_per_launch"]
-        roof["profile_matches_source"] = pr["matches_source"]
-        issue_peak = ISSUE_PER_CLK * sms * mhz * 1e6 / 1e9
-        roof["issue_view"] = {"achieved": pr["warp_inst_per_launch"] / ks / 1e9, "peak": issue_peak,
-                              "unit": "Ginst/s", "frac": pr["warp_inst_per_launch"] / ks / 1e9 / issue_peak}
-    roof["smem_view"] = {"achieved": s2, "peak": smem_peak, "unit": "GB/s", "frac": s2 / smem_peak if s2 else None,
-                         "peak_kind": f"derived: {SMEM_BYTES_PER_CLK} B per SM per clock x {sms} SMs x {mhz:.0f} MHz",
-                         "what": "S2 bytes (one pass over the segment bitmap per level per segment) / hard-leaf "
-                                 "kernels' time; the kernel keeps chunk counters instead of sweeping, so this "
-                                 "counts work it does not do"}
+    rows["k_hard_shared"]["smem_view"] = {
+        "achieved": s2, "peak": smem_peak, "unit": "GB/s", "frac": s2 / smem_peak if s2 else None,
+        "peak_kind": f"derived: {SMEM_BYTES_PER_CLK} B per SM per clock x {sms} SMs x {mhz:.0f} MHz",
+        "what": "S2 bytes (one pass over the segment bitmap per level per segment) / hard-leaf kernels' time; "
+                "the kernel keeps chunk counters instead of sweeping, so this counts work it does not do"}
+    main = max(rows, key=lambda n: rows[n]["kernel_ms"])
+    roof = dict(rows[main])
+    roof["other"] = rows["k_easy" if main == "k_hard_shared" else "k_hard_shared"]
     tot = statistics.median(dev_ms)
     names = sorted({n for k in kern for n in k})
     shares = {n: {"ms": statistics.median(k.get(n, 0.0) for k in kern),
@@ -578,7 +588,7 @@ def main():
         "plain": plain,
         "batched_over_plain": (value / plain["value"]) if plain else None,
         "e2e_over_plain": ((nq / t_e2e) / plain["value"]) if plain else None,
-        "s2_gbs": roof["smem_view"]["achieved"],
+        "s2_gbs": (hard_bytes[-1] / (statistics.median(hard_ms) / 1000.0)) / 1e9 if statistics.median(hard_ms) else None,
         "kernel_ms": shares,
         "roofline": roof,
         "cpu_baseline": cpu,

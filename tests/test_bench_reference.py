@@ -31,3 +31,38 @@ def test_reference_arm_json_line():
         queries = 4096
 
     assert line["config"] == bench.arm_config(A, 1)
+
+
+def test_reference_arm_loads_no_product_library():
+    """The CPU arms take alpha(x) from the oracle: the product library is never
+    mapped into the reference arm's process."""
+    code = ("import sys, runpy; sys.argv = ['bench.py', '--impl', 'reference', '--steps', '1', '--warmup', '1', "
+            "'--ref-step-s', '0.5']; runpy.run_path('bench.py', run_name='__main__'); "
+            "maps = open('/proc/self/maps').read(); "
+            "assert 'libcudapix_b200' not in maps, 'product library loaded'; print('NOLIB')")
+    r = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True, timeout=300, cwd=ROOT)
+    assert r.returncode == 0, r.stderr[-2000:]
+    assert "NOLIB" in r.stdout
+
+
+def test_roofline_from_profiles_and_live_spans():
+    """The roofline object: the dominant kernel by live CUDA-event time, ALU
+    instructions of one launch from its committed ncu profile over the live
+    duration, against 2 ALU warp instructions per SM per clock at the sampled
+    clock; both committed profiles were taken of the current kernel sources."""
+    sys.path.insert(0, ROOT)
+    import bench
+
+    class Ctx:
+        def sm_count(self):
+            return 148
+
+    kern = [{"k_easy": 42.0, "k_hard_shared": 38.0, "k_p2": 4.0}] * 3
+    roof, shares = bench.roofline(kern, [40.0] * 3, [1e11] * 3, [85.0] * 3, {"sm_mhz": 1965.0}, Ctx())
+    assert roof["bound"] == "alu" and roof["kernel"].startswith("k_easy")
+    assert roof["other"]["kernel"].startswith("k_hard_shared")
+    for r in (roof, roof["other"]):
+        assert r["profile_matches_source"] is True, r["profile"]
+        assert 0.3 < r["frac"] < 1.0
+        assert abs(r["peak"] - 2.0 * 148 * 1965e6 / 1e9) < 1e-6
+    assert abs(shares["k_easy"]["share"] - 42.0 / 85.0) < 1e-9
