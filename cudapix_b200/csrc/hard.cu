@@ -109,23 +109,26 @@ __global__ void __launch_bounds__(512, 2) k_hard(const QD *__restrict__ qd, uint
         if (lane < nl) level_params<XT>(lv, x, y, P[gb + lane - 1], lo_w, hi_w, bd_lo, bd_hi);
         const uint32_t lp = lv.p, lmlo = lv.mlo, lmhi = lv.mhi, lr0 = lv.r0, li0 = lv.i0;
         const XT lxp = lv.xp;
+        // levels of the block with candidates in the sub-segment (most levels of
+        // the high segments have none: they only cross off)
+        const unsigned act = __ballot_sync(FULL, lane < nl && lv.mhi > lv.mlo);
         LvlOut mine = {0, 0, 0xFFFFFFFFu, 0};
         for (uint32_t k = 0; k < nl; k++) {
             const uint32_t b = gb + k;
             const uint32_t p = __shfl_sync(FULL, lp, k);
-            const uint32_t mlo = __shfl_sync(FULL, lmlo, k), mhi = __shfl_sync(FULL, lmhi, k);
-            XT xp;
-            if (sizeof(XT) == 8) {
-                xp = (XT)__shfl_sync(FULL, (unsigned long long)lxp, k);
-            } else {
-                const unsigned long long a0 = __shfl_sync(FULL, (unsigned long long)lxp, k);
-                const unsigned long long a1 = __shfl_sync(FULL, (unsigned long long)((u128)lxp >> 64), k);
-                xp = (XT)(((u128)a1 << 64) | a0);
-            }
             const uint32_t cnt_b = tot;
             int32_t ms_b = 0;
             uint32_t job_b = 0xFFFFFFFFu;
-            if (mhi > mlo) {
+            if ((act >> k) & 1u) {
+                const uint32_t mlo = __shfl_sync(FULL, lmlo, k), mhi = __shfl_sync(FULL, lmhi, k);
+                XT xp;
+                if (sizeof(XT) == 8) {
+                    xp = (XT)__shfl_sync(FULL, (unsigned long long)lxp, k);
+                } else {
+                    const unsigned long long a0 = __shfl_sync(FULL, (unsigned long long)lxp, k);
+                    const unsigned long long a1 = __shfl_sync(FULL, (unsigned long long)((u128)lxp >> 64), k);
+                    xp = (XT)(((u128)a1 << 64) | a0);
+                }
                 // lane prefixes of the sub-segment from the chunk counters
                 const uint32_t run = counter_sum(cnt8 + c0, CPT);
                 uint32_t inc = run;
