@@ -448,11 +448,21 @@ __global__ void __launch_bounds__(kThreads) k_easy(const QD *__restrict__ qd, ui
             const uint64_t j = r - e.nsp;
             const uint64_t k0 = e.klo + 1 + j * kEasyClu, k1 = min(e.khi, e.klo + (j + 1) * kEasyClu);
             uint64_t ps = 0;
-            for (uint64_t k = k0 + lane; k <= k1; k += 32) {
-                uint64_t v = (uint64_t)cpx_qdiv(xp, (uint64_t)__ldg(P + k - 1));
+            // x/(p p_k) <= qhi < 2^31 for k > klo: cpx_quot40 when x < 2^64 and
+            // x/p < 2^40, cpx_quot53 when x/p < 2^53, else cpx_qdiv
+            const bool f40 = sizeof(XT) == 8 && (uint64_t)xp < (1ull << 40);
+            const bool f53 = !f40 && xp < ((XT)1 << 53);
+            const double xpd = (double)(uint64_t)xp;
+            auto g = [&](uint64_t k) -> uint64_t {
+                const uint32_t pk = __ldg(P + k - 1);
+                uint64_t v = f40 ? cpx_quot40((uint64_t)xp, xpd, pk)
+                                 : (f53 ? cpx_quot53((uint64_t)xp, xpd, pk) : (uint64_t)cpx_qdiv(xp, (uint64_t)pk));
                 v = v < e.q1 ? e.q1 : (v > e.qhi ? e.qhi : v);
-                ps += cpx_pi_dev(T, v);
-            }
+                return cpx_pi_ge2(T, v);
+            };
+            uint64_t k = k0 + lane;
+            for (; k + 32 <= k1; k += 64) ps += g(k) + g(k + 32);
+            if (k <= k1) ps += g(k);
             i128 add = (i128)ps;
             if (j == 0 && lane == 0)
                 add += ((i128)e.klo - (i128)b + 2) * (i128)cpx_pi_dev(T, e.qhi) -
