@@ -283,9 +283,10 @@ __device__ __forceinline__ uint32_t cross_off(uint32_t *bm, uint8_t *cnt8, uint3
         }
     } else if (i0 != 0xFFFFFFFFu) {
         // p >= 128: the lanes of one step clear bits p apart, so they touch
-        // distinct words and distinct chunk counters (plain read-modify-write)
-        for (uint64_t i = (uint64_t)i0 + (uint64_t)lane * p; i < Lw; i += 32ull * p) {
-            const uint32_t w = (uint32_t)(i >> 5), bit = 1u << (i & 31);
+        // distinct words and distinct chunk counters (plain read-modify-write).
+        // Bit indices stay in 32 bits while i0 + 32 p does (Lw <= 2^20).
+        auto clear = [&](uint32_t i) {
+            const uint32_t w = i >> 5, bit = 1u << (i & 31);
             const uint32_t ch = base_ch + (w >> 2);
             uint32_t *pw = bm + ((swz(ch, s) << 2) | (w & 3));
             const uint32_t old = *pw;
@@ -294,6 +295,11 @@ __device__ __forceinline__ uint32_t cross_off(uint32_t *bm, uint8_t *cnt8, uint3
                 cleared++;
                 cnt8[ch] = (uint8_t)(cnt8[ch] - 1);
             }
+        };
+        if (p < (1u << 26)) {
+            for (uint32_t i = i0 + lane * p; i < Lw; i += 32u * p) clear(i);
+        } else {
+            for (uint64_t i = (uint64_t)i0 + (uint64_t)lane * p; i < Lw; i += 32ull * p) clear((uint32_t)i);
         }
     }
     return cleared;
