@@ -11,6 +11,7 @@
 // Layout in HBM (see cpx_int.cuh): the pi table is one 16-byte entry per 128
 // integers {64-bit odd-number bitmap, odd primes below the entry}, so pi(n)
 // costs one 16-byte load and a popcount, and a table to N takes N/8 bytes.
+#include <mutex>
 #include <algorithm>
 
 #include "cpx_internal.h"
@@ -178,21 +179,29 @@ __device__ __forceinline__ uint32_t first_odd_multiple_idx(uint64_t lo, uint64_t
     return (uint32_t)((m - lo - 1) >> 1);
 }
 
-__global__ void __launch_bounds__(kThreads) k_sieve_table(uint64_t w0, const uint32_t *__restrict__ sp,
-                                                          uint32_t nsp, uint32_t ncoop,
-                                                          cpx_pient *__restrict__ T,
-                                                          uint64_t *__restrict__ segtot)
+// One CTA sieves MUL table blocks of kTabSegWords entries (2^18 odd numbers
+// each) with MUL x 256 threads and writes, per block, its entries (prefix
+// relative to the block) and its total.  A CTA pays the start offset of every
+// sieving prime once for all its numbers, so MUL = 4 (2^20 odd numbers, 128 KB
+// of dynamic shared memory) spreads that cost over four times the numbers
+// for the large windows of P2 beyond the resident table.
+template <int MUL>
+__global__ void __launch_bounds__(kThreads * MUL) k_sieve_table(uint64_t w0, const uint32_t *__restrict__ sp,
+                                                                uint32_t nsp, uint32_t ncoop,
+                                                                cpx_pient *__restrict__ T,
+                                                                uint64_t *__restrict__ segtot)
 {
-    constexpr uint32_t NW32 = kTabSegWords * 2;  // 8192 words = 2^18 bits
+    constexpr uint32_t NT = kThreads * MUL;
+    constexpr uint32_t NW32 = kTabSegWords * 2 * MUL;  // 8192 MUL words = 2^18 MUL bits
     constexpr uint32_t NBITS = NW32 * 32;
-    __shared__ uint32_t bm[NW32];
+    extern __shared__ uint32_t bm[];  // NW32 words
     __shared__ uint32_t off[kCoopMax];
     __shared__ uint32_t pat[160];
     __shared__ uint32_t lomod[kSmallCnt];
-    __shared__ uint64_t wsum[kThreads / 32];
+    __shared__ uint64_t wsum[NT / 32];
     const uint32_t tid = threadIdx.x;
-    const uint64_t wbase = w0 + (uint64_t)blockIdx.x * kTabSegWords;
-    const uint64_t lo = wbase * 128, hi = lo + kTabSegNumbers;
+    const uint64_t wbase = w0 + (uint64_t)blockIdx.x * kTabSegWords * MUL;
+    const uint64_t lo = wbase * 128, hi = lo + kTabSegNumbers * MUL;
 
     // residue masks: pat[o_p + r] = bits k < 32 with (r + 2k) % p == 0
     if (tid < 158) {
@@ -204,7 +213,7 @@ __global__ void __launch_bounds__(kThreads) k_sieve_table(uint64_t w0, const uin
         pat[tid] = m;
     }
     if (tid < kSmallCnt) lomod[tid] = (uint32_t)((lo + 1) % c_small[tid]);
-    for (uint32_t k = tid; k < ncoop; k += kThreads)
+    for (uint32_t k = tid; k < ncoop; k += NT)
         off[k] = first_odd_multiple_idx(lo, hi, sp[k], true);
     __syncthreads();
 
@@ -215,11 +224,11 @@ __global__ void __launch_bounds__(kThreads) k_sieve_table(uint64_t w0, const uin
         for (int i = 0; i < kSmallCnt; i++) {
             const uint32_t p = c_small[i];
             r[i] = (lomod[i] + (64u * tid) % p) % p;
-            step[i] = (64u * kThreads) % p;
+            step[i] = (64u * NT) % p;
             base[i] = o;
             o += p;
         }
-        for (uint32_t w = tid; w < NW32; w += kThreads) {
+        for (uint32_t w = tid; w < NW32; w += NT) {
             uint32_t m = 0;
 #pragma unroll
             for (int i = 0; i < kSmallCnt; i++) {
@@ -236,9 +245,9 @@ __global__ void __launch_bounds__(kThreads) k_sieve_table(uint64_t w0, const uin
         const uint32_t i0 = off[k];
         if (i0 == 0xFFFFFFFFu) continue;
         const uint32_t p = sp[k];
-        for (uint32_t i = i0 + tid * p; i < NBITS; i += kThreads * p) atomicAnd(&bm[i >> 5], ~(1u << (i & 31)));
+        for (uint32_t i = i0 + tid * p; i < NBITS; i += NT * p) atomicAnd(&bm[i >> 5], ~(1u << (i & 31)));
     }
-    for (uint32_t k = ncoop + tid; k < nsp; k += kThreads) {
+    for (uint32_t k = ncoop + tid; k < nsp; k += NT) {
         const uint64_t p = sp[k];
         if (p * p >= hi) break;
         uint32_t i0 = first_odd_multiple_idx(lo, hi, p, true);
@@ -256,6 +265,7 @@ __global__ void __launch_bounds__(kThreads) k_sieve_table(uint64_t w0, const uin
     __syncthreads();
 
     // per-warp popcount totals, then a warp-level scan writing {bits, prefix}
+    // with prefixes relative to the warp's table block (8 warps a block)
     const int lane = tid & 31, wi = tid >> 5;
     const uint64_t *bm64 = reinterpret_cast<const uint64_t *>(bm);
     constexpr uint32_t PER_WARP = kTabSegWords / (kThreads / 32);  // 512
@@ -265,8 +275,9 @@ __global__ void __launch_bounds__(kThreads) k_sieve_table(uint64_t w0, const uin
     for (int d = 16; d > 0; d >>= 1) s += __shfl_down_sync(0xffffffffu, s, d);
     if (lane == 0) wsum[wi] = s;
     __syncthreads();
+    const int blk = wi / (kThreads / 32);
     uint64_t run = 0;
-    for (int k = 0; k < wi; k++) run += wsum[k];
+    for (int k = blk * (kThreads / 32); k < wi; k++) run += wsum[k];
     for (uint32_t i = 0; i < PER_WARP / 32; i++) {
         const uint32_t wl = wi * PER_WARP + 32 * i + lane;
         const uint64_t b = bm64[wl];
@@ -283,10 +294,10 @@ __global__ void __launch_bounds__(kThreads) k_sieve_table(uint64_t w0, const uin
         reinterpret_cast<ulonglong2 *>(T)[wbase - w0 + wl] = e;
         run += __shfl_sync(0xffffffffu, inc, 31);
     }
-    if (tid == 0) {
+    if (tid < MUL) {
         uint64_t t = 0;
-        for (int k = 0; k < kThreads / 32; k++) t += wsum[k];
-        segtot[blockIdx.x] = t;
+        for (int k = 0; k < kThreads / 32; k++) t += wsum[tid * (kThreads / 32) + k];
+        segtot[(uint64_t)blockIdx.x * MUL + tid] = t;
     }
 }
 
@@ -353,7 +364,26 @@ uint64_t build_pitable_window(cpx_ctx *ctx, uint64_t w0, uint64_t nwords, cpx_pi
     // sieving primes P[11..] = 37, 41, ...; the kernel stops at p^2 >= segment top
     const uint32_t nsp_all = (uint32_t)(tb.prm_n > 11 ? tb.prm_n - 11 : 0);
     const uint32_t ncoop = std::min<uint32_t>(kCoopMax, nsp_all);
-    k_sieve_table<<<(unsigned)nseg, kThreads, 0, ctx->stream>>>(w0, tb.P + 11, nsp_all, ncoop, T, segtot);
+    // four table blocks a CTA when the window is large and a multiple of four blocks
+    constexpr int kMul = 4;
+    const size_t smem4 = kTabSegWords * 2 * kMul * 4;
+    if (nseg % kMul == 0 && nseg >= (uint64_t)kMul * ctx->sm_count && ctx->smem_optin >= smem4 + 8192) {
+        static std::mutex m;
+        static int done_dev = -1;
+        {
+            std::lock_guard<std::mutex> g(m);
+            if (done_dev != ctx->device) {
+                CPX_CUDA(cudaFuncSetAttribute(k_sieve_table<kMul>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                              (int)smem4));
+                done_dev = ctx->device;
+            }
+        }
+        k_sieve_table<kMul><<<(unsigned)(nseg / kMul), kThreads * kMul, smem4, ctx->stream>>>(w0, tb.P + 11, nsp_all,
+                                                                                              ncoop, T, segtot);
+    } else {
+        k_sieve_table<1><<<(unsigned)nseg, kThreads, kTabSegWords * 2 * 4, ctx->stream>>>(w0, tb.P + 11, nsp_all,
+                                                                                         ncoop, T, segtot);
+    }
     CPX_LAUNCH("k_sieve_table");
     note_launch(ctx);
     scan_u64(ctx, segtot, nseg);
