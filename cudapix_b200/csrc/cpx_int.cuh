@@ -208,20 +208,48 @@ __device__ __forceinline__ u128 cpx_qdiv(u128 n, uint64_t d)
     return cpx_udiv128_slow(n, d);
 }
 
-// floor(n / d) for n < 2^40 and d < 2^32, with nd = n as a double.  The
-// reciprocal estimate comes from the hardware approximation (relative error
-// at most 2^-22); one Newton-Raphson step in double brings it below 2^-43, so
-// trunc(n rd) is within 1 of the quotient (< 2^40), and the sign and size of
-// n - q d fix it without a branch.
-__device__ __forceinline__ uint64_t cpx_quot40(uint64_t n, double nd, uint32_t d)
+#endif  // __CUDACC__
+
+// floor(n / d) for n < 2^40 and 1 <= d < 2^32, with nd = n as a double, from
+// a reciprocal estimate r0 with |d r0 - 1| < 2^-22 (the hardware
+// approximation of 1/d rounded to float: at most 1 ulp of the approximation
+// plus the rounding of d to float).  One Newton-Raphson step with its target
+// raised by 2^-42,
+//   rd = r0 + r0 (1 + 2^-42 - d r0) = (1/d) (1 - e^2 + 2^-42 (1 + e)),  e = d r0 - 1,
+// lies in (1/d, (1/d)(1 + 2^-41.9)) after the two roundings of the fused
+// steps (e^2 < 2^-44), so t = n rd rounded toward +infinity satisfies
+// n/d <= t < n/d + 2^40 2^-41.9: trunc(t) is floor(n/d) or floor(n/d) + 1,
+// and a single comparison of q d with n settles which (q d <= n + d < 2^41).
+// QT = uint32_t when floor(n/d) < 2^32 - 1.  The host form takes r0 from its
+// caller and rounds the product up exactly (error-free product, then the
+// next double up when the rounded-to-nearest product was low).
+template <class QT> CPX_HD QT cpx_quot40_core(uint64_t n, double nd, uint32_t d, float r0)
+{
+    const double r = (double)r0;
+    const double rd = fma(r, fma(-(double)d, r, 1.0 + 0x1p-42), r);
+#if defined(__CUDA_ARCH__)
+    const double t = __dmul_ru(nd, rd);
+    QT q;
+    if constexpr (sizeof(QT) == 4) q = __double2uint_rz(t);
+    else q = __double2ull_rz(t);
+#else
+    double t = nd * rd;
+    if (std::fma(nd, rd, -t) > 0) t = std::nextafter(t, INFINITY);
+    const QT q = (QT)t;
+#endif
+    return q - (QT)((uint64_t)q * d > n);
+}
+
+#if defined(__CUDACC__)
+__device__ __forceinline__ float cpx_rcp_approx(uint32_t d)
 {
     float rf;
     asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(rf) : "f"(__uint2float_rn(d)));
-    const double r = (double)rf;
-    const double rd = __fma_rn(r, __fma_rn(-(double)d, r, 1.0), r);
-    const uint64_t u = __double2ull_rz(__dmul_rn(nd, rd));
-    const int64_t rem = (int64_t)(n - u * d);
-    return u + (rem >= (int64_t)d) - (rem < 0);
+    return rf;
+}
+__device__ __forceinline__ uint64_t cpx_quot40(uint64_t n, double nd, uint32_t d)
+{
+    return cpx_quot40_core<uint64_t>(n, nd, d, cpx_rcp_approx(d));
 }
 
 // pi(floor(n / d)) of an easy leaf whose dividend n = x/p is below 2^40 and
@@ -230,7 +258,7 @@ __device__ __forceinline__ uint64_t cpx_quot40(uint64_t n, double nd, uint32_t d
 // j = ((u - 1) mod 128) / 2.
 __device__ __forceinline__ uint64_t cpx_pi_quot40(const cpx_pient *__restrict__ T, uint64_t n, double nd, uint32_t d)
 {
-    const uint32_t m = (uint32_t)cpx_quot40(n, nd, d) - 1;
+    const uint32_t m = cpx_quot40_core<uint32_t>(n, nd, d, cpx_rcp_approx(d)) - 1;
     const ulonglong2 e = __ldg(reinterpret_cast<const ulonglong2 *>(T) + (m >> 7));
     const uint32_t j = (m & 127u) >> 1;
     return 1 + e.y + (uint64_t)__popcll(e.x << (63 - j));

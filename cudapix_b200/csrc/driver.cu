@@ -524,9 +524,9 @@ void compute_needs(const BatchReq &rq, std::vector<QD> &qd, TableNeed &need, boo
             N = std::max<uint64_t>(N, std::max<uint64_t>(r4 * r4 + 2, y + 1));
         }
         if (mask & TERM_EASY) {
-            // the p of the easy leaves (p <= icbrt(x)) and the u primes of their
-            // clustered parts (u <= min(p^2, sqrt(x/p)) <= x^(2/5))
-            Pneed = std::max<uint64_t>(Pneed, std::max<uint64_t>(cx + 1, easy_u_bound(x)));
+            // the p of the easy leaves (p <= icbrt(x)), their sparse q (q <= y) and
+            // the u primes of their clustered parts (u <= min(p^2, sqrt(x/p)) <= x^(2/5))
+            Pneed = std::max<uint64_t>(Pneed, std::max<uint64_t>(std::max(cx, y) + 1, easy_u_bound(x)));
             Y = std::max(Y, y);
         }
         if (mask == TERM_PI) N = std::max<uint64_t>(N, y + 1);

@@ -266,7 +266,9 @@ __global__ void __launch_bounds__(kThreads) k_trivial(const QD *__restrict__ qd,
 // composite m.
 //
 // Per p the q range (qlo, qhi] is split at q1 ~ sqrt(x/p).  Below q1 every q
-// gives its own u and the leaves are taken one by one (sparse part).  Above
+// gives its own u and the leaves are taken one by one (sparse part): the q
+// are the primes p_k, k in (pi(qlo), pi(q1)], read from the resident prime
+// list (which reaches y), 32 consecutive k a warp step.  Above
 // q1 runs of consecutive primes q share pi(x/(pq)) (clustered part): with
 // G(k) = pi(clamp(x/(p p_k), q1, qhi)) the primes q of the run with
 // pi(x/(pq)) = k number G(k) - G(k+1), and summation by parts turns
@@ -276,11 +278,12 @@ __global__ void __launch_bounds__(kThreads) k_trivial(const QD *__restrict__ qd,
 // table lookup per prime u instead of per leaf.  The u primes come from the
 // resident prime list, so q1 is raised until x/(p (q1 + 1)) <= prm_max.
 
-constexpr uint64_t kEasyChunk = 64;   // pi-table entries of q per sparse work chunk
-constexpr uint64_t kEasyClu = 512;    // u primes per clustered work chunk
+constexpr uint64_t kEasySparse = 2048;  // primes q per sparse work chunk
+constexpr uint64_t kEasyClu = 512;      // u primes per clustered work chunk
 
 struct EasyP {
     uint64_t qlo, qhi, q1;  // sparse q in (qlo, q1], clustered q in (q1, qhi]
+    uint64_t kq0, kq1;      // pi(qlo), pi(q1): the sparse q are p_k, kq0 < k <= kq1
     uint64_t klo, khi;      // pi(x / (p qhi)), pi(x / (p (q1 + 1)))
     uint64_t nsp, ncl;      // work chunks of the two parts
 };
@@ -304,7 +307,13 @@ __device__ __noinline__ bool easy_plan(XT x, uint64_t y, uint64_t p, uint64_t pr
     e.qlo = qlo;
     e.qhi = qhi;
     e.q1 = q1;
-    e.nsp = (q1 > qlo) ? (((q1 - 1) >> 7) - (qlo >> 7) + kEasyChunk) / kEasyChunk : 0;
+    if (q1 > qlo) {
+        e.kq0 = cpx_pi_dev(T, qlo);
+        e.kq1 = cpx_pi_dev(T, q1);
+    } else {
+        e.kq0 = e.kq1 = 0;
+    }
+    e.nsp = (e.kq1 - e.kq0 + kEasySparse - 1) / kEasySparse;
     if (qhi > q1) {
         e.klo = cpx_pi_dev(T, (uint64_t)cpx_qdiv(xp, qhi));
         e.khi = cpx_pi_dev(T, (uint64_t)cpx_qdiv(xp, q1 + 1));
@@ -338,12 +347,8 @@ __global__ void k_easy_count(const QD *__restrict__ qd, uint32_t Q, const uint64
 }
 
 // Pass 2: each warp owns a contiguous slice of chunks.  A sparse chunk is
-// kEasyChunk table entries of the q range of one p (two entries per lane); a
-// clustered chunk is kEasyClu consecutive u primes of one p.  The sparse
-// primes q of a chunk are gathered into the warp's buffer and answered 32 at
-// a time, so that a lane whose table entries hold many primes does not hold
-// up the others.
-constexpr uint32_t kEasyBuf = 512;  // gathered q per warp
+// kEasySparse consecutive primes q of one p (lane l takes k = k0 + l, k0 + l +
+// 32, ...); a clustered chunk is kEasyClu consecutive u primes of one p.
 template <class XT>
 __global__ void __launch_bounds__(kThreads) k_easy(const QD *__restrict__ qd, uint32_t Q,
                                                    const uint64_t *__restrict__ pre, uint64_t total_units,
@@ -354,8 +359,6 @@ __global__ void __launch_bounds__(kThreads) k_easy(const QD *__restrict__ qd, ui
 {
     const int lane = threadIdx.x & 31;
     const WarpSlice sl = warp_slice(off[total_units]);
-    __shared__ uint32_t s_q[kThreads / 32][kEasyBuf];
-    uint32_t *qbuf = s_q[threadIdx.x >> 5];
     LaneAcc a;
     // decoded state of the current p, kept across its consecutive chunks
     uint64_t c_unit = ~0ull, c_first = 0, c_last = 0, b = 0;
@@ -385,65 +388,33 @@ __global__ void __launch_bounds__(kThreads) k_easy(const QD *__restrict__ qd, ui
         }
         const uint64_t r = ch - c_first;
         if (r < e.nsp) {
-            const uint64_t w_beg = (e.qlo >> 7) + r * kEasyChunk;
-            const uint64_t w_end = min(w_beg + kEasyChunk, ((e.q1 - 1) >> 7) + 1);
-            uint64_t ps = 0, cnt = 0;
-            uint32_t nbuf = 0;
-            // x < 2^64 and x/p < 2^40: every quotient below 2^32, taken by
-            // cpx_pi_quot40; else x/p < 2^53 and x/p^2 < 2^44 (q > p): cpx_quot53
-            const bool fast = sizeof(XT) == 8 && (uint64_t)xp < (1ull << 40);
-            const bool fast53 = !fast && xp < ((XT)1 << 53) && ((uint64_t)xp >> 44) < e.qlo;
+            const uint64_t k0 = e.kq0 + 1 + r * kEasySparse, k1 = min(e.kq1, e.kq0 + (r + 1) * kEasySparse);
+            // x < 2^64 and x/p < 2^40: every quotient below 2^30 (u < sqrt(x) and
+            // x < 2^60 here), taken by cpx_pi_quot40; else x/p < 2^53 and x/p^2 <
+            // 2^44 (q > p): cpx_quot53; else the general quotient.  One loop per
+            // case, two leaves a lane a step (their quotients and gathers overlap).
+            const uint32_t *Pq = P + (k0 - 1);
+            const uint32_t nq = (uint32_t)(k1 - k0 + 1);
             const double xpd = (double)(uint64_t)xp;
-            auto leaf = [&](uint32_t q) -> uint64_t {
-                if (fast) return cpx_pi_quot40(T, (uint64_t)xp, xpd, q);
-                if (fast53) return cpx_pi_ge2(T, cpx_quot53((uint64_t)xp, xpd, q));
-                return cpx_pi_dev(T, (uint64_t)cpx_qdiv(xp, (uint64_t)q));
-            };
-            auto flush = [&] {
-                __syncwarp();
-                if (lane < nbuf) cnt += (nbuf - lane + 31) / 32;
-                // two leaves a lane at a time: their quotients and table gathers overlap
-                uint32_t jj = lane;
-                for (; jj + 32 < nbuf; jj += 64) {
-                    const uint32_t qa = qbuf[jj], qb2 = qbuf[jj + 32];
-                    ps += leaf(qa) + leaf(qb2);
-                }
-                if (jj < nbuf) ps += leaf(qbuf[jj]);
-                __syncwarp();
-                nbuf = 0;
-            };
-            for (uint64_t wb = w_beg; wb < w_end; wb += 32) {  // uniform over the warp
-                const uint64_t wq = wb + lane;
-                uint64_t qb = 0;
-                if (wq < w_end) qb = __ldg(reinterpret_cast<const ulonglong2 *>(T) + wq).x & range_mask(wq, e.qlo, e.q1);
-                const uint32_t nq = (uint32_t)__popcll(qb);
-                uint32_t inc = nq;
-#pragma unroll
-                for (int o = 1; o < 32; o <<= 1) {
-                    const uint32_t t = __shfl_up_sync(FULL, inc, o);
-                    if (lane >= o) inc += t;
-                }
-                const uint32_t tot = __shfl_sync(FULL, inc, 31);
-                if (tot > kEasyBuf) {  // a dense round: each lane answers its own entry
-                    while (qb) {
-                        const int j2 = __ffsll((long long)qb) - 1;
-                        qb &= qb - 1;
-                        ps += leaf((uint32_t)(128 * wq + 2 * j2 + 1));
-                        cnt++;
-                    }
-                    continue;
-                }
-                if (nbuf + tot > kEasyBuf) flush();
-                uint32_t kk = nbuf + inc - nq;
-                while (qb) {
-                    const int j2 = __ffsll((long long)qb) - 1;
-                    qb &= qb - 1;
-                    qbuf[kk++] = (uint32_t)(128 * wq + 2 * j2 + 1);
-                }
-                nbuf += tot;
+            uint64_t ps = 0;
+            uint32_t t = lane;
+            if (sizeof(XT) == 8 && (uint64_t)xp < (1ull << 40)) {
+                const uint64_t n = (uint64_t)xp;
+                for (; t + 32 < nq; t += 64)
+                    ps += cpx_pi_quot40(T, n, xpd, __ldg(Pq + t)) + cpx_pi_quot40(T, n, xpd, __ldg(Pq + t + 32));
+                if (t < nq) ps += cpx_pi_quot40(T, n, xpd, __ldg(Pq + t));
+            } else if (xp < ((XT)1 << 53) && ((uint64_t)xp >> 44) < e.qlo) {
+                const uint64_t n = (uint64_t)xp;
+                for (; t + 32 < nq; t += 64)
+                    ps += cpx_pi_ge2(T, cpx_quot53(n, xpd, __ldg(Pq + t))) +
+                          cpx_pi_ge2(T, cpx_quot53(n, xpd, __ldg(Pq + t + 32)));
+                if (t < nq) ps += cpx_pi_ge2(T, cpx_quot53(n, xpd, __ldg(Pq + t)));
+            } else {
+                for (; t < nq; t += 32) ps += cpx_pi_dev(T, (uint64_t)cpx_qdiv(xp, (uint64_t)__ldg(Pq + t)));
             }
-            flush();
-            a.v += (i128)ps + (i128)cnt * (2 - (i128)b);
+            i128 add = (i128)ps;
+            if (lane == 0) add += (i128)(k1 - k0 + 1) * (2 - (i128)b);
+            a.v += add;
         } else {
             const uint64_t j = r - e.nsp;
             const uint64_t k0 = e.klo + 1 + j * kEasyClu, k1 = min(e.khi, e.klo + (j + 1) * kEasyClu);
