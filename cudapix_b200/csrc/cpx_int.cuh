@@ -220,24 +220,40 @@ __device__ __forceinline__ u128 cpx_qdiv(u128 n, uint64_t d)
 // steps (e^2 < 2^-44), so t = n rd rounded toward +infinity satisfies
 // n/d <= t < n/d + 2^40 2^-41.9: trunc(t) is floor(n/d) or floor(n/d) + 1,
 // and a single comparison of q d with n settles which (q d <= n + d < 2^41).
-// QT = uint32_t when floor(n/d) < 2^32 - 1.  The host form takes r0 from its
-// caller and rounds the product up exactly (error-free product, then the
-// next double up when the rounded-to-nearest product was low).
-template <class QT> CPX_HD QT cpx_quot40_core(uint64_t n, double nd, uint32_t d, float r0)
+// QT = uint32_t when floor(n/d) < 2^32 - 1.  On the device d becomes a
+// double and trunc(t) an integer through the exponent 2^52 (2^52 + d is
+// exact; 2^52 + t rounded toward zero is 2^52 + trunc(t) for t < 2^52), on
+// the double pipe rather than the conversion unit.  The host form takes r0
+// from its caller and rounds the product up exactly (error-free product,
+// then the next double up when the rounded-to-nearest product was low).
+template <class QT> CPX_HD QT cpx_quot40_est(double nd, uint32_t d, float r0)
 {
     const double r = (double)r0;
-    const double rd = fma(r, fma(-(double)d, r, 1.0 + 0x1p-42), r);
 #if defined(__CUDA_ARCH__)
-    const double t = __dmul_ru(nd, rd);
-    QT q;
-    if constexpr (sizeof(QT) == 4) q = __double2uint_rz(t);
-    else q = __double2ull_rz(t);
+    const double dd = __hiloint2double(0x43300000, (int)d) - 0x1p52;
+    const double rd = fma(r, fma(-dd, r, 1.0 + 0x1p-42), r);
+    const double tt = __dadd_rz(__dmul_ru(nd, rd), 0x1p52);
+    if constexpr (sizeof(QT) == 4) return (QT)__double2loint(tt);
+    else return (QT)(__double_as_longlong(tt) & 0xFFFFFFFFFFFFFull);
 #else
+    const double rd = fma(r, fma(-(double)d, r, 1.0 + 0x1p-42), r);
     double t = nd * rd;
     if (std::fma(nd, rd, -t) > 0) t = std::nextafter(t, INFINITY);
-    const QT q = (QT)t;
+    return (QT)t;
 #endif
+}
+template <class QT> CPX_HD QT cpx_quot40_core(uint64_t n, double nd, uint32_t d, float r0)
+{
+    const QT q = cpx_quot40_est<QT>(nd, d, r0);
     return q - (QT)((uint64_t)q * d > n);
+}
+// The same quotient for d < 2^31 and floor(n/d) < 2^31 - 1, corrected in 32
+// bits: n - q d lies in [0, d) or [-d, 0), so its low 32 bits are below d
+// or at least 2^32 - d > d.
+CPX_HD uint32_t cpx_quot40_small(uint64_t n, double nd, uint32_t d, float r0)
+{
+    const uint32_t q = cpx_quot40_est<uint32_t>(nd, d, r0);
+    return q - (uint32_t)((uint32_t)n - q * d >= d);
 }
 
 #if defined(__CUDACC__)
@@ -252,13 +268,14 @@ __device__ __forceinline__ uint64_t cpx_quot40(uint64_t n, double nd, uint32_t d
     return cpx_quot40_core<uint64_t>(n, nd, d, cpx_rcp_approx(d));
 }
 
-// pi(floor(n / d)) of an easy leaf whose dividend n = x/p is below 2^40 and
-// whose quotient u is below 2^32 (u < sqrt(x) for x < 2^64), by cpx_quot40.
+// pi(floor(n / d)) of an easy leaf whose dividend n = x/p is below 2^40, with
+// d = q < 2^31 and a quotient u below 2^30 (u < sqrt(x), x < 2^60 when x/p <
+// 2^40), by cpx_quot40_small.
 // u >= 2; pi(u) = 1 + entry prefix + bits 0..j of the entry's bitmap,
 // j = ((u - 1) mod 128) / 2.
 __device__ __forceinline__ uint64_t cpx_pi_quot40(const cpx_pient *__restrict__ T, uint64_t n, double nd, uint32_t d)
 {
-    const uint32_t m = cpx_quot40_core<uint32_t>(n, nd, d, cpx_rcp_approx(d)) - 1;
+    const uint32_t m = cpx_quot40_small(n, nd, d, cpx_rcp_approx(d)) - 1;
     const ulonglong2 e = __ldg(reinterpret_cast<const ulonglong2 *>(T) + (m >> 7));
     const uint32_t j = (m & 127u) >> 1;
     return 1 + e.y + (uint64_t)__popcll(e.x << (63 - j));

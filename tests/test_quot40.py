@@ -1,8 +1,9 @@
-"""cpx_quot40_core (cudapix_b200/csrc/cpx_int.cuh), the leaf quotient
-floor(n / d) for n < 2^40 and d < 2^32 of the easy and hard leaves: its host
-form, given every reciprocal estimate the hardware approximation may return
-(the correctly rounded reciprocal of float(d) and the floats one ulp either
-side of it), against integer division on 3 x 10^7 random operands and on edge
+"""cpx_quot40_core and cpx_quot40_small (cudapix_b200/csrc/cpx_int.cuh), the
+leaf quotient floor(n / d) for n < 2^40 and d < 2^32 (d < 2^31 for the form
+corrected in 32 bits) of the easy and hard leaves: their host forms, given
+every reciprocal estimate the hardware approximation may return (the
+correctly rounded reciprocal of float(d) and the floats one ulp either side
+of it), against integer division on 3 x 10^7 random operands and on edge
 operands (exact multiples and their neighbours, divisors that do not fit a
 float, dividends near 2^40).  The host form rounds the product up exactly,
 as the device's __dmul_ru does; the device form is checked through the leaf
@@ -46,6 +47,11 @@ static void check(uint64_t n, uint64_t d)
         if (got != want && bad++ < 5)
             std::printf("MISMATCH n=%llu d=%llu k=%d got=%llu want=%llu\n", (unsigned long long)n,
                         (unsigned long long)d, k, (unsigned long long)got, (unsigned long long)want);
+        if (d < (1ull << 31) && want < 0x7FFFFFFEull) {
+            const uint32_t gs = cpx_quot40_small(n, (double)n, (uint32_t)d, r0);
+            if (gs != want && bad++ < 5)
+                std::printf("MISMATCHS n=%llu d=%llu k=%d got=%u\n", (unsigned long long)n, (unsigned long long)d, k, gs);
+        }
         if (want < 0xFFFFFFFEull) {
             const uint32_t g32 = cpx_quot40_core<uint32_t>(n, (double)n, (uint32_t)d, r0);
             if (g32 != want && bad++ < 5)
