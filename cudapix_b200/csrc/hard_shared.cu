@@ -46,6 +46,7 @@ __host__ __device__ __forceinline__ uint32_t leaf_cap(uint32_t threads) { return
 __host__ __device__ __forceinline__ size_t shared_smem(uint32_t lbits, uint32_t threads)
 {
     size_t o = counts_smem(lbits);
+    o += ((size_t(1) << lbits) / 128) * 2;         // chunk prefixes within their lane
     o += threads * 4;                              // lane prefixes
     o += (threads / 32) * leaf_cap(threads) * 8;   // gathered leaves: m, query | (mu(m) = -1) << 31
     o += (threads / 32) * kGroupMax * 16;  // x/p of the group's queries, per warp
@@ -314,6 +315,8 @@ template <class XT> __device__ __forceinline__ void hard_shared_unit(uint64_t un
     size_t o = L / 8;
     uint8_t *cnt8 = sp + o;
     o += ((L / 128) + 15) & ~size_t(15);
+    uint16_t *pre16 = reinterpret_cast<uint16_t *>(sp + o);  // chunk prefixes within their lane
+    o += (L / 128) * 2;
     uint32_t *wl = reinterpret_cast<uint32_t *>(sp + o) + 32 * warp;  // this warp's lane prefixes
     o += T * 4;
     uint2 *lbuf0 = reinterpret_cast<uint2 *>(sp + o);
@@ -349,7 +352,7 @@ template <class XT> __device__ __forceinline__ void hard_shared_unit(uint64_t un
     presieve(bm, cnt8, P, c, lo, c0, CPT, s);
     __syncwarp();
     const uint64_t w = seg * NW + warp;
-    auto sub_count = [&](uint64_t uu) -> uint32_t { return sub_survivors(uu, lo_w, wl, cnt8, bm, CPT, s, warp); };
+    auto sub_count = [&](uint64_t uu) -> uint32_t { return sub_survivors_pre(uu, lo_w, wl, pre16, bm, CPT, s, warp); };
     // the leaf quotient x/(p m): cpx_quot40 when x < 2^64 and x/p < 2^40 (xpd = x/p as a double)
     auto hq = [&](XT xv, double xvd, uint64_t m) -> uint64_t {
         if (sizeof(XT) == 8 && (uint64_t)xv < (1ull << 40)) return cpx_quot40((uint64_t)xv, xvd, (uint32_t)m);
@@ -401,9 +404,9 @@ template <class XT> __device__ __forceinline__ void hard_shared_unit(uint64_t un
             }
             const unsigned bal = __ballot_sync(FULL, act);
             if (bal) {
-                // lane prefixes of the sub-segment from the chunk counters
+                // chunk and lane prefixes of the sub-segment from the chunk counters
                 uint32_t off0;
-                warp_place(counter_sum(cnt8 + c0, CPT), lane, off0);
+                warp_place(chunk_prefixes(cnt8, pre16, c0, CPT), lane, off0);
                 wl[lane] = off0;
                 if (act) s_xp[lane] = xp;
                 __syncwarp();

@@ -353,6 +353,52 @@ __device__ __forceinline__ uint32_t sub_survivors(uint64_t uu, uint64_t lo_w, co
     return cv + chunk_survivors(reinterpret_cast<const uint4 *>(bm)[swz(ch, s)], jb);
 }
 
+// Survivor prefixes of one lane's chunks [c0, c0 + CPT): pre16[c0 + j] = the
+// counters of chunks c0 .. c0 + j - 1 (below 2^16: CPT 128 <= 2^15 bits);
+// returns the lane's total.  Built once a level that has leaves in the warp's
+// sub-segment, so that a leaf count reads one prefix instead of summing the
+// owner's counters.  CPT a multiple of 8: each counter word gives its four
+// running sums by byte-masked dp4a.
+__device__ __forceinline__ uint32_t chunk_prefixes(const uint8_t *cnt8, uint16_t *pre16, uint32_t c0, uint32_t CPT)
+{
+    uint32_t run = 0;
+    if ((CPT & 7) == 0) {
+        const uint32_t *cw = reinterpret_cast<const uint32_t *>(cnt8 + c0);
+        uint4 *pw = reinterpret_cast<uint4 *>(pre16 + c0);
+        for (uint32_t i = 0; i < (CPT >> 3); i++) {
+            const uint32_t a = cw[2 * i], b = cw[2 * i + 1];
+            uint4 o;
+            o.x = run | (__dp4a(a, 0x00000001u, run) << 16);
+            o.y = __dp4a(a, 0x00000101u, run) | (__dp4a(a, 0x00010101u, run) << 16);
+            run = __dp4a(a, 0x01010101u, run);
+            o.z = run | (__dp4a(b, 0x00000001u, run) << 16);
+            o.w = __dp4a(b, 0x00000101u, run) | (__dp4a(b, 0x00010101u, run) << 16);
+            run = __dp4a(b, 0x01010101u, run);
+            pw[i] = o;
+        }
+    } else {
+        for (uint32_t j = 0; j < CPT; j++) {
+            pre16[c0 + j] = (uint16_t)run;
+            run += cnt8[c0 + j];
+        }
+    }
+    return run;
+}
+
+// sub_survivors from the chunk prefixes of chunk_prefixes: the owner lane's
+// prefix, the chunk's prefix within the owner and the chunk's popcounts.
+__device__ __forceinline__ uint32_t sub_survivors_pre(uint64_t uu, uint64_t lo_w, const uint32_t *wl,
+                                                      const uint16_t *pre16, const uint32_t *bm, uint32_t CPT, int s,
+                                                      uint32_t warp)
+{
+    const uint32_t kk = (uint32_t)((uu - lo_w + 1) >> 1);  // bits [0, kk) of the sub-segment
+    if (!kk) return 0u;
+    const uint32_t jb = kk - 1;
+    const uint32_t chs = jb >> 7;               // chunk in the sub-segment
+    const uint32_t ch = chs + CPT * 32 * warp;  // chunk in the segment
+    return wl[chs >> s] + pre16[ch] + chunk_survivors(reinterpret_cast<const uint4 *>(bm)[swz(ch, s)], jb);
+}
+
 // B(seg) = pi(min(r4, isqrt((x - 1) / lo), isqrt(hi - 1))): the levels b a
 // segment [lo, hi) sieves for an x with iroot4(x) = r4.  p_b^2 lo < x bounds
 // the levels whose leaves can reach the segment or a later one; p_b^2 < hi
