@@ -375,7 +375,7 @@ def arm_config(args, world):
     """The workload both arms report (the reference arm runs it on the host cores)."""
     return {"workload": "batch4096: x = floor(10^e), e ~ U[9,14], numpy default_rng(0)",
             "queries": args.queries, "c": 6,
-            "alpha": "tuning table: 1/8 of the reference alpha(x) (y >= icbrt x) for queries with 16 or more "
+            "alpha": "tuning table: 0.094 of the reference alpha(x) (y >= icbrt x) for queries with 16 or more "
                      "others within half a decade of x, else the decade's tuned alpha",
             "l2": "flushed before every timed step (256 MiB write)",
             "tuning": os.path.relpath(TUNING, ROOT) if os.path.exists(TUNING) else None,

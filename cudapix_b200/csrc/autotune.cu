@@ -197,19 +197,24 @@ void tune_save(const cpx_ctx *ctx, const char *path)
     fclose(f);
 }
 
-// Reads the file tune_save writes (one entry object per line).
+// Reads the file tune_save writes (one entry object per line, though any
+// layout of the same objects reads the same: every "decade" key is parsed).
 void tune_load(cpx_ctx *ctx, const char *path)
 {
     FILE *f = fopen(path, "r");
     if (!f) fail(CPX_EINVAL, std::string("cannot read ") + path);
+    std::string text;
+    {
+        char buf[4096];
+        size_t n;
+        while ((n = fread(buf, 1, sizeof buf, f)) > 0) text.append(buf, n);
+    }
+    fclose(f);
     TuneEntry tab[kTuneDecades] = {}, batch = {};
     uint32_t bdec[kTuneDecades] = {};
-    bool any = false, have_batch = false, fmt = false;
-    char line[512];
-    while (fgets(line, sizeof line, f)) {
-        if (strstr(line, "cudapix_b200 tuning 1")) fmt = true;
-        const char *p = strstr(line, "\"decade\"");
-        if (!p) continue;
+    bool any = false, have_batch = false;
+    const bool fmt = text.find("cudapix_b200 tuning 1") != std::string::npos;
+    for (const char *p = strstr(text.c_str(), "\"decade\""); p; p = strstr(p + 1, "\"decade\"")) {
         unsigned e, am, lb, th, off;
         double ms;
         if (sscanf(p,
@@ -218,10 +223,8 @@ void tune_load(cpx_ctx *ctx, const char *path)
                    &e, &am, &lb, &th, &off, &ms) != 6 ||
             (e >= kTuneDecades && e != kBatchEntry && (e < kBatchDecade0 || e >= kBatchDecade0 + kTuneDecades)) ||
             (th != 128 && th != 256 && th != 512 && th != 1024) ||
-            (lb && (lb < 15 || lb > 20))) {
-            fclose(f);
+            (lb && (lb < 15 || lb > 20)))
             fail(CPX_EINVAL, std::string("malformed tuning entry in ") + path);
-        }
         const TuneEntry t{am, lb, th, off, (float)ms};
         if (e == kBatchEntry) {
             batch = t;
@@ -233,7 +236,6 @@ void tune_load(cpx_ctx *ctx, const char *path)
             any = true;
         }
     }
-    fclose(f);
     if (!fmt || (!any && !have_batch)) fail(CPX_EINVAL, std::string("no tuning entries in ") + path);
     for (uint32_t e = 0; e < kTuneDecades; e++) ctx->tune[e] = tab[e];
     ctx->tuned = any;

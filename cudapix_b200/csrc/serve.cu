@@ -223,9 +223,12 @@ static void run_lane(cpx_server *S, size_t li)
 
 // Admission data of one request: its table bounds and a device footprint
 // estimate (per (segment, level) outputs of the hard leaves, 8 bytes each,
-// plus the per-query records).  A lane runs a request with the per-decade
-// tuning when its batch is small and with the batch tuning otherwise (the
-// alpha, hence y and z, differ), so the bounds cover both.
+// plus the per-query records).  The alpha a lane runs a request with depends
+// on its batch: the per-decade tuning in batches of up to 4 queries; above
+// that the batch scale, the decade's own batch scale, or the untuned alpha
+// (no batch entry, few neighbours without a decade alpha, or a batch planned
+// again without the batch alpha).  y and z differ with alpha, so the bounds
+// cover every one of them.
 static Req make_req(cpx_server *S, u128 x, Clock::time_point t)
 {
     const cpx_params &P = S->cfg.params;
@@ -244,15 +247,26 @@ static Req make_req(cpx_server *S, u128 x, Clock::time_point t)
     bool wide = false;
     compute_needs(rq, qd, r.need, wide);
     QD d = qd[0];
-    if (M->batch_tuned && M->batch_tune.alpha_milli && !P.alpha_num) {
-        BatchReq rb = rq;
-        rb.tune = nullptr;
-        rb.alpha_scale = M->batch_tune.alpha_milli;
+    auto also = [&](const BatchReq &rb) {
         std::vector<QD> qb;
         TableNeed nb;
         compute_needs(rb, qb, nb, wide);
         r.need = merge(r.need, nb);
         if (qb[0].z > d.z) d = qb[0];
+    };
+    if (!P.alpha_num) {
+        BatchReq rb = rq;
+        rb.tune = nullptr;
+        also(rb);  // the untuned alpha
+        if (M->batch_tuned && M->batch_tune.alpha_milli) {
+            rb.alpha_scale = M->batch_tune.alpha_milli;
+            also(rb);
+            const uint32_t e = decade_of(x);
+            if (e < kTuneDecades && M->batch_alpha_dec[e]) {
+                rb.alpha_scale = M->batch_alpha_dec[e];
+                also(rb);
+            }
+        }
     }
     r.x = x;
     r.t_arrive = t;
@@ -389,6 +403,7 @@ int cpx_serve_create(cpx_ctx *ctx, const cpx_serve_config *cfg, cpx_server **out
             l->tuned = ctx->tuned;
             l->batch_tune = ctx->batch_tune;
             l->batch_tuned = ctx->batch_tuned;
+            for (uint32_t e = 0; e < kTuneDecades; e++) l->batch_alpha_dec[e] = ctx->batch_alpha_dec[e];
             S->lanes.push_back(l);
         }
         ctx->server_attached = true;

@@ -37,3 +37,24 @@ def test_autotune_keeps_results_and_round_trips(cpx, ctx, tmp_path):
     with pytest.raises(cpx.CpxError):
         own.autotune_batch(xs[:3])
     own.close()
+
+
+def test_tuning_file_layout_does_not_matter(cpx, tmp_path):
+    """The committed table read from its own file and from the same JSON on one
+    line gives the same entries (per decade, batch, per-decade batch alpha)."""
+    import json
+    import os
+
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    src = os.path.join(root, "cudapix_b200", "tuning", "b200.json")
+    one = tmp_path / "one_line.json"
+    one.write_text(json.dumps(json.load(open(src))))
+    a, b = cpx.Context(0), cpx.Context(0)
+    a.tune_load(src)
+    b.tune_load(str(one))
+    decades = [e["decade"] for e in json.load(open(src))["entries"]]
+    assert len(decades) >= 10
+    for d in decades:
+        assert a.tune_get(d) == b.tune_get(d), d
+    a.close()
+    b.close()

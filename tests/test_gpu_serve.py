@@ -46,6 +46,34 @@ def test_replay_poisson_trace(cpx, ctx):
     assert st["completed"] == n and st["table_growths"] == 0
 
 
+def test_tuned_lanes_cover_every_alpha(cpx, ctx, tmp_path):
+    """Lanes of a tuned context run large batches with the batch alpha, the
+    decade's own batch alpha (the committed table has them for 10^16 and
+    10^17) or, without a batch alpha, the untuned one; the admission bounds
+    cover each, so no request fails on table coverage."""
+    import json
+    import os
+
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    src = os.path.join(root, "cudapix_b200", "tuning", "b200.json")
+    t = json.load(open(src))
+    off = dict(t, entries=[dict(e, alpha_scale_milli=0) if e["decade"] == 99 else e for e in t["entries"]])
+    path_off = tmp_path / "no_batch_alpha.json"
+    path_off.write_text(json.dumps(off))  # one line: every entry is read all the same
+    xs = _xs(11, 96, 10, 16.4) + [10**16 + 61, 2 * 10**16 + 3]
+    alone = cpx.pi_batch(xs, ctx=ctx)
+    for path in (src, str(path_off)):
+        own = cpx.Context(0)
+        own.tune_load(path)
+        with cpx.Server(own, lanes=2, reserve_x=10**12) as srv:
+            tickets = [srv.submit(x) for x in xs]
+            got = [srv.wait(t)[0] for t in tickets]
+            st = srv.stats()
+        own.close()
+        assert got == alone, path
+        assert st["failed"] == 0 and st["completed"] == len(xs)
+
+
 def test_tables_grow_on_demand(cpx, ctx):
     own = cpx.Context(0)
     with cpx.Server(own, lanes=2) as srv:
