@@ -258,7 +258,7 @@ __global__ void __launch_bounds__(512, 2) k_hard(const QD *__restrict__ qd, uint
                 __syncwarp();
             }
             // ---- cross off p_b in the sub-segment
-            const uint32_t cleared = cross_off(bm, cnt8, p, __shfl_sync(FULL, lr0, k), __shfl_sync(FULL, li0, k), c0, cw0,
+            const uint32_t cleared = cross_off<true>(bm, cnt8, p, __shfl_sync(FULL, lr0, k), __shfl_sync(FULL, li0, k), c0, cw0,
                                                CPT, s, CPT * 32 * warp, lane, Lw);
             tot -= __reduce_add_sync(FULL, cleared);
             __syncwarp();

@@ -234,6 +234,11 @@ static __device__ __noinline__ void level_params(LvlPar<XT> &o, XT x, uint64_t y
 // Crosses p off one warp's sub-segment of Lw bits (chunks [base_ch, base_ch +
 // 32 CPT) of the segment); the lane owns chunks [c0, c0 + CPT), cw0 = c0 -
 // base_ch.  Keeps the chunk counters current; returns the bits the lane cleared.
+// kOwnWords: primes below 128 update each multiple's word and counter without
+// a branch (measured on a B200: 4% faster for the lone-query sieve of pi(1e20)
+// with 128 threads, 1% slower for the batch-shared sieve, which keeps the
+// branch).
+template <bool kOwnWords = false>
 __device__ __forceinline__ uint32_t cross_off(uint32_t *bm, uint8_t *cnt8, uint32_t p, uint32_t r0, uint32_t i0,
                                               uint32_t c0, uint32_t cw0, uint32_t CPT, int s, uint32_t base_ch,
                                               uint32_t lane, uint32_t Lw)
@@ -261,6 +266,38 @@ __device__ __forceinline__ uint32_t cross_off(uint32_t *bm, uint8_t *cnt8, uint3
                 reinterpret_cast<uint4 *>(bm)[swz(c0 + j, s)] = make_uint4(a4[0], a4[1], a4[2], a4[3]);
             }
             cleared += cj;
+        }
+    } else if (p < 128 && kOwnWords) {
+        // at most one multiple per word: each lane jumps from multiple to
+        // multiple inside its own chunks (its words and counters only, so
+        // without a branch).  The lane's chunks c share c >> s = c0 >> s, so
+        // their swizzle is one XOR of bits 2..4 of the word index.
+        if (i0 != 0xFFFFFFFFu) {
+            const uint32_t b0 = cw0 * 128, b1 = b0 + CPT * 128;  // the lane's bits of the sub-segment
+            uint32_t i = i0;
+            if (b0 > i0) {
+                // k = ceil(n / p), n = b0 - i0 < 2^21: trunc(n / p) from the
+                // approximate reciprocal is within 1 of floor(n / p), so k lies in
+                // [t - 1, t + 2]; step up from t - 1 while k p < n
+                const int32_t n = (int32_t)(b0 - i0), pi = (int32_t)p;
+                int32_t k = (int32_t)__float2uint_rz((float)n * cpx_rcp_approx(p)) - 1;
+                k += k * pi < n;
+                k += k * pi < n;
+                k += k * pi < n;
+                i = i0 + (uint32_t)k * p;
+            }
+            const uint32_t kx = s ? (((c0 >> s) & 7u) << 2) : 0u;
+            uint32_t *bmw = bm + (base_ch << 2);
+            uint8_t *cw8 = cnt8 + base_ch;
+            for (; i < b1; i += p) {
+                const uint32_t w = i >> 5;
+                uint32_t *pw = bmw + (w ^ kx);
+                const uint32_t old = *pw, hit = old & (1u << (i & 31));
+                *pw = old ^ hit;
+                const uint32_t h = hit ? 1u : 0u;
+                cw8[w >> 2] = (uint8_t)(cw8[w >> 2] - h);
+                cleared += h;
+            }
         }
     } else if (p < 128) {
         // at most one multiple per word: each lane jumps from multiple to
