@@ -276,6 +276,15 @@ static std::vector<uint32_t> batch_alpha_scales(const u128 *xs, uint32_t Q, uint
     return sc;
 }
 
+// Groups that share one sieve of segment sg in the batch-shared sieve.  The
+// early segments hold most of the leaves, so a unit of many groups there
+// would outlast the rest of the launch; the later ones are mostly crossing
+// off, which the groups of a block share.
+static uint32_t shared_block(uint64_t sg)
+{
+    return sg < 4 ? 1u : sg < 16 ? 2u : sg < 64 ? 4u : kBlockMax;
+}
+
 // Bytes of the counting sweep's carry rows for the queries `order` of a
 // shared sieve with segments of 2^lbits odd numbers and `threads` per block.
 static uint64_t carry_row_bytes(const std::vector<QD> &qd, const std::vector<uint32_t> &order,
@@ -811,7 +820,7 @@ replan:  // again without the batch alpha when its shared sieve would not fit (b
     // ---- the batch-shared sieve: groups, and the carry rows of its counting
     // sweep (row b: the sub-segments of the segments that sieve level b)
     std::vector<HardGroup> groups;
-    std::vector<uint64_t> pre_grp(1, 0), lvl_off;
+    std::vector<uint64_t> units, lvl_off;
     uint64_t sh_nseg = 0, sh_r4max = 0;
     u128 sh_xmax = 0;
     uint32_t sh_nlv = 0;
@@ -830,10 +839,21 @@ replan:  // again without the batch alpha when its shared sieve would not fit (b
                 hg.nseg = std::max(hg.nseg, d.nseg);
             }
             groups.push_back(hg);
-            pre_grp.push_back(pre_grp.back() + hg.nseg);
             sh_nseg = std::max(sh_nseg, hg.nseg);
             sh_xmax = std::max(sh_xmax, hg.xmax);
             sh_r4max = std::max(sh_r4max, hg.r4max);
+        }
+        // units, segment-major: at segment sg the groups with nseg > sg (a
+        // prefix: z descending) in blocks of shared_block(sg) consecutive
+        // groups, each block sieving the segment once for all of them
+        for (uint64_t sg = 0; sg < sh_nseg; sg++) {
+            size_t ng = 0;
+            while (ng < groups.size() && groups[ng].nseg > sg) ng++;
+            const uint32_t G = shared_block(sg);
+            for (size_t g = 0; g < ng; g += G) {
+                const uint64_t n = std::min<size_t>(G, ng - g);
+                units.push_back(sg << 32 | (uint64_t)g << 4 | (n - 1));
+            }
         }
         const uint64_t nbm = host_pi(hP, sh_r4max);
         sh_nlv = nbm > c ? (uint32_t)(nbm - c) : 0;
@@ -844,9 +864,15 @@ replan:  // again without the batch alpha when its shared sieve would not fit (b
             lvl_off[lv + 1] = lvl_off[lv] + NW * n;
             ent += (double)n;
         }
-        for (const HardGroup &hg : groups) {
-            const uint64_t nbg = host_pi(hP, hg.r4max);
-            for (uint64_t b = c + 1; b <= nbg; b++) ent += (double)segments_at_level(hg.xmax, span, hP[b - 1], 0, hg.nseg);
+        for (const uint64_t u : units) {
+            // levels the unit sieves: those of its first group (the largest x)
+            const HardGroup &hg = groups[(u >> 4) & 0x0FFFFFFF];
+            const uint64_t lo = (u >> 32) * span, hi = lo + span;
+            uint64_t v = hg.r4max;
+            if (lo) v = std::min<uint64_t>(v, cpx_isqrt((hg.xmax - 1) / lo));
+            v = std::min<uint64_t>(v, cpx_isqrt((u128)(hi - 1)));
+            const uint64_t nb = host_pi(hP, v);
+            if (nb > c) ent += (double)(nb - c);
         }
         hard_bytes = ent * (double)(1ull << sh_lbits) / 8.0;
         lbits_max = sh_lbits;
@@ -869,10 +895,9 @@ replan:  // again without the batch alpha when its shared sieve would not fit (b
     const size_t qd_bytes = sizeof(QD) * Q, pre_bytes = (pre.size() * 8 + 15) & ~size_t(15);
     const size_t elv_bytes = elv.size() * sizeof(EasyLvl);
     const size_t grp_bytes = groups.size() * sizeof(HardGroup);
-    const size_t pg_bytes = (pre_grp.size() * 8 + 15) & ~size_t(15), lo_bytes = (lvl_off.size() * 8 + 15) & ~size_t(15);
-    const bool persist = shared && ctx->hard_persist && pre_grp.back() <= 0xFFFFFFFFull;
-    const size_t ord_bytes = persist ? ((pre_grp.back() * 4 + 15) & ~size_t(15)) : 0;
-    const size_t stage_bytes = qd_bytes + pre_bytes + elv_bytes + grp_bytes + pg_bytes + lo_bytes + ord_bytes;
+    const size_t pg_bytes = (units.size() * 8 + 15) & ~size_t(15), lo_bytes = (lvl_off.size() * 8 + 15) & ~size_t(15);
+    const bool persist = shared && ctx->hard_persist;
+    const size_t stage_bytes = qd_bytes + pre_bytes + elv_bytes + grp_bytes + pg_bytes + lo_bytes;
     const size_t acc_words = (size_t)Q * kAccStride;
     unsigned char *dbuf = (unsigned char *)ctx->b_work[0].get(stage_bytes + acc_words * 8 + 64);
     QD *d_qd = reinterpret_cast<QD *>(dbuf);
@@ -900,15 +925,12 @@ replan:  // again without the batch alpha when its shared sieve would not fit (b
         pl.sh_nseg = sh_nseg;
         pl.sh_r4max = sh_r4max;
         pl.sh_xmax = sh_xmax;
-        pl.n_gunits = pre_grp.back();
+        pl.n_gunits = units.size();
         pl.n_carry = lvl_off.back();
         pl.grp = reinterpret_cast<const HardGroup *>(d_sh);
-        pl.pre_grp = reinterpret_cast<const uint64_t *>(d_sh + grp_bytes);
+        pl.units = reinterpret_cast<const uint64_t *>(d_sh + grp_bytes);
         pl.lvl_off = reinterpret_cast<const uint64_t *>(d_sh + grp_bytes + pg_bytes);
-        if (persist) {
-            pl.unit_order = reinterpret_cast<const uint32_t *>(d_sh + grp_bytes + pg_bytes + lo_bytes);
-            pl.unit_next = d_acc + acc_words;  // zeroed with the accumulators
-        }
+        if (persist) pl.unit_next = d_acc + acc_words;  // zeroed with the accumulators
         pl.carry = ctx->b_work[4].as<uint64_t>(pl.n_carry + 1);
         const size_t ntab = groups.size() * (size_t)sh_nlv * 32, xb = wide ? 16 : 8;
         unsigned char *tab = static_cast<unsigned char *>(ctx->b_work[5].get(ntab * (xb + 8) + 64));
@@ -981,17 +1003,8 @@ replan:  // again without the batch alpha when its shared sieve would not fit (b
     if (shared) {
         unsigned char *h_sh = stage.data() + qd_bytes + pre_bytes + elv_bytes;
         memcpy(h_sh, groups.data(), grp_bytes);
-        memcpy(h_sh + grp_bytes, pre_grp.data(), pre_grp.size() * 8);
+        memcpy(h_sh + grp_bytes, units.data(), units.size() * 8);
         memcpy(h_sh + grp_bytes + pg_bytes, lvl_off.data(), lvl_off.size() * 8);
-        if (persist) {
-            // segment-major: every group's segment 0, then segment 1, ... (the
-            // early segments of a group hold most of its leaves)
-            uint32_t *ord = reinterpret_cast<uint32_t *>(h_sh + grp_bytes + pg_bytes + lo_bytes);
-            size_t k = 0;
-            for (uint64_t sg = 0; sg < sh_nseg; sg++)
-                for (size_t g = 0; g < groups.size(); g++)
-                    if (sg < groups[g].nseg) ord[k++] = (uint32_t)(pre_grp[g] + sg);
-        }
     }
     CPX_CUDA(cudaMemcpyAsync(dbuf, stage.data(), stage.size(), cudaMemcpyHostToDevice, ctx->stream));
     CPX_CUDA(cudaMemsetAsync(d_acc, 0, acc_words * 8 + 8, ctx->stream));  // and the unit counter

@@ -51,6 +51,8 @@ __host__ __device__ __forceinline__ size_t shared_smem(uint32_t lbits, uint32_t 
     o += (threads / 32) * leaf_cap(threads) * 8;   // gathered leaves: m, query | (mu(m) = -1) << 31
     o += (threads / 32) * kGroupMax * 16;  // x/p of the group's queries, per warp
     o += (threads / 32) * kGroupMax * 12;  // per-warp, per-query level sums and Sum(-mu)
+    o += kBlockMax * kGroupMax * 12;       // per (group, slot): query, y, level threshold
+    o += kBlockMax * kGroupMax * 16;       // per (group, slot): the hard sum over the unit
     return o;
 }
 
@@ -280,34 +282,49 @@ constexpr uint32_t kLaneEntries = 64;
 // an SM and 128 (no spills) when 16 do.  The launch takes the variant whose
 // MINB blocks fit the SM's shared memory with this segment size.
 #define CPX_HS_PARAMS                                                                                          \
-    const QD *__restrict__ qd, const HardGroup *__restrict__ grp, const uint64_t *__restrict__ pre_grp,          \
-        uint32_t ngrp, uint64_t total, uint32_t lbits, uint32_t c, const uint32_t *__restrict__ P, uint32_t np, \
+    const QD *__restrict__ qd, const HardGroup *__restrict__ grp, const uint64_t *__restrict__ units,            \
+        uint64_t total, uint32_t lbits, uint32_t c, const uint32_t *__restrict__ P, uint32_t np, \
         const int32_t *__restrict__ MU, const cpx_pient *__restrict__ Tpi, const uint64_t *__restrict__ lvl_off, \
         uint32_t nlv, const uint64_t *__restrict__ carry, unsigned long long *__restrict__ acc,                   \
         HardJob *__restrict__ jobs, unsigned int *__restrict__ njobs, uint64_t *__restrict__ job_units,          \
         unsigned char *__restrict__ snap, unsigned int *__restrict__ nsnap, uint32_t max_jobs, uint32_t lbits_sub, \
         uint32_t offload_min, const XT *__restrict__ gxp, const uint2 *__restrict__ gae
 #define CPX_HS_ARGS                                                                                             \
-    qd, grp, pre_grp, ngrp, total, lbits, c, P, np, MU, Tpi, lvl_off, nlv, carry, acc, jobs, njobs, job_units, snap, \
+    qd, grp, units, total, lbits, c, P, np, MU, Tpi, lvl_off, nlv, carry, acc, jobs, njobs, job_units, snap, \
         nsnap, max_jobs, lbits_sub, offload_min, gxp, gae
 
-// one (group, segment) unit of the shared sieve, by one CTA
+// one unit of the shared sieve, by one CTA: a segment and up to kBlockMax
+// consecutive groups (z descending), packed as seg << 32 | g0 << 4 | (n - 1).
+// The segment is sieved once for all of them, and each level answers every
+// group's leaves in turn.
 template <class XT> __device__ __forceinline__ void hard_shared_unit(uint64_t unit, CPX_HS_PARAMS)
 {
     extern __shared__ uint4 smem4[];
-    __shared__ uint32_t s_B;
-    const uint32_t g = find_q(pre_grp, ngrp, unit);
-    const HardGroup &G = grp[g];
-    const uint64_t seg = unit - pre_grp[g];
+    __shared__ uint32_t s_Bg[kBlockMax], s_ng[kBlockMax];
+    const uint64_t ud = units[unit];
+    const uint64_t seg = ud >> 32;
+    const uint32_t g0 = (uint32_t)(ud >> 4) & 0x0FFFFFFFu, ngr = (uint32_t)(ud & 15) + 1;
     const uint32_t T = blockDim.x, tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, NW = T >> 5;
     const uint32_t L = 1u << lbits, NC = L >> 7, CPT = NC / T;
     const int s = __ffs(CPT) - 1;
     const uint32_t Lw = L / NW;
     const uint64_t span = 2ull * L, lo = seg * span;
     const uint64_t lo_w = lo + 2ull * Lw * warp, hi_w = lo_w + 2ull * Lw;
-    if (tid == 0) s_B = seg_levels<XT>((XT)G.xmax, G.r4max, lo, lo + span, P, np);
+    // per group: the levels the segment sieves for it (0: none, the group's
+    // queries end below the segment) and its query count
+    if (tid < kBlockMax) {
+        uint32_t bg = 0, n = 0;
+        if (tid < ngr && seg < grp[g0 + tid].nseg) {
+            const HardGroup &G = grp[g0 + tid];
+            bg = min(seg_levels<XT>((XT)G.xmax, G.r4max, lo, lo + span, P, np), c + nlv);
+            n = G.n;
+        }
+        s_Bg[tid] = bg;
+        s_ng[tid] = n;
+    }
     __syncthreads();
-    const uint32_t B = min(s_B, c + nlv);
+    uint32_t B = 0;
+    for (uint32_t g = 0; g < ngr; g++) B = max(B, s_Bg[g]);
     if (B <= c) return;  // uniform over the CTA
 
     unsigned char *sp = reinterpret_cast<unsigned char *>(smem4);
@@ -328,25 +345,39 @@ template <class XT> __device__ __forceinline__ void hard_shared_unit(uint64_t un
     unsigned long long *s_sum = reinterpret_cast<unsigned long long *>(sp + o) + 32 * warp;
     o += NW * 32 * 8;
     int *s_ms = reinterpret_cast<int *>(sp + o) + 32 * warp;
+    o += NW * 32 * 4;
+    // per (group, slot) of the block: the query, its y and its level
+    // threshold, and its hard sum over the unit (two words, added by atomics)
+    uint32_t *s_qj = reinterpret_cast<uint32_t *>(sp + o);
+    uint32_t *s_yj = s_qj + kBlockMax * 32;
+    uint32_t *s_pt = s_yj + kBlockMax * 32;
+    o += kBlockMax * 32 * 12;
+    unsigned long long *s_acc = reinterpret_cast<unsigned long long *>(sp + o);
     s_sum[lane] = 0;
     s_ms[lane] = 0;
-
-    // this lane's query
-    const uint32_t nq = G.n;
-    const uint32_t qj = lane < nq ? G.q[lane] : 0xFFFFFFFFu;
-    // the lane's query has leaves in the warp's sub-segment at level b only
-    // if lo_w <= z, p^2 < hi_w and x / (p hi_w) < y, i.e. p > pthr =
-    // floor(x / (y hi_w)); y < 2^31
-    bool qin = false;
-    uint32_t yj = 0, pthr = 0xFFFFFFFFu;
-    if (lane < nq) {
-        const QD &d = qd[qj];
-        yj = (uint32_t)d.y;
-        qin = lo_w <= d.z;
-        const u128 t = (u128)xload<XT>(d) / ((u128)d.y * hi_w);
-        pthr = t < 0xFFFFFFFFull ? (uint32_t)t : 0xFFFFFFFFu;
+    // A query has leaves in the segment at level b only if lo <= z, p^2 < hi
+    // and x / (p hi) < y, i.e. p > pthr = floor(x / (y hi)) (hi the segment's
+    // end; each warp's exact candidate range decides the rest); y < 2^31.
+    // pthr = 0xFFFFFFFF: no leaves (lo > z, or no query in the slot).
+    for (uint32_t t = tid; t < kBlockMax * 32; t += T) {
+        const uint32_t g = t >> 5, j = t & 31;
+        uint32_t qv = 0xFFFFFFFFu, yv = 0, pt = 0xFFFFFFFFu;
+        if (g < ngr && j < s_ng[g]) {
+            qv = grp[g0 + g].q[j];
+            const QD &d = qd[qv];
+            yv = (uint32_t)d.y;
+            if (lo <= d.z) {
+                const u128 tt = (u128)xload<XT>(d) / ((u128)d.y * (lo + span));
+                pt = tt < 0xFFFFFFFFull ? (uint32_t)tt : 0xFFFFFFFFu;
+            }
+        }
+        s_qj[t] = qv;
+        s_yj[t] = yv;
+        s_pt[t] = pt;
+        s_acc[2 * t] = 0;
+        s_acc[2 * t + 1] = 0;
     }
-    i128 accq = 0;  // this lane's query: its hard sum over the CTA's part of the segment
+    __syncthreads();
 
     const uint32_t c0 = CPT * tid, cw0 = c0 - CPT * 32 * warp;
     presieve(bm, cnt8, P, c, lo, c0, CPT, s);
@@ -359,7 +390,6 @@ template <class XT> __device__ __forceinline__ void hard_shared_unit(uint64_t un
         return (uint64_t)cpx_qdiv(xv, m);
     };
     const Recip r_lo{lo_w, lo_w ? 1.0 / (double)lo_w : 0.0}, r_hi{hi_w, 1.0 / (double)hi_w};
-    const size_t gbase = (size_t)g * nlv * 32 + lane;  // this lane's slot in the group's level table
 
     for (uint32_t gb = c + 1; gb <= B; gb += 32) {
         const uint32_t nl = min(32u, B - gb + 1);
@@ -380,14 +410,19 @@ template <class XT> __device__ __forceinline__ void hard_shared_unit(uint64_t un
             const uint32_t b = gb + k;
             const uint32_t p = __shfl_sync(FULL, lp, k);
             const uint64_t pp = (uint64_t)p * p;
+            bool built = false;  // the level's chunk and lane prefixes
+            for (uint32_t g = 0; g < ngr; g++) {
+            if (b > s_Bg[g]) continue;  // uniform: the group's queries end below this level here
+            const uint32_t tq = 32 * g + lane;  // this lane's slot of group g
+            const uint32_t qj = s_qj[tq], yj = s_yj[tq], pthr = s_pt[tq], nq = s_ng[g];
             // Candidates (mlo, mhi] of this lane's query in the warp's
             // sub-segment.  None unless some u in it satisfies u <= z,
             // u >= p^2 and x/(p hi_w) < y (else m > y).
             XT xp = 0;
             uint32_t mlo = 0, mhi = 0;
             bool act = false;
-            if (qin && hi_w > pp && p > pthr) {
-                const size_t gi = gbase + (size_t)(b - c - 1) * 32;
+            if (hi_w > pp && p > pthr) {
+                const size_t gi = ((size_t)(g0 + g) * nlv + (b - c - 1)) * 32 + lane;
                 xp = gxp[gi];
                 const uint2 ae = gae[gi];  // y/p, min(y, x/p^3)
                 uint64_t a = ae.x;
@@ -404,10 +439,13 @@ template <class XT> __device__ __forceinline__ void hard_shared_unit(uint64_t un
             }
             const unsigned bal = __ballot_sync(FULL, act);
             if (bal) {
-                // chunk and lane prefixes of the sub-segment from the chunk counters
-                uint32_t off0;
-                warp_place(chunk_prefixes(cnt8, pre16, c0, CPT), lane, off0);
-                wl[lane] = off0;
+                if (!built) {
+                    // chunk and lane prefixes of the sub-segment from the chunk counters
+                    uint32_t off0;
+                    warp_place(chunk_prefixes(cnt8, pre16, c0, CPT), lane, off0);
+                    wl[lane] = off0;
+                    built = true;
+                }
                 if (act) s_xp[lane] = xp;
                 __syncwarp();
                 const uint64_t C = __shfl_sync(FULL, lC, k);  // survivors below the sub-segment
@@ -464,7 +502,7 @@ template <class XT> __device__ __forceinline__ void hard_shared_unit(uint64_t un
                             }
                         }
                     }
-                    accq += (i128)sv + (i128)C * (i128)sm;
+                    if (sv || sm) cpx_atomic_add_i128(s_acc + 2 * tq, (i128)sv + (i128)C * (i128)sm);
                     __syncwarp();
                 } else {
                 // running sums of the query of this lane's last leaf
@@ -582,39 +620,36 @@ template <class XT> __device__ __forceinline__ void hard_shared_unit(uint64_t un
                 __syncwarp();
                 // the level's sums of this lane's query: Sum(-mu)(carry + count)
                 if (lane < nq) {
-                    accq += (i128)(int64_t)s_sum[lane] + (i128)C * (i128)s_ms[lane];
+                    const i128 v = (i128)(int64_t)s_sum[lane] + (i128)C * (i128)s_ms[lane];
+                    if (v) cpx_atomic_add_i128(s_acc + 2 * tq, v);
                     s_sum[lane] = 0;
                     s_ms[lane] = 0;
                 }
                 __syncwarp();
                 }
             }
+            }  // groups
             // ---- cross off p_b in the sub-segment
             cross_off(bm, cnt8, p, __shfl_sync(FULL, lr0, k), __shfl_sync(FULL, li0, k), c0, cw0, CPT, s,
                       CPT * 32 * warp, lane, Lw);
             __syncwarp();
         }
     }
-    __syncthreads();  // every warp is past its levels: the leaf buffers take the per-warp totals
-    i128 *red = reinterpret_cast<i128 *>(lbuf0);
-    red[32 * warp + lane] = accq;
-    __syncthreads();
-    if (warp == 0 && lane < nq) {
-        i128 t = 0;
-        for (uint32_t ww = 0; ww < NW; ww++) t += red[32 * ww + lane];
-        acc_add(acc, qj, ACC_HARD, t);
+    __syncthreads();  // every warp is past its levels: the block's sums are complete
+    for (uint32_t t = tid; t < ngr * 32; t += T) {
+        if (s_qj[t] == 0xFFFFFFFFu) continue;
+        const i128 v = (i128)(((u128)s_acc[2 * t + 1] << 64) | s_acc[2 * t]);
+        if (v) acc_add(acc, s_qj[t], ACC_HARD, v);
     }
 }
 
-// The kernel: one CTA per unit (unit_order null), or a persistent grid whose
-// CTAs take units from the device counter `next` in the order unit_order
-// gives, so that the heaviest units start first and no CTA waits at the end
-// for a late wave.
+// The kernel: one CTA per unit (next null), or a persistent grid whose CTAs
+// take units in order from the device counter `next` (segment-major, so that
+// the heaviest units start first and no CTA waits at the end for a late wave).
 template <class XT, int TMAX, int MINB>
-__global__ void __launch_bounds__(TMAX, MINB)
-    k_hard_shared(const uint32_t *__restrict__ unit_order, unsigned long long *__restrict__ next, CPX_HS_PARAMS)
+__global__ void __launch_bounds__(TMAX, MINB) k_hard_shared(unsigned long long *__restrict__ next, CPX_HS_PARAMS)
 {
-    if (!unit_order) {
+    if (!next) {
         if (blockIdx.x < total) hard_shared_unit<XT>(blockIdx.x, CPX_HS_ARGS);
         return;
     }
@@ -625,7 +660,7 @@ __global__ void __launch_bounds__(TMAX, MINB)
         __syncthreads();
         const unsigned long long k = s_k;
         if (k >= total) return;
-        hard_shared_unit<XT>(unit_order[k], CPX_HS_ARGS);
+        hard_shared_unit<XT>(k, CPX_HS_ARGS);
     }
 }
 
@@ -679,9 +714,8 @@ template <class XT> static void shared_go(cpx_ctx *ctx, const Plan &pl)
         auto go = [&](auto kern, int minb) {
             const size_t smem = shared_smem(pl.sh_lbits, T);
             unsigned grid = (unsigned)pl.n_gunits;
-            if (pl.unit_order) grid = (unsigned)std::min<uint64_t>(pl.n_gunits, (uint64_t)minb * ctx->sm_count);
-            kern<<<grid, T, smem, ctx->stream>>>(
-                pl.unit_order, pl.unit_next, pl.qd, pl.grp, pl.pre_grp, pl.n_grp, pl.n_gunits, pl.sh_lbits, pl.c, tb.P,
+            if (pl.unit_next) grid = (unsigned)std::min<uint64_t>(pl.n_gunits, (uint64_t)minb * ctx->sm_count);
+            kern<<<grid, T, smem, ctx->stream>>>(pl.unit_next, pl.qd, pl.grp, pl.units, pl.n_gunits, pl.sh_lbits, pl.c, tb.P,
                 (uint32_t)tb.prm_n, tb.MU, tb.T, pl.lvl_off, pl.sh_nlv, pl.carry, pl.acc, pl.jobs, pl.njobs,
                 pl.job_units, pl.snap, pl.nsnap, pl.max_jobs, lbits_sub,
                 (uint32_t)std::min<uint64_t>(pl.offload_min, 0xFFFFFFFFull), gxp, pl.gae);

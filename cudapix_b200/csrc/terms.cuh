@@ -56,6 +56,9 @@ struct __align__(16) HardJob {
 // descending).  Its work units are the segments [0, nseg) of the group;
 // xmax and r4max = iroot4(xmax) bound the levels each segment sieves.
 constexpr uint32_t kGroupMax = 32;
+// Consecutive groups that share one sieve of each segment (a work unit of the
+// shared sieve is a block of up to kBlockMax groups and one segment).
+constexpr uint32_t kBlockMax = 8;
 struct __align__(16) HardGroup {
     u128 xmax;
     uint64_t r4max, nseg;
@@ -109,16 +112,16 @@ struct Plan {
     uint64_t sh_nseg = 0, sh_r4max = 0, n_gunits = 0, n_carry = 0;
     u128 sh_xmax = 0;
     const HardGroup *grp = nullptr;
-    const uint64_t *pre_grp = nullptr;  // n_grp + 1 unit offsets
+    // units (n_gunits): a segment and up to kBlockMax consecutive groups,
+    // seg << 32 | g0 << 4 | (n - 1), segment-major
+    const uint64_t *units = nullptr;
     const uint64_t *lvl_off = nullptr;  // sh_nlv + 1 row offsets into carry
     uint64_t *carry = nullptr;
     unsigned int *nsnap = nullptr;      // device counter of snapshot slots
     void *gxp = nullptr;                // x/p per (group, level, slot): uint64 or u128 (wide)
     uint2 *gae = nullptr;               // y/p and min(y, x/p^3) per (group, level, slot)
-    // persistent launch of the shared sieve: its units in the order they are
-    // taken (segment-major: every group's segment 0 first, the heaviest) and
-    // the device counter that hands them out (null: one CTA per unit)
-    const uint32_t *unit_order = nullptr;
+    // persistent launch of the shared sieve: the device counter that hands
+    // out the units in order (null: one CTA per unit)
     unsigned long long *unit_next = nullptr;
 };
 
