@@ -973,7 +973,14 @@ replan:  // again without the batch alpha when its shared sieve would not fit (b
         pl.job_units = ctl + 2;
         pl.snap = static_cast<unsigned char *>(ctx->b_snap.get((pl.max_jobs + 1) * stride));
     }
-    if (pl.n_easy) pl.easy_off = ctx->b_work[7].as<uint64_t>(pl.n_easy + 1);
+    if (pl.n_easy) {
+        // the chunk offsets, then (up to 1 GiB) the units' plans
+        const size_t ob = ((pl.n_easy + 1) * 8 + 63) & ~size_t(63), rb = pl.n_easy * 64;
+        const bool with_rec = rb <= (size_t(1) << 30);
+        unsigned char *eb = static_cast<unsigned char *>(ctx->b_work[7].get(ob + (with_rec ? rb : 0) + 64));
+        pl.easy_off = reinterpret_cast<uint64_t *>(eb);
+        pl.easy_rec = with_rec ? eb + ob : nullptr;
+    }
     uint32_t n_levels = 0;
     if (rq.hard_levels && !qd[0].direct && qd[0].nb > c) {
         n_levels = qd[0].nb - c;

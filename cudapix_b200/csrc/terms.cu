@@ -325,12 +325,35 @@ __device__ __noinline__ bool easy_plan(XT x, uint64_t y, uint64_t p, uint64_t pr
     return true;
 }
 
+// The plan of one easy unit (query, p = p_b), written by pass 1 for pass 2.
+struct __align__(16) EasyRec {
+    u128 xp;
+    uint64_t klo, khi;
+    uint32_t qlo, q1, qhi, kq0;
+    uint32_t kq1, b, q, pad;
+};
+static_assert(sizeof(EasyRec) == 64, "EasyRec is four 16-byte words");
+
+__device__ __forceinline__ void easy_unpack(const EasyRec &r, EasyP &e)
+{
+    e.qlo = r.qlo;
+    e.q1 = r.q1;
+    e.qhi = r.qhi;
+    e.kq0 = r.kq0;
+    e.kq1 = r.kq1;
+    e.klo = r.klo;
+    e.khi = r.khi;
+    e.nsp = (e.kq1 - e.kq0 + kEasySparse - 1) / kEasySparse;
+    e.ncl = e.qhi > e.q1 ? (e.khi > e.klo ? (e.khi - e.klo + kEasyClu - 1) / kEasyClu : 1) : 0;
+}
+
 // Pass 1: work chunks of each p (one thread per p = P[c + i]); cnt[total] is
-// left 0 so that the exclusive scan of cnt ends with the grand total.
+// left 0 so that the exclusive scan of cnt ends with the grand total.  With
+// rec, the units that have leaves also leave their plan there.
 template <class XT>
 __global__ void k_easy_count(const QD *__restrict__ qd, uint32_t Q, const uint64_t *__restrict__ pre, uint64_t total,
                              const uint32_t *__restrict__ P, uint64_t prm_max, const cpx_pient *__restrict__ T,
-                             uint64_t *__restrict__ cnt)
+                             uint64_t *__restrict__ cnt, EasyRec *__restrict__ rec)
 {
     const uint64_t unit = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (unit > total) return;
@@ -343,7 +366,23 @@ __global__ void k_easy_count(const QD *__restrict__ qd, uint32_t Q, const uint64
     const uint64_t p = __ldg(P + d.c + (unit - pre[q]));
     XT xp;
     EasyP e;
-    cnt[unit] = easy_plan<XT>(xload<XT>(d), d.y, p, prm_max, T, xp, e) ? e.nsp + e.ncl : 0;
+    const bool any = easy_plan<XT>(xload<XT>(d), d.y, p, prm_max, T, xp, e);
+    cnt[unit] = any ? e.nsp + e.ncl : 0;
+    if (rec && any && e.nsp + e.ncl) {
+        EasyRec r;
+        r.xp = (u128)xp;
+        r.klo = e.klo;
+        r.khi = e.khi;
+        r.qlo = (uint32_t)e.qlo;
+        r.q1 = (uint32_t)e.q1;
+        r.qhi = (uint32_t)e.qhi;
+        r.kq0 = (uint32_t)e.kq0;
+        r.kq1 = (uint32_t)e.kq1;
+        r.b = d.c + 1 + (uint32_t)(unit - pre[q]);
+        r.q = q;
+        r.pad = 0;
+        rec[unit] = r;
+    }
 }
 
 // Pass 2: each warp owns a contiguous slice of chunks.  A sparse chunk is
@@ -355,7 +394,8 @@ __global__ void __launch_bounds__(kThreads) k_easy(const QD *__restrict__ qd, ui
                                                    const uint64_t *__restrict__ off,
                                                    const uint32_t *__restrict__ P, uint64_t prm_max,
                                                    const cpx_pient *__restrict__ T,
-                                                   unsigned long long *__restrict__ acc)
+                                                   unsigned long long *__restrict__ acc,
+                                                   const EasyRec *__restrict__ rec)
 {
     const int lane = threadIdx.x & 31;
     const WarpSlice sl = warp_slice(off[total_units]);
@@ -366,19 +406,34 @@ __global__ void __launch_bounds__(kThreads) k_easy(const QD *__restrict__ qd, ui
     XT xp = 0;
     EasyP e = {};
     for (uint64_t ch = sl.u0; ch < sl.u1; ch++) {
-        if (ch < c_first || ch > c_last || c_unit == ~0ull) {
-            uint64_t lo = 0, hi = total_units;  // off[lo] <= ch < off[hi]
-            while (hi - lo > 1) {
-                const uint64_t mid = (lo + hi) >> 1;
-                if (__ldg(off + mid) <= ch) lo = mid;
-                else hi = mid;
+        if (ch > c_last || c_unit == ~0ull) {
+            // the unit of chunk ch: a binary search for the slice's first
+            // chunk, then a walk forward (units without leaves have no chunks)
+            if (c_unit == ~0ull) {
+                uint64_t lo = 0, hi = total_units;  // off[lo] <= ch < off[hi]
+                while (hi - lo > 1) {
+                    const uint64_t mid = (lo + hi) >> 1;
+                    if (__ldg(off + mid) <= ch) lo = mid;
+                    else hi = mid;
+                }
+                c_unit = lo;
+            } else {
+                do c_unit++;
+                while (__ldg(off + c_unit + 1) <= ch);
             }
-            c_unit = lo;
-            q = find_q(pre, Q, c_unit);
-            const QD &d = qd[q];
-            const uint64_t i = c_unit - __ldg(pre + q);
-            b = d.c + 1 + i;  // p = p_b
-            easy_plan<XT>(xload<XT>(d), d.y, __ldg(P + d.c + i), prm_max, T, xp, e);
+            if (rec) {
+                const EasyRec r = rec[c_unit];
+                xp = (XT)r.xp;
+                easy_unpack(r, e);
+                b = r.b;
+                q = r.q;
+            } else {
+                q = find_q(pre, Q, c_unit);
+                const QD &d = qd[q];
+                const uint64_t i = c_unit - __ldg(pre + q);
+                b = d.c + 1 + i;  // p = p_b
+                easy_plan<XT>(xload<XT>(d), d.y, __ldg(P + d.c + i), prm_max, T, xp, e);
+            }
             c_first = __ldg(off + c_unit);
             c_last = c_first + e.nsp + e.ncl - 1;
         }
@@ -596,14 +651,15 @@ void launch_easy(cpx_ctx *ctx, const Plan &pl)
 {
     if (!pl.n_easy) return;
     uint64_t *off = pl.easy_off;
+    EasyRec *rec = static_cast<EasyRec *>(pl.easy_rec);
     const unsigned gc = (unsigned)((pl.n_easy + 1 + 255) / 256);
     const Tables &tb = ctx->tab;
     if (pl.wide)
         k_easy_count<u128><<<gc, 256, 0, ctx->stream>>>(pl.qd, pl.Q, pl.pre_easy, pl.n_easy, tb.P, tb.prm_max,
-                                                         tb.T, off);
+                                                         tb.T, off, rec);
     else
         k_easy_count<uint64_t><<<gc, 256, 0, ctx->stream>>>(pl.qd, pl.Q, pl.pre_easy, pl.n_easy, tb.P, tb.prm_max,
-                                                             tb.T, off);
+                                                             tb.T, off, rec);
     CPX_LAUNCH("k_easy_count");
     note_launch(ctx);
     scan_u64(ctx, off, pl.n_easy + 1);
@@ -611,10 +667,10 @@ void launch_easy(cpx_ctx *ctx, const Plan &pl)
     KSpan ks(ctx, "k_easy");
     if (pl.wide)
         k_easy<u128><<<grid, kThreads, 0, ctx->stream>>>(pl.qd, pl.Q, pl.pre_easy, pl.n_easy, off, tb.P, tb.prm_max,
-                                                         tb.T, pl.acc);
+                                                         tb.T, pl.acc, rec);
     else
         k_easy<uint64_t><<<grid, kThreads, 0, ctx->stream>>>(pl.qd, pl.Q, pl.pre_easy, pl.n_easy, off, tb.P,
-                                                             tb.prm_max, tb.T, pl.acc);
+                                                             tb.prm_max, tb.T, pl.acc, rec);
     CPX_LAUNCH("k_easy");
     note_launch(ctx);
 }

@@ -103,6 +103,7 @@ struct Plan {
     uint32_t n_elv = 0;
     uint64_t n_ecomp = 0;
     uint64_t *easy_off = nullptr;  // n_easy + 1 chunk offsets of the easy leaves
+    void *easy_rec = nullptr;      // n_easy unit plans (EasyRec, 64 B each), or null: k_easy plans itself
     HardLevel *hard_levels = nullptr;  // per-level outputs of query 0 (a part of a split query)
     // batch-shared sieve (hard_shared.cu): one counting sweep over the
     // segments [0, sh_nseg) for xmax, carries per (sub-segment, level) in
