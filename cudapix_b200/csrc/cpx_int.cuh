@@ -210,16 +210,17 @@ __device__ __forceinline__ u128 cpx_qdiv(u128 n, uint64_t d)
 
 #endif  // __CUDACC__
 
-// floor(n / d) for n < 2^40 and 1 <= d < 2^32, with nd = n as a double, from
-// a reciprocal estimate r0 with |d r0 - 1| < 2^-22 (the hardware
-// approximation of 1/d rounded to float: at most 1 ulp of the approximation
-// plus the rounding of d to float).  One Newton-Raphson step with its target
-// raised by 2^-42,
+// floor(n / d) for 1 <= d < 2^32 and n < 2^53 (nd = n as a double, exact)
+// with a quotient below 2^41 (every n < 2^40 qualifies), from a reciprocal
+// estimate r0 with |d r0 - 1| < 2^-22 (the hardware approximation of 1/d
+// rounded to float: at most 1 ulp of the approximation plus the rounding of
+// d to float).  One Newton-Raphson step with its target raised by 2^-42,
 //   rd = r0 + r0 (1 + 2^-42 - d r0) = (1/d) (1 - e^2 + 2^-42 (1 + e)),  e = d r0 - 1,
 // lies in (1/d, (1/d)(1 + 2^-41.9)) after the two roundings of the fused
 // steps (e^2 < 2^-44), so t = n rd rounded toward +infinity satisfies
-// n/d <= t < n/d + 2^40 2^-41.9: trunc(t) is floor(n/d) or floor(n/d) + 1,
-// and a single comparison of q d with n settles which (q d <= n + d < 2^41).
+// n/d <= t < n/d + (n/d) 2^-41.8 < n/d + 0.6: trunc(t) is floor(n/d) or
+// floor(n/d) + 1, and a single comparison of q d with n settles which
+// (q d <= n + d < 2^54).
 // QT = uint32_t when floor(n/d) < 2^32 - 1.  On the device d becomes a
 // double and trunc(t) an integer through the exponent 2^52 (2^52 + d is
 // exact; 2^52 + t rounded toward zero is 2^52 + trunc(t) for t < 2^52), on

@@ -86,6 +86,11 @@ bool dr_domain_ok(u128 x, uint64_t y, uint32_t c)
 // An upper bound of x^(2/5), at most 2^31: the u primes an easy leaf's
 // clustered part needs (the kernels fall back to single leaves above the
 // resident prime list, so the bound only has to be close).
+// P2 takes its primes from the prime list for sqrt x up to this bound (the
+// list then holds up to 28 M primes, 112 MB); beyond it from pi-table bitmaps
+constexpr uint64_t kP2PrimeMax = 1ull << 29;
+static uint64_t tb_prm_max(const cpx_ctx *ctx) { return ctx->tab.P ? ctx->tab.prm_max : 0; }
+
 static uint64_t easy_u_bound(u128 x)
 {
     const long double v = powl((long double)x, 0.4L) * 1.001L + 16.0L;
@@ -522,6 +527,8 @@ void compute_needs(const BatchReq &rq, std::vector<QD> &qd, TableNeed &need, boo
                 Pneed = std::max<uint64_t>(Pneed, cpx_isqrt((u128)d.z) + 2);
             } else {
                 N = std::max<uint64_t>(N, std::max(d.z, sx) + 1);
+                // the primes p of P2 from the prime list (k_p2_primes)
+                if (sx <= kP2PrimeMax) Pneed = std::max<uint64_t>(Pneed, sx + 1);
             }
         }
         if (mask & TERM_TRIV) N = std::max<uint64_t>(N, std::max(y, cx) + 1);
@@ -711,6 +718,14 @@ replan:  // again without the batch alpha when its shared sieve would not fit (b
         }
     }
 
+    // P2 walks the prime list when it reaches every query's sqrt x (and the
+    // batch has no windowed P2); else pi-table entries of candidates
+    bool p2_primes = (mask & TERM_P2) != 0;
+    for (uint32_t i = 0; i < Q && p2_primes; i++) {
+        const QD &d = qd[i];
+        if (!d.direct && d.sx > d.y && (d.p2win || d.sx > kP2PrimeMax || d.sx > tb_prm_max(ctx))) p2_primes = false;
+    }
+
     // ---- units per kernel family (queries planned in parallel blocks)
     std::vector<uint64_t> pre(6 * (size_t)(Q + 1), 0);
     uint64_t *p_ord = pre.data(), *p_p2 = p_ord + (Q + 1), *p_triv = p_p2 + (Q + 1), *p_easy = p_triv + (Q + 1),
@@ -730,7 +745,14 @@ replan:  // again without the batch alpha when its shared sieve would not fit (b
                 const u128 x = d.x;
                 const uint64_t pc = kSmallPrimes[c];
                 if (mask & TERM_ORD) n_ord = ((d.y + 1) / 2 + 3) / 4;
-                if ((mask & TERM_P2) && d.sx > d.y && !d.p2win) n_p2 = ((d.sx - 1) >> 7) - (d.y >> 7) + 1;
+                if ((mask & TERM_P2) && d.sx > d.y && !d.p2win) {
+                    if (p2_primes) {
+                        d.piy = (uint32_t)host_pi(hP, d.y);
+                        n_p2 = host_pi(hP, d.sx) - d.piy;
+                    } else {
+                        n_p2 = ((d.sx - 1) >> 7) - (d.y >> 7) + 1;
+                    }
+                }
                 if (mask & TERM_TRIV) n_triv = (d.cx > d.tx) ? ((d.cx - 1) >> 7) - (d.tx >> 7) + 1 : 1;
                 // primes p_c < p <= icbrt(x) (or <= easy_pmax)
                 const uint64_t pe = rq.easy_pmax ? std::min<uint64_t>(d.cx, rq.easy_pmax) : d.cx;
@@ -887,6 +909,7 @@ replan:  // again without the batch alpha when its shared sieve would not fit (b
     pl.lbits_max = lbits_max;
     pl.n_ord = p_ord[Q];
     pl.n_p2 = p_p2[Q];
+    pl.p2_primes = p2_primes;
     pl.n_triv = p_triv[Q];
     pl.n_easy = p_easy[Q];
     pl.n_seg = p_seg[Q];

@@ -124,6 +124,50 @@ __global__ void __launch_bounds__(kThreads) k_p2(const QD *__restrict__ qd, uint
     warp_flush(a, acc, ACC_P2);
 }
 
+// P2 by the prime list, when it reaches every query's sqrt x: one prime
+// p = p_k per lane, k in (pi(y), pi(sqrt x)], adding pi(x/p) - k + 1.  The
+// quotient x/p < z is cpx_quot40_core's when x < 2^53 and z < 2^41.
+template <class XT>
+__global__ void __launch_bounds__(kThreads) k_p2_primes(const QD *__restrict__ qd, uint32_t Q,
+                                                        const uint64_t *__restrict__ pre, uint64_t total,
+                                                        const uint32_t *__restrict__ P,
+                                                        const cpx_pient *__restrict__ T,
+                                                        unsigned long long *__restrict__ acc)
+{
+    const WarpSlice sl = warp_slice(total);
+    const int lane = threadIdx.x & 31;
+    LaneAcc a;
+    QCache qc;
+    XT x = 0;
+    double xd = 0.0;
+    uint64_t k0 = 0;
+    bool fast = false;
+    int64_t s = 0;  // this lane's sum for query a.q since the last fold
+    for (uint64_t base = sl.u0; base < sl.u1; base += 32) {
+        const uint64_t u = base + lane;
+        if (u < sl.u1) {
+            const uint32_t q = qlookup(qc, pre, Q, u);
+            if (q != a.q) {
+                a.v += s;
+                s = 0;
+                lane_switch(a, q, acc, ACC_P2);
+                const QD &d = qd[q];
+                x = xload<XT>(d);
+                k0 = d.piy;
+                fast = ((u128)x >> 53) == 0 && (d.z >> 41) == 0;
+                xd = (double)(uint64_t)x;
+            }
+            const uint64_t k = k0 + 1 + (u - qc.lo);
+            const uint32_t p = __ldg(P + k - 1);
+            const uint64_t v = fast ? cpx_quot40_core<uint64_t>((uint64_t)x, xd, p, cpx_rcp_approx(p))
+                                    : (uint64_t)cpx_qdiv(x, (uint64_t)p);
+            s += (int64_t)cpx_pi_ge2(T, v) - (int64_t)k + 1;  // v >= p >= 2
+        }
+    }
+    a.v += s;
+    warp_flush(a, acc, ACC_P2);
+}
+
 // P2 for a query whose z lies beyond the resident pi table: the values
 // v = x/p in [A, B) of one table window.  One lane per table entry of p
 // candidates in (plo, phi] (p with x/p in the window); pi(v) = base + odd
@@ -624,7 +668,14 @@ void launch_p2(cpx_ctx *ctx, const Plan &pl)
 {
     if (!pl.n_p2) return;
     KSpan ks(ctx, "k_p2");
-    if (pl.wide)
+    if (pl.p2_primes) {
+        if (pl.wide)
+            k_p2_primes<u128><<<grid_for(ctx, pl.n_p2), kThreads, 0, ctx->stream>>>(pl.qd, pl.Q, pl.pre_p2, pl.n_p2,
+                                                                                    ctx->tab.P, ctx->tab.T, pl.acc);
+        else
+            k_p2_primes<uint64_t><<<grid_for(ctx, pl.n_p2), kThreads, 0, ctx->stream>>>(
+                pl.qd, pl.Q, pl.pre_p2, pl.n_p2, ctx->tab.P, ctx->tab.T, pl.acc);
+    } else if (pl.wide)
         k_p2<u128><<<grid_for(ctx, pl.n_p2), kThreads, 0, ctx->stream>>>(pl.qd, pl.Q, pl.pre_p2, pl.n_p2,
                                                                          ctx->tab.T, pl.acc);
     else

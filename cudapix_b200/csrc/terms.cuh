@@ -12,7 +12,8 @@ struct __align__(16) QD {
     uint32_t c, nb;                 // nb = pi(r4)
     uint32_t lbits, direct;         // hard segment = 2^lbits odd numbers; direct = count by table
     uint64_t nseg;                  // hard-leaf segments over [0, z]
-    uint32_t p2win, pad;            // p2win: P2 by pi-table windows over [sqrt x, z] (z beyond the table)
+    uint32_t p2win;                 // P2 by pi-table windows over [sqrt x, z] (z beyond the table)
+    uint32_t piy;                   // pi(y) when P2 walks the prime list (Plan::p2_primes)
     uint64_t seg0;                  // first hard-leaf segment (a part of a query split over GPUs)
 };
 
@@ -102,6 +103,7 @@ struct Plan {
     const EasyLvl *elv = nullptr;
     uint32_t n_elv = 0;
     uint64_t n_ecomp = 0;
+    bool p2_primes = false;        // P2 units are the primes of (y, sqrt x] (k_p2_primes), else pi-table entries
     uint64_t *easy_off = nullptr;  // n_easy + 1 chunk offsets of the easy leaves
     void *easy_rec = nullptr;      // n_easy unit plans (EasyRec, 64 B each), or null: k_easy plans itself
     HardLevel *hard_levels = nullptr;  // per-level outputs of query 0 (a part of a split query)

@@ -1,13 +1,13 @@
 """cpx_quot40_core and cpx_quot40_small (cudapix_b200/csrc/cpx_int.cuh), the
-leaf quotient floor(n / d) for n < 2^40 and d < 2^32 (d < 2^31 for the form
-corrected in 32 bits) of the easy and hard leaves: their host forms, given
-every reciprocal estimate the hardware approximation may return (the
-correctly rounded reciprocal of float(d) and the floats one ulp either side
-of it), against integer division on 3 x 10^7 random operands and on edge
+quotient floor(n / d) for n < 2^53, d < 2^32 and a quotient below 2^41 (d <
+2^31 for the form corrected in 32 bits) of the leaves and of P2: their host
+forms, given every reciprocal estimate the hardware approximation may return
+(the correctly rounded reciprocal of float(d) and the floats one ulp either
+side of it), against integer division on 5 x 10^7 random operands and on edge
 operands (exact multiples and their neighbours, divisors that do not fit a
-float, dividends near 2^40).  The host form rounds the product up exactly,
-as the device's __dmul_ru does; the device form is checked through the leaf
-terms of the GPU tests.  CPU only."""
+float, dividends near 2^40 and 2^53).  The host form rounds the product up
+exactly, as the device's __dmul_ru does; the device form is checked through
+the leaf and P2 terms of the GPU tests.  CPU only."""
 import os
 import subprocess
 import tempfile
@@ -34,7 +34,7 @@ static uint64_t rnd()  // xorshift128+
 static long bad = 0, checked = 0;
 static void check(uint64_t n, uint64_t d)
 {
-    if (!d || d >> 32 || n >> 40) return;
+    if (!d || d >> 32 || n >> 53 || (n / d) >> 41) return;
     const uint64_t want = n / d;
     const float rn = 1.0f / (float)d;
     for (int k = -1; k <= 1; k++) {
@@ -73,11 +73,15 @@ int main(int argc, char **argv)
         check(q * d, d);
         if (q) check(q * d - 1, d);
         check(rnd() >> 24, d);
+        check(rnd() >> 11, d);                                  // n < 2^53 (quotient < 2^41 only)
+        const uint64_t q2 = rnd() >> (64 - 1 - (int)(rnd() % 41));  // quotient < 2^41
+        if (q2 && d < (1ull << 53) / q2) check(q2 * d + rnd() % d, d);
     }
     const uint64_t ds[] = {1, 2, 3, 7, 127, 65535, (1ull << 24) - 1, 1ull << 24, (1ull << 24) + 1, (1ull << 24) + 3,
                            1000003, 2147483647ull, 2147483648ull, 0xFFFFFFFBull, 0xFFFFFFFFull};
     for (uint64_t d : ds)
-        for (uint64_t n : {0ull, 1ull, (1ull << 40) - 1, (1ull << 40) - 2, (1ull << 39), 1099511627689ull})
+        for (uint64_t n : {0ull, 1ull, (1ull << 40) - 1, (1ull << 40) - 2, (1ull << 39), 1099511627689ull,
+                           (1ull << 53) - 1, (1ull << 53) - 2, 9007199254740881ull})
             for (int64_t o = -2; o <= 2; o++) {
                 check(n + o, d);
                 const uint64_t m = (n / d) * d;
