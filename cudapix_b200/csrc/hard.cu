@@ -63,6 +63,7 @@ __global__ void __launch_bounds__(512, 2) k_hard(const QD *__restrict__ qd, uint
     const uint64_t seg = unit - pre_seg[q] + d.seg0;
     const uint64_t lo = seg * 2 * (uint64_t)L;
     const uint64_t lo_w = lo + 2 * (uint64_t)Lw * warp, hi_w = lo_w + 2 * (uint64_t)Lw;
+    const bool q41 = hi_w <= (1ull << 41);  // leaf quotients lie in [lo_w, hi_w)
     const uint64_t off = seg_off[unit];
     if (off + (B - c) > cap) return;  // the host sized the ragged outputs exactly; never write past them
     const XT x = xload<XT>(d);
@@ -189,7 +190,7 @@ __global__ void __launch_bounds__(512, 2) k_hard(const QD *__restrict__ qd, uint
                         __syncwarp();
                         for (uint32_t jj = lane; jj < nbuf; jj += 32) {
                             const uint32_t e = lbuf[jj];
-                            const uint32_t cv = sub_count(leaf_quot(xp, xpd, e & 0x7FFFFFFFu));
+                            const uint32_t cv = sub_count(leaf_quot(xp, xpd, e & 0x7FFFFFFFu, q41));
                             if (e >> 31) {
                                 S += cv;
                                 msl += 1;
@@ -217,7 +218,7 @@ __global__ void __launch_bounds__(512, 2) k_hard(const QD *__restrict__ qd, uint
                                     while (qb) {
                                         const int j = __ffsll((long long)qb) - 1;
                                         qb &= qb - 1;
-                                        S += sub_count(leaf_quot(xp, xpd, 128 * wq + 2 * j + 1));  // mu(q) = -1
+                                        S += sub_count(leaf_quot(xp, xpd, 128 * wq + 2 * j + 1, q41));  // mu(q) = -1
                                         msl += 1;
                                     }
                                     continue;
@@ -330,6 +331,7 @@ __global__ void __launch_bounds__(kThreads) k_hard_leaves(const HardJob *__restr
         const XT xp = (XT)J.xp;
         const double xpd = (double)(uint64_t)xp;
         const uint64_t lo = J.lo;
+        const bool q41 = lo + (2ull << lbits_sub) <= (1ull << 41);  // the sub-segment ends below 2^41
         // survivors of the sub-segment with n <= uu (the carry is added per unit)
         auto count = [&](uint64_t uu) -> uint32_t {
             const uint32_t kk = (uint32_t)((uu - lo + 1) >> 1);
@@ -346,7 +348,7 @@ __global__ void __launch_bounds__(kThreads) k_hard_leaves(const HardJob *__restr
             __syncwarp();
             for (uint32_t jj = lane; jj < nbuf; jj += 32) {
                 const uint32_t e = lbuf[jj];
-                const uint32_t cv = count(leaf_quot(xp, xpd, e & 0x7FFFFFFFu));
+                const uint32_t cv = count(leaf_quot(xp, xpd, e & 0x7FFFFFFFu, q41));
                 if (e >> 31) {
                     S += cv;
                     ms += 1;
@@ -382,7 +384,7 @@ __global__ void __launch_bounds__(kThreads) k_hard_leaves(const HardJob *__restr
                     while (qb) {
                         const int j = __ffsll((long long)qb) - 1;
                         qb &= qb - 1;
-                        S += count(leaf_quot(xp, xpd, 128 * wq + 2 * j + 1));  // mu(q) = -1
+                        S += count(leaf_quot(xp, xpd, 128 * wq + 2 * j + 1, q41));  // mu(q) = -1
                         ms += 1;
                     }
                     continue;

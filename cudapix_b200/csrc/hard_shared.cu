@@ -384,11 +384,9 @@ template <class XT> __device__ __forceinline__ void hard_shared_unit(uint64_t un
     __syncwarp();
     const uint64_t w = seg * NW + warp;
     auto sub_count = [&](uint64_t uu) -> uint32_t { return sub_survivors_pre(uu, lo_w, wl, pre16, bm, CPT, s, warp); };
-    // the leaf quotient x/(p m): cpx_quot40 when x < 2^64 and x/p < 2^40 (xpd = x/p as a double)
-    auto hq = [&](XT xv, double xvd, uint64_t m) -> uint64_t {
-        if (sizeof(XT) == 8 && (uint64_t)xv < (1ull << 40)) return cpx_quot40((uint64_t)xv, xvd, (uint32_t)m);
-        return (uint64_t)cpx_qdiv(xv, m);
-    };
+    // the leaf quotient x/(p m) (leaf_quot: cpx_quot40 when x/p < 2^53; xvd = x/p as a double)
+    const bool q41 = hi_w <= (1ull << 41);  // leaf quotients lie in [lo_w, hi_w)
+    auto hq = [&](XT xv, double xvd, uint64_t m) -> uint64_t { return leaf_quot(xv, xvd, m, q41); };
     const Recip r_lo{lo_w, lo_w ? 1.0 / (double)lo_w : 0.0}, r_hi{hi_w, 1.0 / (double)hi_w};
 
     for (uint32_t gb = c + 1; gb <= B; gb += 32) {

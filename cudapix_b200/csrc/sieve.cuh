@@ -342,11 +342,12 @@ __device__ __forceinline__ uint32_t cross_off(uint32_t *bm, uint8_t *cnt8, uint3
     return cleared;
 }
 
-// A leaf quotient x/(p m) = xp / m: cpx_quot40 when x < 2^64 and xp < 2^40
-// (xpd = xp as a double), else cpx_qdiv.
-template <class XT> __device__ __forceinline__ uint64_t leaf_quot(XT xp, double xpd, uint64_t m)
+// A leaf quotient x/(p m) = xp / m of a leaf in a sub-segment that ends at
+// or below 2^41 (q41, so the quotient is below 2^41): cpx_quot40 when xp <
+// 2^53 (xpd = xp as a double, exact), else cpx_qdiv.
+template <class XT> __device__ __forceinline__ uint64_t leaf_quot(XT xp, double xpd, uint64_t m, bool q41)
 {
-    if (sizeof(XT) == 8 && (uint64_t)xp < (1ull << 40)) return cpx_quot40((uint64_t)xp, xpd, (uint32_t)m);
+    if (q41 && ((u128)xp >> 53) == 0) return cpx_quot40((uint64_t)xp, xpd, (uint32_t)m);
     return (uint64_t)cpx_qdiv(xp, m);
 }
 

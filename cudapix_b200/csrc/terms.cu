@@ -489,9 +489,10 @@ __global__ void __launch_bounds__(kThreads) k_easy(const QD *__restrict__ qd, ui
         if (r < e.nsp) {
             const uint64_t k0 = e.kq0 + 1 + r * kEasySparse, k1 = min(e.kq1, e.kq0 + (r + 1) * kEasySparse);
             // x < 2^64 and x/p < 2^40: every quotient below 2^30 (u < sqrt(x) and
-            // x < 2^60 here), taken by cpx_pi_quot40; else x/p < 2^53 and x/p^2 <
-            // 2^44 (q > p): cpx_quot53; else the general quotient.  One loop per
-            // case, two leaves a lane a step (their quotients and gathers overlap).
+            // x < 2^60 here), taken by cpx_pi_quot40; else x/p < 2^53 with
+            // quotients below 2^41 (x/p < 2^41 qlo): cpx_quot40; below 2^44:
+            // cpx_quot53; else the general quotient.  One loop per case, two
+            // leaves a lane a step (their quotients and gathers overlap).
             const uint32_t *Pq = P + (k0 - 1);
             const uint32_t nq = (uint32_t)(k1 - k0 + 1);
             const double xpd = (double)(uint64_t)xp;
@@ -502,6 +503,13 @@ __global__ void __launch_bounds__(kThreads) k_easy(const QD *__restrict__ qd, ui
                 for (; t + 32 < nq; t += 64)
                     ps += cpx_pi_quot40(T, n, xpd, __ldg(Pq + t)) + cpx_pi_quot40(T, n, xpd, __ldg(Pq + t + 32));
                 if (t < nq) ps += cpx_pi_quot40(T, n, xpd, __ldg(Pq + t));
+            } else if (xp < ((XT)1 << 53) && ((uint64_t)xp >> 41) < e.qlo) {
+                // quotients below 2^41 (q > qlo): cpx_quot40
+                const uint64_t n = (uint64_t)xp;
+                for (; t + 32 < nq; t += 64)
+                    ps += cpx_pi_ge2(T, cpx_quot40(n, xpd, __ldg(Pq + t))) +
+                          cpx_pi_ge2(T, cpx_quot40(n, xpd, __ldg(Pq + t + 32)));
+                if (t < nq) ps += cpx_pi_ge2(T, cpx_quot40(n, xpd, __ldg(Pq + t)));
             } else if (xp < ((XT)1 << 53) && ((uint64_t)xp >> 44) < e.qlo) {
                 const uint64_t n = (uint64_t)xp;
                 for (; t + 32 < nq; t += 64)
@@ -518,15 +526,13 @@ __global__ void __launch_bounds__(kThreads) k_easy(const QD *__restrict__ qd, ui
             const uint64_t j = r - e.nsp;
             const uint64_t k0 = e.klo + 1 + j * kEasyClu, k1 = min(e.khi, e.klo + (j + 1) * kEasyClu);
             uint64_t ps = 0;
-            // x/(p p_k) <= qhi < 2^31 for k > klo: cpx_quot40 when x < 2^64 and
-            // x/p < 2^40, cpx_quot53 when x/p < 2^53, else cpx_qdiv
-            const bool f40 = sizeof(XT) == 8 && (uint64_t)xp < (1ull << 40);
-            const bool f53 = !f40 && xp < ((XT)1 << 53);
+            // x/(p p_k) <= qhi < 2^31 for k > klo: cpx_quot40 when x/p < 2^53,
+            // else cpx_qdiv
+            const bool f40 = xp < ((XT)1 << 53);
             const double xpd = (double)(uint64_t)xp;
             auto g = [&](uint64_t k) -> uint64_t {
                 const uint32_t pk = __ldg(P + k - 1);
-                uint64_t v = f40 ? cpx_quot40((uint64_t)xp, xpd, pk)
-                                 : (f53 ? cpx_quot53((uint64_t)xp, xpd, pk) : (uint64_t)cpx_qdiv(xp, (uint64_t)pk));
+                uint64_t v = f40 ? cpx_quot40((uint64_t)xp, xpd, pk) : (uint64_t)cpx_qdiv(xp, (uint64_t)pk);
                 v = v < e.q1 ? e.q1 : (v > e.qhi ? e.qhi : v);
                 return cpx_pi_ge2(T, v);
             };
