@@ -491,8 +491,7 @@ __global__ void __launch_bounds__(kThreads) k_easy(const QD *__restrict__ qd, ui
             // x < 2^64 and x/p < 2^40: every quotient below 2^30 (u < sqrt(x) and
             // x < 2^60 here), taken by cpx_pi_quot40; else x/p < 2^53 with
             // quotients below 2^41 (x/p < 2^41 qlo): cpx_quot40; below 2^44:
-            // cpx_quot53; else the general quotient.  One loop per case, two
-            // leaves a lane a step (their quotients and gathers overlap).
+            // cpx_quot53; else the general quotient.  One loop per case.
             const uint32_t *Pq = P + (k0 - 1);
             const uint32_t nq = (uint32_t)(k1 - k0 + 1);
             const double xpd = (double)(uint64_t)xp;
@@ -500,16 +499,24 @@ __global__ void __launch_bounds__(kThreads) k_easy(const QD *__restrict__ qd, ui
             uint32_t t = lane;
             if (sizeof(XT) == 8 && (uint64_t)xp < (1ull << 40)) {
                 const uint64_t n = (uint64_t)xp;
-                for (; t + 32 < nq; t += 64)
-                    ps += cpx_pi_quot40(T, n, xpd, __ldg(Pq + t)) + cpx_pi_quot40(T, n, xpd, __ldg(Pq + t + 32));
-                if (t < nq) ps += cpx_pi_quot40(T, n, xpd, __ldg(Pq + t));
+                // four leaves a lane a step: their table gathers overlap
+                for (; t + 96 < nq; t += 128) {
+                    const uint32_t d0 = __ldg(Pq + t), d1 = __ldg(Pq + t + 32), d2 = __ldg(Pq + t + 64),
+                                   d3 = __ldg(Pq + t + 96);
+                    ps += (cpx_pi_quot40(T, n, xpd, d0) + cpx_pi_quot40(T, n, xpd, d1)) +
+                          (cpx_pi_quot40(T, n, xpd, d2) + cpx_pi_quot40(T, n, xpd, d3));
+                }
+                for (; t < nq; t += 32) ps += cpx_pi_quot40(T, n, xpd, __ldg(Pq + t));
             } else if (xp < ((XT)1 << 53) && ((uint64_t)xp >> 41) < e.qlo) {
-                // quotients below 2^41 (q > qlo): cpx_quot40
+                // quotients below 2^41 (q > qlo): cpx_quot40, four leaves a step
                 const uint64_t n = (uint64_t)xp;
-                for (; t + 32 < nq; t += 64)
-                    ps += cpx_pi_ge2(T, cpx_quot40(n, xpd, __ldg(Pq + t))) +
-                          cpx_pi_ge2(T, cpx_quot40(n, xpd, __ldg(Pq + t + 32)));
-                if (t < nq) ps += cpx_pi_ge2(T, cpx_quot40(n, xpd, __ldg(Pq + t)));
+                for (; t + 96 < nq; t += 128) {
+                    const uint32_t d0 = __ldg(Pq + t), d1 = __ldg(Pq + t + 32), d2 = __ldg(Pq + t + 64),
+                                   d3 = __ldg(Pq + t + 96);
+                    ps += (cpx_pi_ge2(T, cpx_quot40(n, xpd, d0)) + cpx_pi_ge2(T, cpx_quot40(n, xpd, d1))) +
+                          (cpx_pi_ge2(T, cpx_quot40(n, xpd, d2)) + cpx_pi_ge2(T, cpx_quot40(n, xpd, d3)));
+                }
+                for (; t < nq; t += 32) ps += cpx_pi_ge2(T, cpx_quot40(n, xpd, __ldg(Pq + t)));
             } else if (xp < ((XT)1 << 53) && ((uint64_t)xp >> 44) < e.qlo) {
                 const uint64_t n = (uint64_t)xp;
                 for (; t + 32 < nq; t += 64)
@@ -537,8 +544,8 @@ __global__ void __launch_bounds__(kThreads) k_easy(const QD *__restrict__ qd, ui
                 return cpx_pi_ge2(T, v);
             };
             uint64_t k = k0 + lane;
-            for (; k + 32 <= k1; k += 64) ps += g(k) + g(k + 32);
-            if (k <= k1) ps += g(k);
+            for (; k + 96 <= k1; k += 128) ps += (g(k) + g(k + 32)) + (g(k + 64) + g(k + 96));
+            for (; k <= k1; k += 32) ps += g(k);
             i128 add = (i128)ps;
             if (j == 0 && lane == 0)
                 add += ((i128)e.klo - (i128)b + 2) * (i128)cpx_pi_dev(T, e.qhi) -
