@@ -385,8 +385,14 @@ template <class XT> __device__ __forceinline__ void hard_shared_unit(uint64_t un
     const uint64_t w = seg * NW + warp;
     auto sub_count = [&](uint64_t uu) -> uint32_t { return sub_survivors_pre(uu, lo_w, wl, pre16, bm, CPT, s, warp); };
     // the leaf quotient x/(p m) (leaf_quot: cpx_quot40 when x/p < 2^53; xvd = x/p as a double)
-    const bool q41 = hi_w <= (1ull << 41);  // leaf quotients lie in [lo_w, hi_w)
-    auto hq = [&](XT xv, double xvd, uint64_t m) -> uint64_t { return leaf_quot(xv, xvd, m, q41); };
+    // leaf quotients lie in [lo_w, hi_w): below 2^31 - 2 the 32-bit corrected
+    // form (m <= y < 2^31), below 2^41 cpx_quot40 (both for x/p < 2^53)
+    const bool q41 = hi_w <= (1ull << 41), q31 = hi_w <= (1ull << 31) - 2;
+    auto hq = [&](XT xv, double xvd, uint64_t m) -> uint64_t {
+        if (q31 && ((u128)xv >> 53) == 0)
+            return cpx_quot40_small((uint64_t)xv, xvd, (uint32_t)m, cpx_rcp_approx((uint32_t)m));
+        return leaf_quot(xv, xvd, m, q41);
+    };
     const Recip r_lo{lo_w, lo_w ? 1.0 / (double)lo_w : 0.0}, r_hi{hi_w, 1.0 / (double)hi_w};
 
     for (uint32_t gb = c + 1; gb <= B; gb += 32) {

@@ -368,7 +368,8 @@ __device__ __forceinline__ uint32_t chunk_survivors(uint4 v4, uint32_t jb)
 __device__ __forceinline__ uint32_t sub_survivors(uint64_t uu, uint64_t lo_w, const uint32_t *wl, const uint8_t *cnt8,
                                                   const uint32_t *bm, uint32_t CPT, int s, uint32_t warp)
 {
-    const uint32_t kk = (uint32_t)((uu - lo_w + 1) >> 1);  // bits [0, kk) of the sub-segment
+    // bits [0, kk) of the sub-segment; uu - lo_w < 2^21, so its low 32 bits suffice
+    const uint32_t kk = ((uint32_t)uu - (uint32_t)lo_w + 1u) >> 1;
     if (!kk) return 0u;
     const uint32_t jb = kk - 1, w = jb >> 5;
     const uint32_t chs = w >> 2, ow = chs >> s;  // chunk in the sub-segment, owning lane
@@ -429,7 +430,8 @@ __device__ __forceinline__ uint32_t sub_survivors_pre(uint64_t uu, uint64_t lo_w
                                                       const uint16_t *pre16, const uint32_t *bm, uint32_t CPT, int s,
                                                       uint32_t warp)
 {
-    const uint32_t kk = (uint32_t)((uu - lo_w + 1) >> 1);  // bits [0, kk) of the sub-segment
+    // bits [0, kk) of the sub-segment; uu - lo_w < 2^21, so its low 32 bits suffice
+    const uint32_t kk = ((uint32_t)uu - (uint32_t)lo_w + 1u) >> 1;
     if (!kk) return 0u;
     const uint32_t jb = kk - 1;
     const uint32_t chs = jb >> 7;               // chunk in the sub-segment
