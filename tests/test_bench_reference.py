@@ -57,12 +57,12 @@ def test_roofline_from_profiles_and_live_spans():
         def sm_count(self):
             return 148
 
-    kern = [{"k_easy": 15.3, "k_hard_shared": 21.0, "k_p2": 2.4}] * 3
-    roof, shares = bench.roofline(kern, [22.0] * 3, [1e11] * 3, [40.0] * 3, {"sm_mhz": 1965.0}, Ctx())
+    kern = [{"k_easy": 12.8, "k_hard_shared": 20.5, "k_p2": 2.4}] * 3
+    roof, shares = bench.roofline(kern, [21.5] * 3, [1e11] * 3, [37.0] * 3, {"sm_mhz": 1965.0}, Ctx())
     assert roof["bound"] == "alu" and roof["kernel"].startswith("k_hard_shared")
     assert roof["other"]["kernel"].startswith("k_easy")
     for r in (roof, roof["other"]):
         assert r["profile_matches_source"] is True, r["profile"]
         assert 0.3 < r["frac"] < 1.0
         assert abs(r["peak"] - 2.0 * 148 * 1965e6 / 1e9) < 1e-6
-    assert abs(shares["k_hard_shared"]["share"] - 21.0 / 40.0) < 1e-9
+    assert abs(shares["k_hard_shared"]["share"] - 20.5 / 37.0) < 1e-9
