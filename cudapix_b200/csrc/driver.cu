@@ -83,14 +83,14 @@ bool dr_domain_ok(u128 x, uint64_t y, uint32_t c)
     return true;
 }
 
-// An upper bound of x^(2/5), at most 2^31: the u primes an easy leaf's
-// clustered part needs (the kernels fall back to single leaves above the
-// resident prime list, so the bound only has to be close).
 // P2 takes its primes from the prime list for sqrt x up to this bound (the
 // list then holds up to 28 M primes, 112 MB); beyond it from pi-table bitmaps
 constexpr uint64_t kP2PrimeMax = 1ull << 29;
 static uint64_t tb_prm_max(const cpx_ctx *ctx) { return ctx->tab.P ? ctx->tab.prm_max : 0; }
 
+// An upper bound of x^(2/5), at most 2^31: the u primes an easy leaf's
+// clustered part needs (the kernels fall back to single leaves above the
+// resident prime list, so the bound only has to be close).
 static uint64_t easy_u_bound(u128 x)
 {
     const long double v = powl((long double)x, 0.4L) * 1.001L + 16.0L;
