@@ -367,10 +367,14 @@ def _u128_array(xs):
     n = len(xs)
     arr = (U128 * max(n, 1))()
     if n:
-        ints = [int(x) for x in xs]
         w = np.frombuffer(arr, dtype=np.uint64).reshape(-1, 2)
-        w[:n, 0] = [x & _M64 for x in ints]
-        w[:n, 1] = [(x >> 64) & _M64 for x in ints]
+        a = np.asarray(xs) if isinstance(xs, (list, tuple, np.ndarray)) else None
+        if a is not None and a.ndim == 1 and a.dtype.kind in "iu" and (a.dtype.kind == "u" or a.min() >= 0):
+            w[:n, 0] = a.astype(np.uint64)  # integers below 2^64: one conversion, high words stay 0
+        else:
+            ints = [int(x) for x in xs]
+            w[:n, 0] = [x & _M64 for x in ints]
+            w[:n, 1] = [(x >> 64) & _M64 for x in ints]
     return arr
 
 
