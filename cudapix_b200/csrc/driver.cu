@@ -93,8 +93,8 @@ static uint64_t tb_prm_max(const cpx_ctx *ctx) { return ctx->tab.P ? ctx->tab.pr
 // resident prime list, so the bound only has to be close).
 static uint64_t easy_u_bound(u128 x)
 {
-    const long double v = powl((long double)x, 0.4L) * 1.001L + 16.0L;
-    return v >= 2147483648.0L ? 2147483648ull : (uint64_t)v;
+    const double v = std::pow((double)x, 0.4) * 1.001 + 16.0;
+    return v >= 2147483648.0 ? 2147483648ull : (uint64_t)v;
 }
 
 // Segments (of `span` integers) that sieve level b, p = p_b: those with
@@ -886,14 +886,21 @@ replan:  // again without the batch alpha when its shared sieve would not fit (b
             lvl_off[lv + 1] = lvl_off[lv] + NW * n;
             ent += (double)n;
         }
+        // every bound below is at most r4max: count among the first nbm primes
+        const auto pend = hP.begin() + std::min<size_t>(hP.size(), nbm + 1);
         for (const uint64_t u : units) {
             // levels the unit sieves: those of its first group (the largest x)
             const HardGroup &hg = groups[(u >> 4) & 0x0FFFFFFF];
             const uint64_t lo = (u >> 32) * span, hi = lo + span;
             uint64_t v = hg.r4max;
-            if (lo) v = std::min<uint64_t>(v, cpx_isqrt((hg.xmax - 1) / lo));
+            if (lo) {
+                const u128 t = (hg.xmax >> 64) ? (hg.xmax - 1) / lo : (u128)((uint64_t)(hg.xmax - 1) / lo);
+                v = std::min<uint64_t>(v, cpx_isqrt(t));
+            }
             v = std::min<uint64_t>(v, cpx_isqrt((u128)(hi - 1)));
-            const uint64_t nb = host_pi(hP, v);
+            const uint64_t nb = (uint64_t)(std::upper_bound(hP.begin(), pend, v,
+                                                            [](uint64_t a, uint32_t b) { return a < b; }) -
+                                           hP.begin());
             if (nb > c) ent += (double)(nb - c);
         }
         hard_bytes = ent * (double)(1ull << sh_lbits) / 8.0;
