@@ -260,8 +260,9 @@ static __device__ __noinline__ bool offload_sets(bool off_j, uint32_t lane, uint
 // Candidate entries (pi-table words or 4-m groups) a lane answers itself;
 // above it on any lane the warp gathers the level's leaves (on the B200 the
 // 4096-query batch took 49.0 / 46.0 / 41.4 / 40.9 ms of this kernel with 8 /
-// 16 / 32 / 64)
-constexpr uint32_t kLaneEntries = 64;
+// 16 / 32 / 64 when each unit held one group; with blocks of groups 20.9 /
+// 20.5 / 20.4 ms with 32 / 64 / 128)
+constexpr uint32_t kLaneEntries = 128;
 
 // (3) One CTA per (group, segment).  Per level, the lanes hold one query
 // each: its x/p and candidate range in the warp's sub-segment.  When no query
