@@ -264,11 +264,12 @@ static __device__ __noinline__ bool offload_sets(bool off_j, uint32_t lane, uint
 // 20.5 / 20.4 ms with 32 / 64 / 128)
 constexpr uint32_t kLaneEntries = 128;
 
-// (3) One CTA per (group, segment).  Per level, the lanes hold one query
-// each: its x/p and candidate range in the warp's sub-segment.  When no query
-// has more than kLaneEntries candidate table entries (98% of the visits of
-// the 4096-query batch, with about 1.3 entries a query), each lane answers
-// its own query's leaves into its 128-bit total.
+// (3) One CTA per unit: a segment and a block of up to kBlockMax groups.  Per
+// level and group, the lanes hold one query each: its x/p and candidate range
+// in the warp's sub-segment.  When no query has more than kLaneEntries
+// candidate table entries (98% of the visits of the 4096-query batch, with
+// about 1.3 entries a query), each lane answers its own query's leaves and
+// adds them into the query's slot of the unit's sums.
 // Otherwise the warp walks the candidates of all the group's queries as one
 // sequence (pi-table words of the prime-only levels, then 4-m groups of
 // packed mu*lpf of the others), 32 words at a time, each lane finding its
@@ -277,7 +278,7 @@ constexpr uint32_t kLaneEntries = 128;
 // are answered 32 at a time.  Each lane keeps a running Sum(-mu) * count and
 // Sum(-mu) for the query of its last leaf and adds them into the warp's
 // per-query slots when the query changes; at the end of the level lane j
-// folds slot j into its total as sum + carry * Sum(-mu).
+// adds slot j into its query's unit sum as sum + carry * Sum(-mu).
 // The launch bounds (at most TMAX threads, at least MINB blocks per SM) set
 // the register budget: 65536 / (TMAX MINB) a thread, 64 when 32 warps share
 // an SM and 128 (no spills) when 16 do.  The launch takes the variant whose
